@@ -1,0 +1,17 @@
+"""cohsearch -- B200 engine for CoherentSearch.jl's coherent search hot path.
+
+The public names mirror the Julia API (src/CoherentSearch.jl:17-51); the hot
+loop runs in ``libcohsearch_cuda.so`` (sm_100a) through its C ABI.
+"""
+from ._lib import CohSearchError, LIB_PATH, load as load_library
+from .fileio import FFTFile, SimpleInf, freqs, write_fft
+from .search import (Candidate, Engine, SearchCache, SearchParams, boxcar_widths, chunk_metrics,
+                     decimation_set, ladder_boxcar_widths, proftype, remove_duplicates,
+                     remove_harmonics, search, write_candidates)
+
+__all__ = [
+    "CohSearchError", "LIB_PATH", "load_library", "FFTFile", "SimpleInf", "freqs", "write_fft",
+    "Candidate", "Engine", "SearchCache", "SearchParams", "boxcar_widths", "chunk_metrics",
+    "decimation_set", "ladder_boxcar_widths", "proftype", "remove_duplicates", "remove_harmonics",
+    "search", "write_candidates",
+]

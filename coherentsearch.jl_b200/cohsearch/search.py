@@ -1,0 +1,356 @@
+"""Host mirror of CoherentSearch.jl's search API over the B200 engine.
+
+Same names, argument meaning and error behaviour as the Julia API
+(src/CoherentSearch.jl:17-51): ``SearchParams``, ``decimation_set``,
+``search``, ``SearchCache``, ``chunk_metrics``, ``Candidate``,
+``remove_duplicates``, ``remove_harmonics``, ``write_candidates``.  The hot
+loop runs in ``libcohsearch_cuda.so`` through the C ABI; only the
+post-processing of the few hundred raw detections (duplicate and harmonic
+collapse, src/search.jl:2148-2214) runs here, as it runs in Julia in the
+reference.  Invalid arguments raise ``ValueError`` (Julia ``ArgumentError``).
+"""
+import ctypes
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+
+# ---------------------------------------------------------------------------
+# Parameters (src/search.jl:131-167, 387-459)
+# ---------------------------------------------------------------------------
+
+
+@dataclass(eq=False)
+class SearchParams:
+    """Tunable search parameters, defaults as src/search.jl:131-144.
+
+    ``synth`` selects the device profile-synthesis arithmetic: ``"fp32"`` (the
+    plain FP32 GPU form), ``"bf16"`` or ``"bf16x3"`` (tensor-core forms).
+    Equality is identity, as ``SearchCache`` keys on the object.
+    """
+    nharms: int = 32
+    m: int = 16
+    numbetween: int = 16
+    hidr: float = 0.5
+    threshold: float = 8.0
+    boxcar_fsp: float = 1.5
+    boxcar_maxfrac: float = 0.3
+    boxcar_medmargin: float = 2.0
+    decimations: List[int] = field(default_factory=lambda: [1])
+    precision: str = "f64"
+    synth: str = "fp32"
+
+    def to_c(self):
+        if self.m % 2:
+            raise ValueError("m must be even")
+        if self.precision not in ("f64", "f32"):
+            raise ValueError(f"precision must be :f64 or :f32, got {self.precision}")
+        if self.synth not in _lib.CS_SYNTH:
+            raise ValueError(f"synth must be one of {sorted(_lib.CS_SYNTH)}")
+        if len(self.decimations) > _lib.CS_MAX_DECIM:
+            raise ValueError("at most 16 decimation factors")
+        p = _lib.cs_params()
+        p.nharms = int(self.nharms)
+        p.m = int(self.m)
+        p.numbetween = int(self.numbetween)
+        p.ndecim = len(self.decimations)
+        for i, k in enumerate(self.decimations):
+            p.decimations[i] = int(k)
+        p.hidr = float(self.hidr)
+        p.threshold = float(self.threshold)
+        p.boxcar_fsp = float(self.boxcar_fsp)
+        p.boxcar_maxfrac = float(self.boxcar_maxfrac)
+        p.boxcar_medmargin = float(self.boxcar_medmargin)
+        p.precision = 0 if self.precision == "f64" else 1
+        p.synth = _lib.CS_SYNTH[self.synth]
+        return p
+
+
+def proftype(params: SearchParams):
+    """src/search.jl:152-156."""
+    if params.precision == "f64":
+        return np.float64
+    if params.precision == "f32":
+        return np.float32
+    raise ValueError(f"precision must be :f64 or :f32, got {params.precision}")
+
+
+def decimation_set(nharms: int, maxdecim: int) -> List[int]:
+    """src/search.jl:166-167."""
+    return [k for k in range(1, max(1, maxdecim) + 1) if nharms // k >= 2]
+
+
+def boxcar_widths(nbins: int, fsp: float = 1.5, maxfrac: float = 0.3) -> List[int]:
+    """src/search.jl:387-396."""
+    wmax = max(1, math.floor(maxfrac * nbins))
+    ws, w = [], 1
+    while w <= wmax:
+        ws.append(w)
+        w = max(math.floor(fsp * w), w + 1)
+    return ws
+
+
+def ladder_boxcar_widths(nbins: int, k: int, params: SearchParams) -> List[int]:
+    """src/search.jl:443-459."""
+    ws = boxcar_widths(nbins, params.boxcar_fsp, params.boxcar_maxfrac)
+    ks = sorted(params.decimations)
+    if len(ks) <= 1 or not all(ks[i + 1] <= 3 * ks[i] for i in range(len(ks) - 1)):
+        return ws
+    kmin, kmax = ks[0], ks[-1]
+    pruned = [w for w in ws if (w >= 2 or k == kmin) and (w <= 6 or k == kmax)]
+    return pruned or ws
+
+
+# ---------------------------------------------------------------------------
+# Candidates and post-processing (src/search.jl:179-191, 2148-2214)
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class Candidate:
+    """src/search.jl:179-191, plus the decimation factor and global trial."""
+    freq: float
+    metric: float
+    r: float
+    nharm: int
+    ducy: float = math.nan
+    k: int = 1
+    trial: int = -1
+
+
+def remove_duplicates(cands: Sequence[Candidate], dr_tol: float = 1.0) -> List[Candidate]:
+    """Collapse runs of near-identical ``r`` to their strongest member."""
+    if not cands:
+        return []
+    order = sorted(range(len(cands)), key=lambda i: cands[i].r)
+    kept = []
+    best = cands[order[0]]
+    prev = best.r
+    for i in order[1:]:
+        c = cands[i]
+        if c.r - prev <= dr_tol:
+            if c.metric > best.metric:
+                best = c
+        else:
+            kept.append(best)
+            best = c
+        prev = c.r
+    kept.append(best)
+    return sorted(kept, key=lambda c: c.freq)
+
+
+def _harmonically_related(r1: float, r2: float, numharm: int, tol: float) -> bool:
+    lo, hi = min(r1, r2), max(r1, r2)
+    if not lo > 0:
+        return False
+    for m in range(1, numharm + 1):
+        n = int(round(m * hi / lo))
+        if 1 <= n <= numharm and abs(m * hi - n * lo) <= tol * m:
+            return True
+    return False
+
+
+def remove_harmonics(cands: Sequence[Candidate], numharm: int = 16, tol: float = 1.0) -> List[Candidate]:
+    """Keep the strongest member of each harmonically related family."""
+    if not cands:
+        return []
+    order = sorted(range(len(cands)), key=lambda i: -cands[i].metric)
+    kept: List[Candidate] = []
+    for i in order:
+        c = cands[i]
+        if not any(_harmonically_related(c.r, k.r, numharm, tol) for k in kept):
+            kept.append(c)
+    return sorted(kept, key=lambda c: c.freq)
+
+
+def write_candidates(cands: Sequence[Candidate], outfile: str, threshold) -> None:
+    """The ``.cohout`` table of src/cli.jl:317-340 ('' writes to stdout)."""
+    lines = ["#       'S/N'      Frequency (Hz)        Period (ms)    #Harm  Ducy(%)"]
+    for i, c in enumerate(cands, 1):
+        ducy = "-" if math.isnan(c.ducy) else f"{100 * c.ducy:.2f}"
+        lines.append(f"{i:<4d}  {c.metric:8.2f}  {c.freq:18.12f}  {1000.0 / c.freq:18.12f}   "
+                     f"{c.nharm:3d}   {ducy:>6s}")
+    if not outfile:
+        print("\n".join(lines))
+        import sys
+        print(f"# {len(cands)} candidates above threshold {threshold}", file=sys.stderr)
+    else:
+        with open(outfile, "w") as f:
+            f.write("\n".join(lines) + "\n")
+
+
+# ---------------------------------------------------------------------------
+# Device engine
+# ---------------------------------------------------------------------------
+
+
+class Engine:
+    """One ``cs_handle``: the device plans, buffers and stream for one
+    ``SearchParams`` (the SearchCache's workspaces, src/search.jl:1914-1961)."""
+
+    def __init__(self, params: SearchParams, device: int = 0):
+        self.lib = _lib.load()
+        self.params = params
+        self.device = device
+        self._h = ctypes.c_void_p()
+        cp = params.to_c()
+        st = self.lib.cs_create(ctypes.byref(self._h), ctypes.byref(cp), int(device))
+        if st == _lib.CS_ERR_INVALID_ARGUMENT:
+            raise ValueError("invalid SearchParams")
+        _lib.check(st, None, "cs_create")
+        self._spec_key = None
+        self._spec_keep = None
+
+    def close(self):
+        if self._h:
+            self.lib.cs_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr):
+        """Issue the engine's work on a caller's cudaStream_t (int pointer; 0 = own)."""
+        _lib.check(self.lib.cs_set_stream(self._h, ctypes.c_void_p(int(stream_ptr) or None)), self._h)
+
+    # -- spectrum ---------------------------------------------------------
+    def set_spectrum(self, ft, force=False):
+        key = (id(ft), ft.N, len(ft.amps))
+        if key == self._spec_key and not force:
+            return
+        amps = np.ascontiguousarray(ft.amps, dtype=np.complex64)
+        st = self.lib.cs_set_spectrum(self._h, amps.ctypes.data, len(amps), int(ft.N), float(ft.inf.dt))
+        _lib.check(st, self._h, "cs_set_spectrum")
+        self._spec_key = key
+
+    def set_spectrum_host(self, ptr: int, namps: int, N: int, dt: float):
+        """Copy a spectrum from host memory at ``ptr`` (pinned for full speed)."""
+        st = self.lib.cs_set_spectrum(self._h, ctypes.c_void_p(ptr), int(namps), int(N), float(dt))
+        _lib.check(st, self._h, "cs_set_spectrum")
+        self._spec_key = ("host", ptr, namps, N)
+
+    def set_spectrum_device(self, ptr: int, namps: int, N: int, dt: float, keep=None):
+        """Attach a spectrum already resident on the device (no copy)."""
+        st = self.lib.cs_set_spectrum_device(self._h, ctypes.c_void_p(ptr), int(namps), int(N), float(dt))
+        _lib.check(st, self._h, "cs_set_spectrum_device")
+        self._spec_key = ("device", ptr, namps, N)
+        self._spec_keep = keep
+
+    # -- calls ------------------------------------------------------------
+    def search_raw(self, lofreq=0.1, hifreq=100.0, lobin=100, blocksize=2048, threshold=None,
+                   exact_all=False, cap=1 << 16) -> np.ndarray:
+        thr = self.params.threshold if threshold is None else threshold
+        while True:
+            out = np.zeros(cap, dtype=_lib.CAND_DTYPE)
+            n = ctypes.c_int64()
+            st = self.lib.cs_search(self._h, float(lofreq), float(hifreq), int(lobin), int(blocksize),
+                                    float(thr), int(bool(exact_all)), out.ctypes.data, cap,
+                                    ctypes.byref(n))
+            if st == _lib.CS_ERR_CAPACITY and n.value > cap:
+                cap = int(n.value)
+                continue
+            _lib.check(st, self._h, "cs_search")
+            return out[:n.value]
+
+    def stats(self) -> dict:
+        s = _lib.cs_stats()
+        _lib.check(self.lib.cs_search_stats(self._h, ctypes.byref(s)), self._h, "cs_search_stats")
+        return {n: getattr(s, n) for n, _ in s._fields_}
+
+    def block_values(self):
+        n = ctypes.c_int64()
+        self.lib.cs_search_block_values(self._h, None, None, 0, ctypes.byref(n))
+        sig = np.zeros(n.value, np.float32)
+        nv = np.zeros(n.value, np.int32)
+        _lib.check(self.lib.cs_search_block_values(self._h, sig.ctypes.data, nv.ctypes.data, n.value,
+                                                   ctypes.byref(n)), self._h)
+        return sig, nv
+
+    def trial_metrics(self):
+        n = ctypes.c_int64()
+        self.lib.cs_search_trial_metrics(self._h, None, 0, ctypes.byref(n))
+        out = np.zeros(n.value, np.float32)
+        _lib.check(self.lib.cs_search_trial_metrics(self._h, out.ctypes.data, n.value, ctypes.byref(n)),
+                   self._h)
+        return out
+
+    def chunk_metrics(self, rstart: float, n: int) -> np.ndarray:
+        out = np.zeros(int(n), np.float64)
+        _lib.check(self.lib.cs_chunk_metrics(self._h, float(rstart), int(n), out.ctypes.data), self._h,
+                   "cs_chunk_metrics")
+        return out
+
+    def interp_chunk(self, r_lo: float, t0: int, n: int) -> np.ndarray:
+        out = np.zeros((self.params.nharms, int(n)), np.complex64)
+        _lib.check(self.lib.cs_interp_chunk(self._h, float(r_lo), int(t0), int(n), out.ctypes.data),
+                   self._h, "cs_interp_chunk")
+        return out
+
+
+class SearchCache:
+    """Reusable per-``SearchParams`` device engine (src/search.jl:1914-1961).
+
+    Reuse is keyed on the ``params`` object identity, as in the reference.
+    """
+
+    def __init__(self):
+        self.params = None
+        self.engine: Optional[Engine] = None
+
+    def engine_for(self, params: SearchParams, device: int = 0) -> Engine:
+        if self.engine is None or self.params is not params or self.engine.device != device:
+            if self.engine is not None:
+                self.engine.close()
+            self.engine = Engine(params, device)
+            self.params = params
+        return self.engine
+
+
+def _to_candidates(raw: np.ndarray) -> List[Candidate]:
+    return [Candidate(float(c["freq"]), float(c["metric"]), float(c["r"]), int(c["nharm"]),
+                      math.nan, int(c["k"]), int(c["trial"])) for c in raw]
+
+
+def search(ft, params: SearchParams = None, lofreq=0.1, hifreq=100.0, lobin=100, blocksize=2048,
+           threshold=None, remove=True, dr_tol=1.0, harm_remove=True, numharm=16, harm_tol=1.0,
+           progress="none", metricstats=None, normalize=False, verbose=False, wisdom=True,
+           wisdom_file=None, cache: Optional[SearchCache] = None, device: int = 0) -> List[Candidate]:
+    """Coherent harmonic-summing search over ``[lofreq, hifreq]`` Hz
+    (src/search.jl:2002-2111) on the device.
+
+    ``wisdom``/``wisdom_file`` are accepted for compatibility; no FFTW plans
+    exist on the device path.  ``metricstats``/``normalize`` are not built.
+    """
+    params = SearchParams() if params is None else params
+    if progress not in ("none", "text", "bar"):
+        raise ValueError(f"progress must be :none, :text or :bar, got :{progress}")
+    if metricstats is not None or normalize:
+        raise NotImplementedError("metricstats/normalize are not built on the device path yet")
+    thr = params.threshold if threshold is None else threshold
+    eng = cache.engine_for(params, device) if cache is not None else Engine(params, device)
+    eng.set_spectrum(ft)
+    raw = eng.search_raw(lofreq, hifreq, lobin, blocksize, thr)
+    cands = _to_candidates(raw)
+    if remove:
+        cands = remove_duplicates(cands, dr_tol)
+    else:
+        cands = sorted(cands, key=lambda c: c.freq)
+    if harm_remove:
+        cands = remove_harmonics(cands, numharm, harm_tol)
+    return cands
+
+
+def chunk_metrics(ft, params: SearchParams, rstart: float, n: int, lodr=None, cache=None,
+                  device: int = 0) -> np.ndarray:
+    """Equivalence bridge (src/search.jl:1740-1755) on the device."""
+    if lodr is not None and lodr != params.hidr / params.nharms:
+        raise ValueError("lodr must equal hidr/nharms")
+    eng = cache.engine_for(params, device) if cache is not None else Engine(params, device)
+    eng.set_spectrum(ft)
+    return eng.chunk_metrics(rstart, n)

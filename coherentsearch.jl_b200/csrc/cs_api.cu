@@ -1,0 +1,775 @@
+// cs_api.cu -- host side of libcohsearch_cuda.so: the C ABI of cohsearch.h,
+// the FP64 plan tables, the decimation levels and the wave orchestration.
+//
+// All FP64 bookkeeping that decides bin ranges, trial counts, valid decimated
+// trials and candidate frequencies is evaluated here with the reference's own
+// expressions (no contraction: built with -ffp-contract=off), so those values
+// are bit-identical to the reference's.
+#include "cohsearch.h"
+#include "cs_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace cs;
+
+#define CS_VERSION_STRING "cohsearch-b200 0.1.0 (sm_100a)"
+
+namespace {
+
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t need) {
+        if (need == 0) need = 16;
+        if (need <= bytes) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, need);
+        if (e == cudaSuccess) bytes = need;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+struct LevelHost {
+    int k, Hk, nbins;
+    std::vector<int> widths;
+};
+
+// sin(pi x), cos(pi x) for x in [0, 1), reduced so that pi*x is formed only on
+// [0, 1/4]; the reference uses Julia's sinpi/cispi (src/directinterp.jl:392).
+double sinpi_d(double x) {
+    if (x <= 0.25) return std::sin(M_PI * x);
+    if (x <= 0.75) return std::cos(M_PI * (x - 0.5));
+    return std::sin(M_PI * (1.0 - x));
+}
+double cospi_d(double x) {
+    if (x <= 0.25) return std::cos(M_PI * x);
+    if (x <= 0.75) return -std::sin(M_PI * (x - 0.5));
+    return -std::cos(M_PI * (1.0 - x));
+}
+
+int64_t gcd64(int64_t a, int64_t b) {
+    while (b) {
+        int64_t t = a % b;
+        a = b;
+        b = t;
+    }
+    return a < 0 ? -a : a;
+}
+
+// trial_grid_rational (src/directinterp.jl:217-225): the smallest-denominator
+// rational p/q, q <= 2^16, within 8 eps(lodr) of lodr.  Two distinct rationals
+// with denominators <= 2^16 are >= 2^-32 apart, so a scan over q finds exactly
+// the value `rationalize(Int, lodr; tol=1e-13)` returns whenever the reference
+// accepts it.
+bool trial_grid_rational(double lodr, int64_t* pnum, int64_t* q) {
+    if (!(lodr > 0)) return false;
+    const double eps8 = 8.0 * (std::nextafter(lodr, INFINITY) - lodr);
+    for (int64_t qq = 1; qq <= (1 << 16); ++qq) {
+        const double pp = std::nearbyint(lodr * (double)qq);
+        if (pp >= 1 && std::fabs(pp / (double)qq - lodr) <= eps8) {
+            const int64_t g = gcd64((int64_t)pp, qq);
+            *pnum = (int64_t)pp / g;
+            *q = qq / g;
+            return true;
+        }
+    }
+    return false;
+}
+
+// boxcar_widths (src/search.jl:387-396).
+std::vector<int> boxcar_widths(int nbins, double fsp, double maxfrac) {
+    const int64_t wmax = std::max<int64_t>(1, (int64_t)std::floor(maxfrac * (double)nbins));
+    std::vector<int> ws;
+    int64_t w = 1;
+    while (w <= wmax) {
+        ws.push_back((int)w);
+        w = std::max<int64_t>((int64_t)std::floor(fsp * (double)w), w + 1);
+        if (ws.size() > 4096) break;
+    }
+    return ws;
+}
+
+// ladder_boxcar_widths (src/search.jl:443-459).
+std::vector<int> ladder_widths(int nbins, int k, const cs_params& p) {
+    std::vector<int> ws = boxcar_widths(nbins, p.boxcar_fsp, p.boxcar_maxfrac);
+    std::vector<int> ks(p.decimations, p.decimations + p.ndecim);
+    std::sort(ks.begin(), ks.end());
+    if (ks.size() <= 1) return ws;
+    for (size_t i = 0; i + 1 < ks.size(); ++i)
+        if (!(ks[i + 1] <= 3 * ks[i])) return ws;  // _LADDER_WMAX ÷ 2 = 3
+    const int kmin = ks.front(), kmax = ks.back();
+    std::vector<int> pr;
+    for (int w : ws)
+        if ((w >= 2 || k == kmin) && (w <= 6 || k == kmax)) pr.push_back(w);
+    return pr.empty() ? ws : pr;
+}
+
+struct HostPlans {
+    std::vector<DevHarm> harms;
+    std::vector<float> w;
+    std::vector<float2> a;
+    std::vector<uint8_t> c;
+};
+
+// build_direct_plans with Float32 weights (src/directinterp.jl:342-405): every
+// table entry computed in FP64 and rounded once.  The device indexes W as
+// [i][p] so that consecutive trials (consecutive p) read consecutive words.
+void build_plans(const cs_params& p, double r_lo, HostPlans& out) {
+    const double lodr = p.hidr / (double)p.nharms;
+    int64_t pnum = 1, q = 1;
+    const bool rq = trial_grid_rational(lodr, &pnum, &q);
+    const int m = p.m, m2 = m / 2;
+    out.harms.clear();
+    out.w.clear();
+    out.a.clear();
+    out.c.clear();
+    for (int h = 1; h <= p.nharms; ++h) {
+        const double hr = (double)h * r_lo;
+        const double fl = std::floor(hr);
+        DevHarm d{};
+        d.h = h;
+        d.rfloor0 = (int64_t)fl;
+        d.dr0 = hr - fl;
+        d.hr_lo = (double)d.rfloor0 + d.dr0;
+        d.dh = (double)h * lodr;
+        if (!rq) {
+            d.P = 0;
+            d.q = 1;
+            d.pnum = 1;
+            out.harms.push_back(d);
+            continue;
+        }
+        const int64_t step = (int64_t)h * pnum;
+        const int64_t s = step % q;
+        const int64_t P = q / gcd64(step, q);
+        d.P = (int32_t)P;
+        d.q = (int32_t)q;
+        d.pnum = (int32_t)pnum;
+        d.w_off = (int64_t)out.w.size();
+        d.a_off = (int64_t)out.a.size();
+        out.w.resize(out.w.size() + (size_t)m * P);
+        out.a.resize(out.a.size() + P);
+        out.c.resize(out.c.size() + P);
+        int64_t res = 0;
+        for (int64_t pp = 0; pp < P; ++pp) {
+            const double u = d.dr0 + (double)res / (double)q;
+            const bool carry = u >= 1.0;
+            const double dr = carry ? u - 1.0 : u;
+            out.c[d.a_off + pp] = carry ? 1 : 0;
+            if (dr == 0.0) {
+                out.a[d.a_off + pp] = make_float2(1.0f, 0.0f);
+                for (int i = 0; i < m; ++i) out.w[d.w_off + (int64_t)i * P + pp] = (i == m2 - 1) ? 1.0f : 0.0f;
+            } else {
+                const double sn = sinpi_d(dr), cs_ = cospi_d(dr);
+                const double ar = (sn * cs_) / M_PI;
+                const double ai = -((sn * sn) / M_PI);
+                out.a[d.a_off + pp] = make_float2((float)ar, (float)ai);
+                for (int i = 0; i < m; ++i)
+                    out.w[d.w_off + (int64_t)i * P + pp] = (float)(1.0 / (dr - (double)(i + 1 - m2)));
+            }
+            res += s;
+            if (res >= q) res -= q;
+        }
+        out.harms.push_back(d);
+    }
+}
+
+}  // namespace
+
+struct cs_handle {
+    cs_params p{};
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;      // the stream work is issued on
+    cudaStream_t own_stream = nullptr;  // the handle's own stream
+    std::string err;
+    std::vector<LevelHost> levels;
+    int maxbins = 0, maxwmax = 0;
+    std::vector<DevLevel> dlev;
+    // spectrum
+    const float2* amps = nullptr;
+    DBuf amps_owned;
+    int64_t namps = 0, N = 0;
+    double dt = 0.0;
+    bool has_spec = false;
+    int64_t spec_h2d_bytes = 0;   // bytes of the last host spectrum copy, charged to the next search
+    // device buffers
+    DBuf d_levels, d_tw, d_harms, d_wtab, d_atab, d_ctab, d_nvalid, d_X, d_Q0, d_sub, d_sigma,
+        d_tmetric, d_items, d_counts, d_cands;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cs_stats stats{};
+    std::vector<float> last_sigma;
+    std::vector<int32_t> last_nvalid;
+    std::vector<float> last_tmetric;
+    int last_nlev = 0;
+    int last_Nprof = 0;
+};
+
+namespace {
+
+cs_status fail(cs_handle* H, cs_status st, const std::string& msg) {
+    if (H) H->err = msg;
+    return st;
+}
+
+cs_status cuda_fail(cs_handle* H, cudaError_t e, const char* where) {
+    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+    return fail(H, e == cudaErrorMemoryAllocation ? CS_ERR_OUT_OF_MEMORY : CS_ERR_CUDA, m);
+}
+
+#define CS_CUDA(call, where)                                   \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return cuda_fail(H, e_, where); \
+    } while (0)
+
+template <class T>
+cudaError_t upload(DBuf& b, const std::vector<T>& v, cudaStream_t st) {
+    cudaError_t e = b.ensure(v.size() * sizeof(T));
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+cs_status validate(const cs_params* p) {
+    if (!p) return CS_ERR_INVALID_ARGUMENT;
+    if (p->nharms < 1) return CS_ERR_INVALID_ARGUMENT;
+    if (p->m < 2 || (p->m % 2) != 0) return CS_ERR_INVALID_ARGUMENT;  // "m must be even"
+    if (!(p->hidr > 0)) return CS_ERR_INVALID_ARGUMENT;
+    if (p->ndecim < 0 || p->ndecim > CS_MAX_DECIM) return CS_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < p->ndecim; ++i)
+        if (p->decimations[i] < 1 || p->nharms / p->decimations[i] < 1) return CS_ERR_INVALID_ARGUMENT;
+    if (p->precision != 0 && p->precision != 1) return CS_ERR_INVALID_ARGUMENT;
+    if (!(p->boxcar_fsp > 0) || !(p->boxcar_maxfrac > 0)) return CS_ERR_INVALID_ARGUMENT;
+    if (p->synth != CS_SYNTH_FP32 && p->synth != CS_SYNTH_BF16 && p->synth != CS_SYNTH_BF16X3)
+        return CS_ERR_INVALID_ARGUMENT;
+    return CS_OK;
+}
+
+// Levels: the base fold k = 1, then every k > 1 of params.decimations in
+// order (Workspace.decims, src/search.jl:1251-1254).
+cs_status build_levels(cs_handle* H) {
+    const cs_params& p = H->p;
+    std::vector<int> ks{1};
+    for (int i = 0; i < p.ndecim; ++i)
+        if (p.decimations[i] > 1) ks.push_back(p.decimations[i]);
+    if ((int)ks.size() > kMaxLevels) return fail(H, CS_ERR_UNSUPPORTED, "more than 16 decimation levels");
+    H->levels.clear();
+    H->dlev.clear();
+    H->maxbins = 0;
+    H->maxwmax = 0;
+    std::vector<float> tw;
+    for (int k : ks) {
+        LevelHost L;
+        L.k = k;
+        L.Hk = p.nharms / k;
+        L.nbins = 2 * L.Hk;
+        L.widths = ladder_widths(L.nbins, k, p);
+        if (L.nbins > kMaxBins) return fail(H, CS_ERR_UNSUPPORTED, "nharms > 128 is not built");
+        if ((int)L.widths.size() > kMaxWidths)
+            return fail(H, CS_ERR_UNSUPPORTED, "more than 64 boxcar widths per level");
+        if (L.widths.back() > kMaxBins)
+            return fail(H, CS_ERR_UNSUPPORTED, "boxcar widths wider than 256 bins");
+        DevLevel d{};
+        d.k = k;
+        d.Hk = L.Hk;
+        d.nbins = L.nbins;
+        d.nw = (int)L.widths.size();
+        d.wmax = L.widths.back();
+        d.np = ((L.Hk + 1) + 7) / 8 * 8;
+        d.tw_off = (int64_t)tw.size();
+        for (int i = 0; i < d.nw; ++i) {
+            d.widths[i] = L.widths[i];
+            d.rsqrtw[i] = (float)(1.0 / std::sqrt((double)L.widths[i]));
+        }
+        const int Nb = L.nbins;
+        tw.resize(tw.size() + 2 * (size_t)L.Hk * d.np, 0.0f);
+        float* C2 = tw.data() + d.tw_off;
+        float* S2 = C2 + (size_t)L.Hk * d.np;
+        for (int j = 1; j < L.Hk; ++j)
+            for (int n = 0; n <= L.Hk; ++n) {
+                const double ang = 2.0 * M_PI * (double)(((int64_t)j * n) % Nb) / (double)Nb;
+                C2[(size_t)j * d.np + n] = (float)(2.0 * std::cos(ang));
+                S2[(size_t)j * d.np + n] = (float)(-2.0 * std::sin(ang));
+            }
+        H->maxbins = std::max(H->maxbins, L.nbins);
+        H->maxwmax = std::max(H->maxwmax, d.wmax);
+        H->levels.push_back(L);
+        H->dlev.push_back(d);
+    }
+    CS_CUDA(upload(H->d_levels, H->dlev, H->stream), "upload levels");
+    CS_CUDA(upload(H->d_tw, tw, H->stream), "upload twiddles");
+    return CS_OK;
+}
+
+// Number of trials j < n of a block whose k-fold lies below Nyquist: the
+// prefix `decim_pass!` scores (src/search.jl:1680-1683), found by bisection
+// on the same (monotone) FP64 predicate.
+int nvalid_decim(int k, double rstart, double lodr, int n, double nyq) {
+    auto ok = [&](int j) { return (double)k * (rstart + (double)j * lodr) < nyq; };
+    if (n <= 0 || !ok(0)) return 0;
+    if (ok(n - 1)) return n;
+    int lo = 0, hi = n - 1;  // ok(lo), !ok(hi)
+    while (hi - lo > 1) {
+        const int mid = lo + (hi - lo) / 2;
+        if (ok(mid)) lo = mid; else hi = mid;
+    }
+    return hi;
+}
+
+struct RunSpec {
+    double r_lo;          // plan anchor: global trial 0 sits at r_lo
+    double lodr;
+    int64_t nblocks;
+    int Nprof;
+    int64_t t_base;       // global trial of block 0
+    int64_t t_end;        // one past the last global trial
+    int nlev;             // levels used (prefix of H->levels)
+    bool exact_all;
+    float threshold;
+    float medcut;
+    bool interp_only;     // stop after interpolation (cs_interp_chunk)
+    bool keep_diag;       // keep sigma/nvalid/tmetric of the run on the host
+};
+
+cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands, float2* x_out) {
+    const cs_params& p = H->p;
+    HostPlans plans;
+    build_plans(p, R.r_lo, plans);
+    for (const DevHarm& d : plans.harms) {
+        const double lim = 4.6e18;
+        if ((double)R.t_end * (double)d.h * (double)d.pnum > lim)
+            return fail(H, CS_ERR_UNSUPPORTED, "trial index times harmonic overflows 64-bit phase state");
+    }
+    CS_CUDA(upload(H->d_harms, plans.harms, H->stream), "upload plans");
+    CS_CUDA(upload(H->d_wtab, plans.w, H->stream), "upload weights");
+    CS_CUDA(upload(H->d_atab, plans.a, H->stream), "upload phases");
+    CS_CUDA(upload(H->d_ctab, plans.c, H->stream), "upload carries");
+    const int64_t plan_bytes = (int64_t)(plans.harms.size() * sizeof(DevHarm) + plans.w.size() * sizeof(float) +
+                                         plans.a.size() * sizeof(float2) + plans.c.size());
+
+    const int Nprof = R.Nprof;
+    const int win_max = (int)std::ceil((double)(Nprof - 1 + 64) * p.hidr) + p.m + 4;
+    if ((size_t)win_max * sizeof(float2) > 200 * 1024)
+        return fail(H, CS_ERR_UNSUPPORTED, "blocksize*hidr too large for the shared-memory bin window");
+    int maxbins = 0, maxwmax = 0;
+    for (int l = 0; l < R.nlev; ++l) {
+        maxbins = std::max(maxbins, H->dlev[l].nbins);
+        maxwmax = std::max(maxwmax, H->dlev[l].wmax);
+    }
+    const size_t smem_synth = synth_fp32_smem(p.nharms, maxbins, maxwmax);
+    if (smem_synth > 227 * 1024) return fail(H, CS_ERR_UNSUPPORTED, "profile tile exceeds shared memory");
+
+    const int nlev = R.nlev;
+    const size_t per_blk = (size_t)p.nharms * Nprof * sizeof(float2) +
+                           (size_t)nlev * Nprof * sizeof(float) * (R.exact_all ? 2 : 1) +
+                           (size_t)nlev * kSigmaCap * sizeof(float) +
+                           (size_t)nlev * Nprof * (sizeof(DevItem) + sizeof(DevCand)) + 64;
+    const size_t budget = (size_t)3 << 30;
+    const int64_t WB = std::max<int64_t>(1, std::min<int64_t>(R.nblocks, (int64_t)(budget / per_blk)));
+
+    CS_CUDA(H->d_X.ensure((size_t)WB * p.nharms * Nprof * sizeof(float2)), "alloc X");
+    if (!R.interp_only) {
+        CS_CUDA(H->d_Q0.ensure((size_t)WB * nlev * Nprof * sizeof(float)), "alloc Q0");
+        CS_CUDA(H->d_sub.ensure((size_t)WB * nlev * kSigmaCap * sizeof(float)), "alloc sub");
+        CS_CUDA(H->d_sigma.ensure((size_t)WB * nlev * sizeof(float)), "alloc sigma");
+        CS_CUDA(H->d_nvalid.ensure((size_t)WB * nlev * sizeof(int32_t)), "alloc nvalid");
+        CS_CUDA(H->d_items.ensure((size_t)WB * nlev * Nprof * sizeof(DevItem)), "alloc items");
+        CS_CUDA(H->d_cands.ensure((size_t)WB * nlev * Nprof * sizeof(DevCand)), "alloc cands");
+        if (R.exact_all)
+            CS_CUDA(H->d_tmetric.ensure((size_t)WB * nlev * Nprof * sizeof(float)), "alloc tmetric");
+    }
+    CS_CUDA(H->d_counts.ensure(4 * sizeof(int32_t)), "alloc counters");
+
+    cs_stats& S = H->stats;
+    S = cs_stats{};
+    S.h2d_bytes = H->spec_h2d_bytes + plan_bytes;
+    H->spec_h2d_bytes = 0;
+    S.blocks = R.nblocks;
+    S.trials = R.t_end - R.t_base;
+    if (R.keep_diag) {
+        H->last_sigma.assign((size_t)R.nblocks * nlev, 0.0f);
+        H->last_nvalid.assign((size_t)R.nblocks * nlev, 0);
+        if (R.exact_all) H->last_tmetric.assign((size_t)R.nblocks * nlev * Nprof, 0.0f);
+        else H->last_tmetric.clear();
+        H->last_nlev = nlev;
+        H->last_Nprof = Nprof;
+    }
+    const double nyq = (double)H->N / 2.0;
+    std::vector<int32_t> nvalid;
+    std::vector<DevCand> wave_c;
+    int32_t counts[4];
+
+    for (int64_t c0 = 0; c0 < R.nblocks; c0 += WB) {
+        const int nb = (int)std::min<int64_t>(WB, R.nblocks - c0);
+        WaveArgs a{};
+        a.amps = H->amps;
+        a.namps = H->namps;
+        a.Nhalf = H->N / 2;
+        a.nharms = p.nharms;
+        a.m = p.m;
+        a.nlev = nlev;
+        a.Nprof = Nprof;
+        a.t_first = R.t_base + c0 * (int64_t)Nprof;
+        a.total = R.t_end;
+        a.nblk = nb;
+        a.blk_base = (int32_t)c0;
+        a.harms = H->d_harms.as<DevHarm>();
+        a.wtab = H->d_wtab.as<float>();
+        a.atab = H->d_atab.as<float2>();
+        a.ctab = H->d_ctab.as<uint8_t>();
+        a.levels = H->d_levels.as<DevLevel>();
+        a.tw = H->d_tw.as<float>();
+        a.nvalid = H->d_nvalid.as<int32_t>();
+        a.X = H->d_X.as<float2>();
+        a.Q0 = H->d_Q0.as<float>();
+        a.sub = H->d_sub.as<float>();
+        a.sigma = H->d_sigma.as<float>();
+        a.tmetric = R.exact_all ? H->d_tmetric.as<float>() : nullptr;
+        a.items = H->d_items.as<DevItem>();
+        a.n_items = H->d_counts.as<int32_t>();
+        a.cap_items = (int32_t)std::min<int64_t>((int64_t)nb * nlev * Nprof, INT32_MAX);
+        a.cands = H->d_cands.as<DevCand>();
+        a.n_cands = H->d_counts.as<int32_t>() + 1;
+        a.cap_cands = a.cap_items;
+        a.threshold = R.threshold;
+        a.medcut = R.medcut;
+        a.exact_all = R.exact_all ? 1 : 0;
+        int* d_err = H->d_counts.as<int32_t>() + 2;
+
+        nvalid.assign((size_t)nb * nlev, 0);
+        for (int b = 0; b < nb; ++b) {
+            const int64_t c = c0 + b;
+            const int64_t i0 = c * (int64_t)Nprof;  // trial offset of the block
+            const int n = (int)std::min<int64_t>(Nprof, R.t_end - (R.t_base + i0));
+            const double rstart = R.r_lo + (double)(R.t_base + i0) * R.lodr;
+            for (int l = 0; l < nlev; ++l) {
+                const int k = H->dlev[l].k;
+                nvalid[(size_t)b * nlev + l] = (k == 1) ? n : nvalid_decim(k, rstart, R.lodr, n, nyq);
+                S.profiles += nvalid[(size_t)b * nlev + l];
+            }
+        }
+        CS_CUDA(cudaMemsetAsync(H->d_counts.p, 0, 4 * sizeof(int32_t), H->stream), "reset counters");
+        CS_CUDA(cudaEventRecord(H->ev[0], H->stream), "event");
+        CS_CUDA(launch_interp(a, H->stream, win_max, d_err), "interp launch");
+        CS_CUDA(cudaEventRecord(H->ev[1], H->stream), "event");
+        S.launches += 1;
+        if (!R.interp_only) {
+            CS_CUDA(upload(H->d_nvalid, nvalid, H->stream), "upload nvalid");
+            S.h2d_bytes += (int64_t)(nvalid.size() * sizeof(int32_t));
+            a.nvalid = H->d_nvalid.as<int32_t>();
+            CS_CUDA(launch_synth_fp32(a, H->stream, (int)smem_synth), "synth launch");
+            CS_CUDA(cudaEventRecord(H->ev[2], H->stream), "event");
+            CS_CUDA(launch_sigma(a, H->stream), "sigma launch");
+            CS_CUDA(cudaEventRecord(H->ev[3], H->stream), "event");
+            if (!R.exact_all) {
+                CS_CUDA(launch_flag(a, H->stream), "flag launch");
+                S.launches += 1;
+            }
+            CS_CUDA(launch_rescue(a, H->stream, H->num_sms), "rescue launch");
+            CS_CUDA(cudaEventRecord(H->ev[4], H->stream), "event");
+            S.launches += 3;
+        }
+        CS_CUDA(cudaMemcpyAsync(counts, H->d_counts.p, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                H->stream),
+                "read counters");
+        CS_CUDA(cudaStreamSynchronize(H->stream), "wave");
+        S.d2h_bytes += 4 * sizeof(int32_t);
+        if (counts[2] != 0) return fail(H, CS_ERR_CUDA, "interpolation window exceeded its bound");
+        float ms = 0.0f;
+        CS_CUDA(cudaEventElapsedTime(&ms, H->ev[0], H->ev[1]), "timing");
+        S.ms_interp += ms;
+        if (!R.interp_only) {
+            CS_CUDA(cudaEventElapsedTime(&ms, H->ev[1], H->ev[2]), "timing");
+            S.ms_synth += ms;
+            CS_CUDA(cudaEventElapsedTime(&ms, H->ev[2], H->ev[3]), "timing");
+            S.ms_sigma += ms;
+            CS_CUDA(cudaEventElapsedTime(&ms, H->ev[3], H->ev[4]), "timing");
+            S.ms_rescue += ms;
+            CS_CUDA(cudaEventElapsedTime(&ms, H->ev[0], H->ev[4]), "timing");
+            S.ms_total += ms;
+        } else {
+            S.ms_total += ms;
+        }
+        S.waves += 1;
+        if (R.interp_only) {
+            if (x_out)
+                CS_CUDA(cudaMemcpy(x_out, H->d_X.p, (size_t)nb * p.nharms * Nprof * sizeof(float2),
+                                   cudaMemcpyDeviceToHost),
+                        "read amplitudes");
+            continue;
+        }
+        const int n_items = counts[0], n_c = counts[1];
+        S.rescued += R.exact_all ? 0 : n_items;
+        S.candidates += n_c;
+        if (!R.exact_all && n_items > a.cap_items) return fail(H, CS_ERR_CAPACITY, "rescue list overflow");
+        if (n_c > a.cap_cands) return fail(H, CS_ERR_CAPACITY, "candidate list overflow");
+        if (cands && n_c > 0) {
+            wave_c.resize(n_c);
+            CS_CUDA(cudaMemcpy(wave_c.data(), H->d_cands.p, (size_t)n_c * sizeof(DevCand),
+                               cudaMemcpyDeviceToHost),
+                    "read candidates");
+            cands->insert(cands->end(), wave_c.begin(), wave_c.end());
+            S.d2h_bytes += (int64_t)n_c * (int64_t)sizeof(DevCand);
+        }
+        if (R.keep_diag) {
+            CS_CUDA(cudaMemcpy(H->last_sigma.data() + (size_t)c0 * nlev, H->d_sigma.p,
+                               (size_t)nb * nlev * sizeof(float), cudaMemcpyDeviceToHost),
+                    "read sigma");
+            std::copy(nvalid.begin(), nvalid.end(), H->last_nvalid.begin() + (size_t)c0 * nlev);
+            S.d2h_bytes += (int64_t)nb * nlev * (int64_t)sizeof(float);
+            if (R.exact_all)
+                CS_CUDA(cudaMemcpy(H->last_tmetric.data() + (size_t)c0 * nlev * Nprof, H->d_tmetric.p,
+                                   (size_t)nb * nlev * Nprof * sizeof(float), cudaMemcpyDeviceToHost),
+                        "read metrics");
+        }
+    }
+    return CS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cs_version(void) { return CS_VERSION_STRING; }
+
+const char* cs_last_error(const cs_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+cs_status cs_create(cs_handle** out, const cs_params* params, int32_t device) {
+    if (!out) return CS_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    cs_status st = validate(params);
+    if (st != CS_OK) return st;
+    if (params->synth != CS_SYNTH_FP32) return CS_ERR_UNSUPPORTED;
+    cs_handle* H = new (std::nothrow) cs_handle();
+    if (!H) return CS_ERR_OUT_OF_MEMORY;
+    H->p = *params;
+    H->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&H->own_stream, cudaStreamNonBlocking);
+    H->stream = H->own_stream;
+    if (e == cudaSuccess) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
+            H->num_sms = sms;
+        for (auto& ev : H->ev)
+            if (e == cudaSuccess) e = cudaEventCreate(&ev);
+    }
+    if (e != cudaSuccess) {
+        cs_destroy(H);
+        return CS_ERR_CUDA;
+    }
+    st = build_levels(H);
+    if (st != CS_OK) {
+        cs_destroy(H);
+        return st;
+    }
+    *out = H;
+    return CS_OK;
+}
+
+cs_status cs_set_stream(cs_handle* H, void* stream) {
+    if (!H) return CS_ERR_INVALID_ARGUMENT;
+    H->stream = stream ? static_cast<cudaStream_t>(stream) : H->own_stream;
+    return CS_OK;
+}
+
+cs_status cs_destroy(cs_handle* H) {
+    if (!H) return CS_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(H->device);
+    if (H->stream) cudaStreamSynchronize(H->stream);
+    if (H->own_stream) cudaStreamSynchronize(H->own_stream);
+    DBuf* bufs[] = {&H->amps_owned, &H->d_levels, &H->d_tw, &H->d_harms, &H->d_wtab, &H->d_atab,
+                    &H->d_ctab, &H->d_nvalid, &H->d_X, &H->d_Q0, &H->d_sub, &H->d_sigma,
+                    &H->d_tmetric, &H->d_items, &H->d_counts, &H->d_cands};
+    for (DBuf* b : bufs) b->release();
+    for (auto& ev : H->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (H->own_stream) cudaStreamDestroy(H->own_stream);
+    delete H;
+    return CS_OK;
+}
+
+static cs_status check_spec_args(cs_handle* H, const float* amps, int64_t namps, int64_t N, double dt) {
+    if (!H) return CS_ERR_INVALID_ARGUMENT;
+    if (!amps || namps < 1 || N < 2 || !(dt > 0))
+        return fail(H, CS_ERR_INVALID_ARGUMENT, "spectrum needs namps >= 1, N >= 2, dt > 0");
+    return CS_OK;
+}
+
+cs_status cs_set_spectrum(cs_handle* H, const float* amps, int64_t namps, int64_t N, double dt) {
+    cs_status st = check_spec_args(H, amps, namps, N, dt);
+    if (st != CS_OK) return st;
+    CS_CUDA(cudaSetDevice(H->device), "set device");
+    CS_CUDA(H->amps_owned.ensure((size_t)namps * sizeof(float2)), "alloc spectrum");
+    CS_CUDA(cudaMemcpyAsync(H->amps_owned.p, amps, (size_t)namps * sizeof(float2), cudaMemcpyHostToDevice,
+                            H->stream),
+            "copy spectrum");
+    H->spec_h2d_bytes = namps * (int64_t)sizeof(float2);
+    H->amps = H->amps_owned.as<float2>();
+    H->namps = namps;
+    H->N = N;
+    H->dt = dt;
+    H->has_spec = true;
+    return CS_OK;
+}
+
+cs_status cs_set_spectrum_device(cs_handle* H, const float* d_amps, int64_t namps, int64_t N, double dt) {
+    cs_status st = check_spec_args(H, d_amps, namps, N, dt);
+    if (st != CS_OK) return st;
+    if ((reinterpret_cast<uintptr_t>(d_amps) & 7u) != 0)
+        return fail(H, CS_ERR_INVALID_ARGUMENT, "device spectrum must be 8-byte aligned");
+    H->amps = reinterpret_cast<const float2*>(d_amps);
+    H->namps = namps;
+    H->N = N;
+    H->dt = dt;
+    H->has_spec = true;
+    return CS_OK;
+}
+
+cs_status cs_search(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
+                    double threshold, int32_t exact_all, cs_candidate* out, int64_t cap, int64_t* n_out) {
+    if (!H || !n_out || (cap > 0 && !out) || cap < 0) return CS_ERR_INVALID_ARGUMENT;
+    *n_out = 0;
+    if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");
+    CS_CUDA(cudaSetDevice(H->device), "set device");
+    const cs_params& p = H->p;
+    // Band bookkeeping of `search` (src/search.jl:2016-2027).
+    const double T = (double)H->N * H->dt;
+    const double lodr = p.hidr / (double)p.nharms;
+    double r_lo = lofreq * T;
+    if (lobin != 100) r_lo = (double)lobin;
+    const double r_hi = hifreq * T;
+    const double span = std::floor((r_hi - r_lo) / lodr);
+    if (!(span == span) || span > 4.0e15) return fail(H, CS_ERR_INVALID_ARGUMENT, "band is not finite");
+    const int64_t total = std::max<int64_t>(0, (int64_t)span + 1);
+    H->stats = cs_stats{};
+    if (total == 0) return CS_OK;
+    const int Nprof = (int)std::max<int64_t>(1, blocksize);
+    if (blocksize > (1 << 16)) return fail(H, CS_ERR_UNSUPPORTED, "blocksize above 65536 is not built");
+    RunSpec R{};
+    R.r_lo = r_lo;
+    R.lodr = lodr;
+    R.Nprof = Nprof;
+    R.nblocks = (total + Nprof - 1) / Nprof;
+    R.t_base = 0;
+    R.t_end = total;
+    R.nlev = (int)H->levels.size();
+    R.exact_all = exact_all != 0;
+    R.threshold = (float)threshold;
+    R.medcut = exact_all ? -INFINITY : (float)(threshold - p.boxcar_medmargin);
+    R.keep_diag = true;
+    std::vector<DevCand> raw;
+    cs_status st = run_blocks(H, R, &raw, nullptr);
+    if (st != CS_OK) return st;
+    // Reference order with one task: by block, base fold then each decimation
+    // level in params order, ascending trial (src/search.jl:1809-1859).
+    std::sort(raw.begin(), raw.end(), [](const DevCand& x, const DevCand& y) {
+        if (x.blk != y.blk) return x.blk < y.blk;
+        if (x.lev != y.lev) return x.lev < y.lev;
+        return x.j < y.j;
+    });
+    const int64_t n = (int64_t)raw.size();
+    for (int64_t i = 0; i < std::min(n, cap); ++i) {
+        const DevCand& c = raw[i];
+        const LevelHost& L = H->levels[c.lev];
+        const int64_t i0 = (int64_t)c.blk * Nprof;
+        const double rstart = r_lo + (double)i0 * lodr;
+        cs_candidate o{};
+        if (L.k == 1) {
+            o.r = rstart + (double)c.j * lodr;           // rf, src/search.jl:1833
+            o.nharm = p.nharms;
+        } else {
+            o.r = (double)L.k * (rstart + (double)c.j * lodr);  // r_dec, src/search.jl:1696
+            o.nharm = L.Hk;
+        }
+        o.freq = o.r / T;
+        o.metric = (double)c.metric;
+        o.k = L.k;
+        o.trial = i0 + c.j;
+        out[i] = o;
+    }
+    *n_out = n;
+    if (n > cap) return fail(H, CS_ERR_CAPACITY, "candidate array too small");
+    return CS_OK;
+}
+
+cs_status cs_search_stats(const cs_handle* H, cs_stats* out) {
+    if (!H || !out) return CS_ERR_INVALID_ARGUMENT;
+    *out = H->stats;
+    return CS_OK;
+}
+
+cs_status cs_chunk_metrics(cs_handle* H, double rstart, int64_t n, double* out) {
+    if (!H || !out || n < 1 || n > (1 << 16)) return CS_ERR_INVALID_ARGUMENT;
+    if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");
+    CS_CUDA(cudaSetDevice(H->device), "set device");
+    RunSpec R{};
+    R.r_lo = rstart;
+    R.lodr = H->p.hidr / (double)H->p.nharms;
+    R.Nprof = (int)n;
+    R.nblocks = 1;
+    R.t_base = 0;
+    R.t_end = n;
+    R.nlev = 1;
+    R.exact_all = true;
+    R.threshold = INFINITY;
+    R.medcut = -INFINITY;
+    R.keep_diag = true;
+    cs_status st = run_blocks(H, R, nullptr, nullptr);
+    if (st != CS_OK) return st;
+    for (int64_t j = 0; j < n; ++j) out[j] = (double)H->last_tmetric[j];
+    return CS_OK;
+}
+
+cs_status cs_interp_chunk(cs_handle* H, double r_lo, int64_t t0, int64_t n, float* out) {
+    if (!H || !out || n < 1 || n > (1 << 16) || t0 < 0) return CS_ERR_INVALID_ARGUMENT;
+    if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");
+    CS_CUDA(cudaSetDevice(H->device), "set device");
+    RunSpec R{};
+    R.r_lo = r_lo;
+    R.lodr = H->p.hidr / (double)H->p.nharms;
+    R.Nprof = (int)n;
+    R.nblocks = 1;
+    R.t_base = t0;
+    R.t_end = t0 + n;
+    R.nlev = 1;
+    R.interp_only = true;
+    return run_blocks(H, R, nullptr, reinterpret_cast<float2*>(out));
+}
+
+cs_status cs_search_block_values(const cs_handle* H, float* sigma, int32_t* nvalid, int64_t cap,
+                                 int64_t* n_out) {
+    if (!H || !n_out) return CS_ERR_INVALID_ARGUMENT;
+    const int64_t n = (int64_t)H->last_sigma.size();
+    *n_out = n;
+    if (cap < n) return CS_ERR_CAPACITY;
+    if (sigma) std::copy(H->last_sigma.begin(), H->last_sigma.end(), sigma);
+    if (nvalid) std::copy(H->last_nvalid.begin(), H->last_nvalid.end(), nvalid);
+    return CS_OK;
+}
+
+cs_status cs_search_trial_metrics(const cs_handle* H, float* out, int64_t cap, int64_t* n_out) {
+    if (!H || !n_out) return CS_ERR_INVALID_ARGUMENT;
+    const int64_t n = (int64_t)H->last_tmetric.size();
+    *n_out = n;
+    if (cap < n) return CS_ERR_CAPACITY;
+    if (out) std::copy(H->last_tmetric.begin(), H->last_tmetric.end(), out);
+    return CS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,106 @@
+// cs_internal.h -- device data layout shared by the host orchestration
+// (cs_api.cu) and the kernels (cs_kernels.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cs {
+
+constexpr int kMaxLevels = 16;     // decimation factors per search
+constexpr int kMaxWidths = 64;     // boxcar widths per level
+constexpr int kMaxBins = 256;      // profile bins (nharms <= 128)
+constexpr int kSigmaCap = 8192;    // _BOXCAR_SIGMA_SAMPLES, src/search.jl:462
+constexpr int kTileTrials = 64;    // trials per CTA in the FP32 synthesis kernel
+
+// One harmonic's rational trial-grid recipe (DirectPlan, src/directinterp.jl:179-204).
+// Global trial t of the search evaluates harmonic h at Fourier frequency
+// h*r_lo + t*h*pnum/q; its phase row is p = t mod P, its integer bin is
+// floor(h*r_t) = rfloor0 + (t*h*pnum) div q + carry[p].
+struct DevHarm {
+    int32_t h;
+    int32_t P;          // phase-cycle length q / gcd(h*pnum, q); 0 => per-trial FP64 path
+    int32_t q;
+    int32_t pnum;
+    int64_t rfloor0;    // floor(h * r_lo)
+    double dr0;         // h*r_lo - rfloor0
+    double hr_lo;       // rfloor0 + dr0 (per-trial path)
+    double dh;          // h * lodr (per-trial path)
+    int64_t w_off;      // W[i][p] at wtab[w_off + i*P + p], i < m
+    int64_t a_off;      // A[p] at atab[a_off + p], carry[p] at ctab[a_off + p]
+};
+
+// One decimation level k: profiles of nbins = 2*Hk bins from base harmonics k, 2k, ..., Hk*k.
+struct DevLevel {
+    int32_t k;
+    int32_t Hk;
+    int32_t nbins;
+    int32_t nw;
+    int32_t wmax;
+    int32_t np;         // padded twiddle row length (multiple of 8, >= Hk+1)
+    int64_t tw_off;     // C2[j][n] at tw[tw_off + j*np + n], S2 at tw[tw_off + Hk*np + j*np + n]
+    int32_t widths[kMaxWidths];
+    float rsqrtw[kMaxWidths];  // 1/sqrt(w), for the gate
+};
+
+// Device candidate record: block, level, trial within block, metric.
+struct DevCand {
+    int32_t blk;
+    int32_t lev;
+    int32_t j;
+    float metric;
+};
+
+// Rescue work item (block, level, trial within block).
+struct DevItem {
+    int32_t blk;
+    int32_t lev;
+    int32_t j;
+    int32_t pad;
+};
+
+// Everything one wave of blocks needs; device pointers.
+struct WaveArgs {
+    const float2* amps;
+    int64_t namps;
+    int64_t Nhalf;
+    int32_t nharms;
+    int32_t m;
+    int32_t nlev;
+    int32_t Nprof;
+    int64_t t_first;        // global trial index of the wave's first block
+    int64_t total;          // trials in the whole search
+    int32_t nblk;           // blocks in this wave
+    int32_t blk_base;       // index of the wave's first block in the search
+    const DevHarm* harms;
+    const float* wtab;
+    const float2* atab;
+    const uint8_t* ctab;
+    const DevLevel* levels;
+    const float* tw;
+    const int32_t* nvalid;  // [nblk][nlev]
+    float2* X;              // [nblk][nharms][Nprof]
+    float* Q0;              // [nblk][nlev][Nprof] zero-baseline gate (unscaled by 1/sigma)
+    float* sub;             // [nblk][nlev][kSigmaCap] |profile| samples for sigma
+    float* sigma;           // [nblk][nlev]
+    float* tmetric;         // [nblk][nlev][Nprof] exact metrics (exact_all mode) or nullptr
+    DevItem* items;         // rescue list
+    int32_t* n_items;
+    int32_t cap_items;
+    DevCand* cands;
+    int32_t* n_cands;
+    int32_t cap_cands;
+    float threshold;
+    float medcut;
+    int32_t exact_all;
+};
+
+// Kernel launchers (cs_kernels.cu).  Each returns the launch error.
+cudaError_t launch_interp(const WaveArgs& a, cudaStream_t st, int win_max, int* err);
+cudaError_t launch_synth_fp32(const WaveArgs& a, cudaStream_t st, int smem_bytes);
+cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st);
+cudaError_t launch_flag(const WaveArgs& a, cudaStream_t st);
+cudaError_t launch_rescue(const WaveArgs& a, cudaStream_t st, int num_sms);
+size_t synth_fp32_smem(int nharms, int maxbins, int maxwmax);
+
+}  // namespace cs

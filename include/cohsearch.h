@@ -1,0 +1,169 @@
+/*
+ * cohsearch.h -- C ABI of libcohsearch_cuda.so, the B200 (sm_100a) engine for
+ * the coherent harmonic-summing search hot path of CoherentSearch.jl.
+ *
+ * The reference has no FFI layer: its seam is the Julia function
+ * `_search_region!` (src/search.jl:1768-1894) called from `search`
+ * (src/search.jl:2002-2111), plus the reference/equivalence entry points
+ * `block_metrics` (src/search.jl:1061-1079) and `chunk_metrics`
+ * (src/search.jl:1740-1755).  Each entry point below names the reference
+ * interface it replaces.  Plain C types only: no CUDA or torch types appear in
+ * these signatures, so Julia (`ccall`), Python (`ctypes`) or C can bind them.
+ *
+ * Error behaviour: every call returns a cs_status; nothing aborts.  Invalid
+ * arguments (the reference's ArgumentError cases) return
+ * CS_ERR_INVALID_ARGUMENT; device failures return CS_ERR_CUDA with text in
+ * cs_last_error().  A handle is not thread-safe (as SearchCache,
+ * src/search.jl:1910-1912); distinct handles may be used concurrently.
+ */
+#ifndef COHSEARCH_H
+#define COHSEARCH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cs_handle cs_handle;
+
+typedef enum cs_status {
+    CS_OK = 0,
+    CS_ERR_INVALID_ARGUMENT = 1, /* bad parameter (reference: ArgumentError) */
+    CS_ERR_NO_SPECTRUM = 2,      /* cs_search before a spectrum was attached */
+    CS_ERR_CAPACITY = 3,         /* output array too small; *n_out = required */
+    CS_ERR_CUDA = 4,             /* CUDA runtime/device error (see cs_last_error) */
+    CS_ERR_OUT_OF_MEMORY = 5,    /* device allocation failed */
+    CS_ERR_TIMEOUT = 6,          /* a bounded device wait ran out */
+    CS_ERR_UNSUPPORTED = 7       /* parameter combination not built */
+} cs_status;
+
+enum { CS_MAX_DECIM = 16 };
+
+/* Profile-synthesis arithmetic on the device. */
+typedef enum cs_synth {
+    CS_SYNTH_FP32 = 0,   /* plain FP32 SIMT synthesis ("plain FP32 GPU form") */
+    CS_SYNTH_BF16 = 1,   /* tcgen05 tensor-core GEMM, BF16 operands, FP32 accumulate */
+    CS_SYNTH_BF16X3 = 2  /* tcgen05 GEMM with split hi+lo BF16 operands (3 products) */
+} cs_synth;
+
+/* Mirrors SearchParams (src/search.jl:131-144). */
+typedef struct cs_params {
+    int32_t nharms;          /* harmonics coherently summed */
+    int32_t m;               /* bins in the interpolation kernel (even) */
+    int32_t numbetween;      /* fine-grid oversampling, reference path only */
+    int32_t ndecim;          /* entries used in decimations[] */
+    int32_t decimations[CS_MAX_DECIM];  /* harmonic-decimation factors k */
+    double hidr;             /* Fourier-bin step at the highest harmonic */
+    double threshold;
+    double boxcar_fsp;
+    double boxcar_maxfrac;
+    double boxcar_medmargin;
+    int32_t precision;       /* reference profile stage: 0 = :f64, 1 = :f32 */
+    int32_t synth;           /* cs_synth */
+} cs_params;
+
+/* One detection (Candidate, src/search.jl:179-191) plus its provenance. */
+typedef struct cs_candidate {
+    double freq;     /* Hz: r / T */
+    double metric;   /* boxcar matched-filter S/N */
+    double r;        /* Fourier frequency in bins (k * fundamental for a k-fold) */
+    int32_t nharm;   /* harmonics summed: floor(nharms / k) */
+    int32_t k;       /* decimation factor that found it */
+    int64_t trial;   /* global index of the fundamental trial */
+} cs_candidate;
+
+/* Per-search counters and device timings, filled by cs_search_stats. */
+typedef struct cs_stats {
+    int64_t trials;          /* fundamental trials searched */
+    int64_t blocks;          /* blocks of `blocksize` trials */
+    int64_t profiles;        /* scored (trial, k) pairs: sum over k of valid trials */
+    int64_t rescued;         /* (trial, k) pairs that took the exact median rescan */
+    int64_t candidates;      /* raw above-threshold detections (before dedup) */
+    int64_t waves;           /* device passes the blocks were split into */
+    int64_t launches;        /* kernels launched by the last call */
+    double ms_interp;        /* CUDA-event time of each stage, summed over waves */
+    double ms_synth;         /* profile synthesis + gate scan */
+    double ms_sigma;
+    double ms_rescue;        /* flag + exact rescan */
+    double ms_total;         /* first to last event of the call */
+    int64_t h2d_bytes;       /* host->device bytes the call copied */
+    int64_t d2h_bytes;       /* device->host bytes the call copied */
+} cs_stats;
+
+/* Create a handle for `params` on CUDA device `device`.  Replaces the setup
+ * half of `search` (plans and workspaces, src/search.jl:2037-2046) and the
+ * SearchCache (src/search.jl:1914-1961): one handle per SearchParams. */
+cs_status cs_create(cs_handle** out, const cs_params* params, int32_t device);
+
+/* Run the handle's work on `stream` (a cudaStream_t passed as void*; NULL
+ * restores the handle's own stream).  Lets a caller order the engine with its
+ * own copies and time it with its own events. */
+cs_status cs_set_stream(cs_handle* h, void* stream);
+
+/* Release all device memory of the handle. */
+cs_status cs_destroy(cs_handle* h);
+
+/* Text of the last error on this handle ("" if none). */
+const char* cs_last_error(const cs_handle* h);
+
+/* Attach a spectrum from HOST memory: namps complex64 values, interleaved
+ * (re, im), amps[0] = DC.re + i*Nyquist, as FFTFile maps it
+ * (src/fileio.jl:64-78); N = time-series length, dt = sample time (s), so
+ * T = N*dt.  The data are copied to the device. */
+cs_status cs_set_spectrum(cs_handle* h, const float* amps, int64_t namps, int64_t N, double dt);
+
+/* As cs_set_spectrum, but `d_amps` is already a DEVICE pointer on the
+ * handle's device.  Nothing is copied; the caller keeps it alive. */
+cs_status cs_set_spectrum_device(cs_handle* h, const float* d_amps, int64_t namps, int64_t N,
+                                 double dt);
+
+/* The hot loop: search fundamentals over [lofreq, hifreq] Hz (or from bin
+ * `lobin` when lobin != 100, the reference's precedence rule) in blocks of
+ * `blocksize` trials, every decimation factor, and write the raw detections
+ * above `threshold` to out[0 .. *n_out).  Replaces `_search_region!`
+ * (src/search.jl:1768-1894) as called by `search` (src/search.jl:2080-2094);
+ * duplicate and harmonic collapse (src/search.jl:2148-2214) stay with the
+ * caller.  exact_all = 1 scores every trial with the exact median baseline
+ * (the reference's medcut = -Inf); 0 uses the zero-baseline gate with
+ * medcut = threshold - boxcar_medmargin.  Candidates come back in the order a
+ * single-task reference run produces them: by block, base fold first then each
+ * decimation factor, ascending trial.  If cap is too small, returns
+ * CS_ERR_CAPACITY with *n_out = the number found (out holds the first cap). */
+cs_status cs_search(cs_handle* h, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
+                    double threshold, int32_t exact_all, cs_candidate* out, int64_t cap,
+                    int64_t* n_out);
+
+/* Counters and stage timings of the last cs_search on this handle. */
+cs_status cs_search_stats(const cs_handle* h, cs_stats* out);
+
+/* Equivalence bridge `chunk_metrics` (src/search.jl:1740-1755): the exact
+ * metric of each of the n trials rstart + j*lodr (one block, global trial 0
+ * at rstart, base fold only), written to out[0..n). */
+cs_status cs_chunk_metrics(cs_handle* h, double rstart, int64_t n, double* out);
+
+/* Interpolated amplitude stack of a chunk (the `ftprofs` rows of
+ * fill_chunk_profiles!, src/search.jl:1280-1290, and fill_harmonic_row_direct!,
+ * src/directinterp.jl:470-572): trials t0 .. t0+n-1 of a search whose global
+ * trial 0 sits at Fourier frequency r_lo.  out is (nharms, n) complex64,
+ * interleaved, harmonic-major; rows the range guard rejects are zero. */
+cs_status cs_interp_chunk(cs_handle* h, double r_lo, int64_t t0, int64_t n, float* out);
+
+/* Diagnostic copies of the last cs_search's per-(block, k) values:
+ * sigma[b * nlev + l] (device block sigma) and nvalid[b * nlev + l]; `cap`
+ * counts entries; nlev = number of decimation factors, l in params order. */
+cs_status cs_search_block_values(const cs_handle* h, float* sigma, int32_t* nvalid, int64_t cap,
+                                 int64_t* n_out);
+
+/* Per-trial metrics of the last cs_search run with exact_all = 1:
+ * out[(b * nlev + l) * blocksize + j]. */
+cs_status cs_search_trial_metrics(const cs_handle* h, float* out, int64_t cap, int64_t* n_out);
+
+/* Library version string. */
+const char* cs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* COHSEARCH_H */

@@ -1,0 +1,78 @@
+"""ctypes binding of the C oracle ``libcs_cpu.so`` (test infrastructure only)."""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        path = _build.build()
+        lib = ctypes.CDLL(path)
+        lib.csref_interp_chunk.restype = ctypes.c_int
+        lib.csref_interp_chunk.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int64,
+                                           ctypes.c_int64, ctypes.c_void_p]
+        lib.csref_plan_tables.restype = ctypes.c_int
+        lib.csref_plan_tables.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_int]
+        lib.csref_search_blocks.restype = ctypes.c_int64
+        lib.csref_search_blocks.argtypes = [
+            ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+            ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int64, ctypes.c_int, ctypes.c_int64,
+            ctypes.c_int64, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
+            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
+        _lib = lib
+    return _lib
+
+
+def interp_chunk(amps, N, nharms, m, hidr, r_lo, t0, n):
+    """(nharms, n) complex64 amplitude stack, FP32-weight production arithmetic."""
+    lib = load()
+    a = np.ascontiguousarray(amps, dtype=np.complex64)
+    out = np.zeros((nharms, n), np.complex64)
+    rc = lib.csref_interp_chunk(a.ctypes.data, len(a), int(N), int(nharms), int(m), float(hidr),
+                                float(r_lo), int(t0), int(n), out.ctypes.data)
+    if rc != 0:
+        raise ValueError("csref_interp_chunk: bad arguments")
+    return out
+
+
+def plan_tables(nharms, m, hidr, r_lo, h, cap=1 << 16):
+    lib = load()
+    W = np.zeros((cap, m), np.float32)
+    A = np.zeros(cap, np.complex64)
+    c = np.zeros(cap, np.uint8)
+    P = lib.csref_plan_tables(int(nharms), int(m), float(hidr), float(r_lo), int(h), W.ctypes.data,
+                              A.ctypes.data, c.ctypes.data, cap)
+    return P, W[:P], A[:P], c[:P].astype(bool)
+
+
+CAND_DTYPE = np.dtype([("blk", "<i4"), ("k", "<i4"), ("j", "<i4"), ("pad", "<f4"), ("metric", "<f8")])
+
+
+def search_blocks(amps, N, dt, nharms, m, hidr, decimations, r_lo, total, blocksize, first_block, nblocks,
+                  threshold, nthreads, exact_all=False, cap=1 << 20):
+    """Run the C port of the production search on blocks [first_block,
+    first_block+nblocks) with `nthreads` threads.  Returns a dict with the
+    candidates (block, k, j, metric), wall seconds and counts."""
+    lib = load()
+    a = np.ascontiguousarray(amps, dtype=np.complex64)
+    dec = np.ascontiguousarray(decimations, dtype=np.int32)
+    out = np.zeros(cap, CAND_DTYPE)
+    sec = ctypes.c_double()
+    resc = ctypes.c_int64()
+    n = lib.csref_search_blocks(a.ctypes.data, len(a), int(N), int(nharms), int(m), float(hidr),
+                                dec.ctypes.data, len(dec), float(r_lo), int(total), int(blocksize),
+                                int(first_block), int(nblocks), float(threshold), int(bool(exact_all)),
+                                int(nthreads), out.ctypes.data, cap, ctypes.byref(sec), ctypes.byref(resc))
+    nblk_real = max(0, min(nblocks, -(-total // blocksize) - first_block))
+    trials = max(0, min(total, (first_block + nblk_real) * blocksize) - first_block * blocksize)
+    return {"cands": out[:min(n, cap)], "ncand": int(n), "seconds": sec.value, "rescued": resc.value,
+            "threads": int(nthreads), "blocks": int(nblk_real), "trials": int(trials)}

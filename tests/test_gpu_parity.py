@@ -1,0 +1,216 @@
+"""Device parity: libcohsearch_cuda.so (through the C ABI) against the oracles.
+
+Tolerances (stated once, used throughout):
+  * amplitudes of the rational trial grid: bit-exact against the C oracle
+    (same FP32 weights, same FMA chain, unfused complex product);
+  * bin ranges, zeroed rows, valid decimated trials, candidate trial indices
+    and decimation factors: exact;
+  * block sigma: |d sigma| / sigma <= 1e-3 (FP32 profiles vs the FP64 oracle
+    can move the median between adjacent order statistics);
+  * S/N: |dS/N| <= 1e-3 * S/N (the plain FP32 path's stated tolerance);
+  * candidate sets: equal outside the exclusion band |S/N - thr| < 1e-3 * thr.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import cs_cpu, cs_ref as o
+from tests.fixtures import PSR_F, multi_spectrum, noise_spectrum, pulsar_spectrum
+
+pytestmark = pytest.mark.gpu
+
+SNR_RTOL = 1e-3
+SIGMA_RTOL = 1e-3
+
+
+def _cs():
+    import cohsearch
+    return cohsearch
+
+
+def _engine(params, amps, N, dt):
+    cs = _cs()
+    eng = cs.Engine(params)
+    eng.set_spectrum(cs.FFTFile.from_array(amps, N, dt))
+    return eng
+
+
+@pytest.mark.parametrize("nharms,m,r_lo,t0,n", [
+    (32, 16, 10010.0, 0, 2048),
+    (60, 32, 5000.0, 0, 256),
+    (60, 16, 4321.7, 777, 1000),        # fractional r_lo, misaligned chunk
+    (32, 16, 123.456, 1_000_003, 37),   # large global trial index
+    (60, 16, 3.0, 0, 512),              # low harmonics fall off the bottom of the file
+    (32, 8, 524288 / 32 - 20.0, 0, 4096),  # top harmonics run past Nyquist
+    (7, 18, 777.77, 12, 300),           # odd nharms, runtime-m kernel
+])
+def test_interp_bitexact_vs_c_oracle(nharms, m, r_lo, t0, n):
+    amps, N, dt = pulsar_spectrum()
+    cs = _cs()
+    eng = _engine(cs.SearchParams(nharms=nharms, m=m), amps, N, dt)
+    got = eng.interp_chunk(r_lo, t0, n)
+    want = cs_cpu.interp_chunk(amps, N, nharms, m, 0.5, r_lo, t0, n)
+    assert got.shape == want.shape
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_interp_nonrational_grid_fp64_path():
+    """A trial step that is no small rational takes the per-trial FP64 path
+    (src/directinterp.jl:623-661)."""
+    amps, N, dt = pulsar_spectrum()
+    cs = _cs()
+    hidr = 0.5 * math.pi / 3.0
+    eng = _engine(cs.SearchParams(nharms=16, m=16, hidr=hidr), amps, N, dt)
+    got = eng.interp_chunk(2000.25, 5, 700)
+    want = cs_cpu.interp_chunk(amps, N, 16, 16, hidr, 2000.25, 5, 700)
+    scale = np.abs(want).max(axis=1, keepdims=True)
+    assert np.array_equal(np.abs(got) == 0, np.abs(want) == 0)
+    assert np.max(np.abs(got - want) / scale) < 1e-6
+
+
+def test_interp_chunk_invariance_on_device():
+    """test/test_search.jl:234-276 on the device: identical bits for any chunking."""
+    amps, N, dt = pulsar_spectrum()
+    cs = _cs()
+    eng = _engine(cs.SearchParams(nharms=32, m=32), amps, N, dt)
+    big = eng.interp_chunk(10010.0, 0, 384)
+    for nsm in (128, 100, 37, 51):
+        t0 = 0
+        while t0 + nsm <= 384:
+            assert np.array_equal(eng.interp_chunk(10010.0, t0, nsm), big[:, t0:t0 + nsm])
+            t0 += nsm
+
+
+@pytest.mark.parametrize("nharms,m,rstart,n", [(32, 32, 10010.0, 256), (60, 16, 5000.0, 2048),
+                                               (60, 32, 9950.0 * 1.0, 500)])
+def test_chunk_metrics_vs_oracle(nharms, m, rstart, n):
+    """chunk_metrics (src/search.jl:1740-1755): device vs the FP64-profile oracle."""
+    amps, N, dt = pulsar_spectrum()
+    cs = _cs()
+    p = cs.SearchParams(nharms=nharms, m=m)
+    got = _engine(p, amps, N, dt).chunk_metrics(rstart, n)
+    want = o.chunk_metrics(amps, N, o.SearchParams(nharms=nharms, m=m), rstart, n, weights=np.float32)
+    assert np.all(np.abs(got - want) <= SNR_RTOL * np.maximum(np.abs(want), 1.0))
+
+
+def _oracle_run(amps, N, dt, op, band, thr, medcut, blocksize=2048):
+    T, lodr, r_lo, r_hi, total, Nprof = o.search_setup(N, dt, op, band[0], band[1], 100, blocksize)
+    return o.search_region(amps, N, T, op, r_lo, r_hi, total, Nprof, thr, medcut, keep_blocks=True)
+
+
+@pytest.mark.parametrize("maxdecim,band,blocksize", [(4, (1.0, 60.0), 2048), (6, (20.0, 900.0), 1000)])
+def test_search_vs_oracle(maxdecim, band, blocksize):
+    """The hot loop end to end (src/search.jl:1768-1894): nvalid exact, sigma
+    and S/N within tolerance, candidate (trial, k) sets equal outside the band."""
+    amps, N, dt = multi_spectrum()
+    cs = _cs()
+    nh = 32
+    thr = 7.0
+    dec = cs.decimation_set(nh, maxdecim)
+    eng = _engine(cs.SearchParams(nharms=nh, m=16, decimations=dec, threshold=thr), amps, N, dt)
+    dev = eng.search_raw(band[0], band[1], 100, blocksize, thr)
+    sig, nv = eng.block_values()
+    op = o.SearchParams(nharms=nh, m=16, decimations=dec, threshold=thr)
+    ref, blocks = _oracle_run(amps, N, dt, op, band, thr, thr - op.boxcar_medmargin, blocksize)
+    nlev = len(dec)
+    levk = [1] + [k for k in dec if k > 1]
+    ref_nv = np.zeros(len(blocks), np.int32)
+    ref_sig = np.zeros(len(blocks))
+    for b in blocks:
+        ref_nv[b.block * nlev + levk.index(b.k)] = b.nvalid
+        ref_sig[b.block * nlev + levk.index(b.k)] = b.sigma
+    assert np.array_equal(nv, ref_nv)
+    ok = ref_sig > 0
+    assert np.all(np.abs(sig[ok] - ref_sig[ok]) <= SIGMA_RTOL * ref_sig[ok])
+    assert np.all(sig[~ok] == 0)
+    dmap = {(int(c["trial"]), int(c["k"])): c for c in dev}
+    rmap = {(blk * blocksize + j, k): c for (blk, k, j, c) in ref}
+    band_hi = thr * (1 + 1e-3)
+    for key, c in rmap.items():
+        if key in dmap:
+            d = dmap[key]
+            assert abs(d["metric"] - c.metric) <= SNR_RTOL * c.metric
+            assert d["r"] == c.r and d["freq"] == c.freq and d["nharm"] == c.nharm
+        else:
+            assert c.metric < band_hi, (key, c.metric)
+    for key, d in dmap.items():
+        if key not in rmap:
+            assert thr < d["metric"] < band_hi, (key, float(d["metric"]))
+    # the device list comes back in the single-task reference order
+    order = [(int(c["trial"]) // blocksize, levk.index(int(c["k"])), int(c["trial"]) % blocksize) for c in dev]
+    assert order == sorted(order)
+    assert len(rmap) > 0
+
+
+def test_exact_all_metrics_vs_oracle():
+    """medcut = -Inf scores every trial exactly (metricstats/normalize mode)."""
+    amps, N, dt = multi_spectrum()
+    cs = _cs()
+    nh = 16
+    dec = cs.decimation_set(nh, 3)
+    eng = _engine(cs.SearchParams(nharms=nh, m=16, decimations=dec), amps, N, dt)
+    band = (2.0, 9.0)
+    eng.search_raw(band[0], band[1], 100, 2048, 1e9, exact_all=True)
+    tm = eng.trial_metrics()
+    sig, nv = eng.block_values()
+    op = o.SearchParams(nharms=nh, m=16, decimations=dec)
+    ref, blocks = _oracle_run(amps, N, dt, op, band, 1e9, -math.inf)
+    nlev = len(dec)
+    levk = [1] + [k for k in dec if k > 1]
+    tm = tm.reshape(-1, nlev, 2048)
+    for b in blocks:
+        got = tm[b.block, levk.index(b.k), :b.nvalid]
+        want = b.metrics[:b.nvalid]
+        assert np.all(np.abs(got - want) <= SNR_RTOL * np.maximum(np.abs(want), 1.0))
+
+
+def test_public_search_detects_the_pulsar():
+    """test/test_search.jl:378-385 through the public host API."""
+    amps, N, dt = pulsar_spectrum()
+    cs = _cs()
+    ft = cs.FFTFile.from_array(amps, N, dt)
+    p = cs.SearchParams(nharms=32, m=32)
+    cands = cs.search(ft, p, lofreq=9.5, hifreq=10.5, threshold=8.0)
+    assert cands
+    best = max(cands, key=lambda c: c.metric)
+    assert abs(best.freq - PSR_F) < 1e-2
+    raw = cs.search(ft, p, lofreq=9.5, hifreq=10.5, threshold=8.0, remove=False, harm_remove=False)
+    assert len(cands) < len(raw)
+
+
+def test_device_gate_does_not_change_candidates():
+    """test/test_search.jl:287-309 on the device."""
+    amps, N, dt = pulsar_spectrum()
+    cs = _cs()
+    ft = cs.FFTFile.from_array(amps, N, dt)
+    kw = dict(lofreq=9.5, hifreq=10.5, threshold=6.0, blocksize=512)
+    g = cs.search(ft, cs.SearchParams(nharms=60, m=32, decimations=cs.decimation_set(60, 4)), **kw)
+    e = cs.search(ft, cs.SearchParams(nharms=60, m=32, decimations=cs.decimation_set(60, 4),
+                                      boxcar_medmargin=math.inf), **kw)
+    assert len(g) == len(e) and g
+    assert all(a.freq == b.freq and a.nharm == b.nharm and a.metric == b.metric for a, b in zip(g, e))
+
+
+def test_pure_noise_has_no_candidates_above_8():
+    amps, N, dt = noise_spectrum()
+    cs = _cs()
+    ft = cs.FFTFile.from_array(amps, N, dt)
+    c = cs.search(ft, cs.SearchParams(nharms=32, decimations=cs.decimation_set(32, 4)), lofreq=1.0,
+                  hifreq=200.0, threshold=8.0)
+    assert c == []
+
+
+def test_error_behaviour():
+    cs = _cs()
+    with pytest.raises(ValueError):
+        cs.Engine(cs.SearchParams(m=15))
+    eng = cs.Engine(cs.SearchParams(nharms=8))
+    with pytest.raises(cs.CohSearchError) as ei:
+        eng.search_raw(1.0, 2.0)
+    assert ei.value.status == 2
+    amps, N, dt = noise_spectrum()
+    eng.set_spectrum(cs.FFTFile.from_array(amps, N, dt))
+    assert len(eng.search_raw(5.0, 4.0)) == 0          # empty band: no trials
+    with pytest.raises(ValueError):
+        eng.chunk_metrics(100.0, 0)

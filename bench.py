@@ -154,12 +154,14 @@ def run_ours(args, rank, world, local_rank):
     eng.set_spectrum_device(d_amps.data_ptr(), namps, N, dt, keep=d_amps)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
+    lof, hif = args.band if args.band else (LOF, HIF)
+
     def step_device():
-        return eng.search_raw(LOF, HIF, 100, BLOCK, THR)
+        return eng.search_raw(lof, hif, 100, BLOCK, THR)
 
     def step_e2e():
         eng.set_spectrum_host(h_amps.data_ptr(), namps, N, dt)
-        return eng.search_raw(LOF, HIF, 100, BLOCK, THR)
+        return eng.search_raw(lof, hif, 100, BLOCK, THR)
 
     for _ in range(args.warmup):
         cands = step_device()
@@ -196,13 +198,34 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
     ms_e2e, _, _, h2d, d2h, _ = timed(step_e2e, args.steps)
     torch.cuda.synchronize()
+    plain = None
+    if args.synth != "fp32" and not args.no_plain:
+        # the plain FP32 GPU form on the same data, for the mixed-vs-plain comparison
+        eng32 = Engine(SearchParams(nharms=NHARMS, m=16, decimations=decimation_set(NHARMS, MAXDECIM),
+                                    threshold=THR, synth="fp32"), device=local_rank)
+        eng32.set_stream(stream.cuda_stream)
+        eng32.set_spectrum_device(d_amps.data_ptr(), namps, N, dt, keep=d_amps)
+        c32 = eng32.search_raw(lof, hif, 100, BLOCK, THR)
+        ms32 = 0.0
+        for _ in range(max(1, args.steps)):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            c32 = eng32.search_raw(lof, hif, 100, BLOCK, THR)
+            e1.record(stream)
+            e1.synchronize()
+            ms32 += e0.elapsed_time(e1)
+        same = bool(np.array_equal(c32, cands)) if len(cands) == len(c32) else False
+        plain = {"ms": ms32 / max(1, args.steps), "same_candidates": same, "ncand": int(len(c32))}
+        del eng32
     if world > 1:
         import torch.distributed as dist
         t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, ms_e2e = float(t[0]), float(t[1])
     res = {"ms": ms, "ms_e2e": ms_e2e, "stage": stage, "launches": launches, "h2d": h2d, "d2h": d2h,
-           "trials": trials, "ncand": ncand, "clocks": clk.summary(), "stats": st}
+           "trials": trials, "ncand": ncand, "clocks": clk.summary(), "stats": st, "plain": plain}
     del eng
     return res
 
@@ -232,8 +255,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--synth", default="fp32", choices=["fp32", "bf16", "bf16x3"])
+    ap.add_argument("--synth", default="fp16", choices=["fp32", "bf16", "fp16"])
     ap.add_argument("--cpu-blocks", type=int, default=None)
+    ap.add_argument("--band", type=float, nargs=2, default=None,
+                    help="search only [LO, HI] Hz (a smaller case of the same kernels, for profiling)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison run")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -294,7 +321,13 @@ def main():
     sm_mhz = res["clocks"].get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
     fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12   # TFLOP/s, nominal
     x_bytes = trials * NHARMS * 8.0
-    if dom == "ms_synth" and args.synth == "fp32":
+    tc_flops = trials * 2.0 * 128 * 352     # dense product per trial: 2 * K(128) * N(352 columns)
+    if dom == "ms_synth" and args.synth != "fp32":
+        achieved = tc_flops / (stage[dom] / 1000.0) / 1e12
+        roof = {"kernel": "k_synth_tc", "bound": "tensor", "achieved": achieved,
+                "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"],
+                "traffic": None, "work": "2*128*352 flops per trial (dense 16-bit product, all levels)"}
+    elif dom == "ms_synth" and args.synth == "fp32":
         fl = trials * (synth_flops_per_trial(frac_valid))
         achieved = fl / (stage[dom] / 1000.0) / 1e12
         roof = {"kernel": "k_synth_fp32", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
@@ -316,6 +349,8 @@ def main():
     roof["stage_ms"] = stage
     cpu = None
     try:
+        if args.no_cpu:
+            raise RuntimeError("skipped (--no-cpu)")
         r = cpu_sample_run(os.cpu_count() or 1, args.cpu_blocks or max(8, 2 * (os.cpu_count() or 1)))
         cpu = {"value": r["trials"] / r["seconds"], "unit": "trials/s", "cores": r["threads"],
                "kind": "port", "sample": f"{r['blocks']} blocks x {BLOCK} trials mid-band of the workload"}
@@ -325,6 +360,16 @@ def main():
     cfg["trials_per_step"] = trials
     cfg["profiles_per_step"] = st["profiles"]
     cfg["candidates_per_step"] = res["ncand"]
+    cfg["rescued_per_step"] = st["rescued"]
+    if args.band:
+        cfg["band_hz"] = list(args.band)
+    if res["plain"]:
+        p = res["plain"]
+        cfg["plain_fp32_trials_per_s"] = world * trials / (p["ms"] / 1000.0)
+        cfg["plain_fp32_ms_per_step"] = p["ms"]
+        cfg["mixed_vs_plain_speedup"] = p["ms"] / (res["ms"] / K)
+        cfg["recall_vs_plain"] = 1.0 if p["same_candidates"] else None
+        cfg["candidates_identical_to_plain"] = p["same_candidates"]
     out = {"metric": METRIC, "value": value, "unit": "trials/s", "n_gpus": world, "steps": K,
            "warmup": args.warmup, "ms_per_step": res["ms"] / K, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.synth == "fp32" else args.synth,

@@ -22,7 +22,7 @@ CS_ERR_TIMEOUT = 6
 CS_ERR_UNSUPPORTED = 7
 CS_MAX_DECIM = 16
 
-CS_SYNTH = {"fp32": 0, "bf16": 1, "bf16x3": 2}
+CS_SYNTH = {"fp32": 0, "bf16": 1, "fp16": 2}
 
 STATUS_NAMES = {
     CS_OK: "CS_OK", CS_ERR_INVALID_ARGUMENT: "CS_ERR_INVALID_ARGUMENT",
@@ -92,6 +92,8 @@ PROTOTYPES = {
     "cs_interp_chunk": (_i32, [_P, _f64, _i64, _i64, _P]),
     "cs_search_block_values": (_i32, [_P, _P, _P, _i64, ctypes.POINTER(_i64)]),
     "cs_search_trial_metrics": (_i32, [_P, _P, _i64, ctypes.POINTER(_i64)]),
+    "cs_set_diagnostics": (_i32, [_P, _i32]),
+    "cs_search_gate_values": (_i32, [_P, _P, _i64, ctypes.POINTER(_i64)]),
     "cs_version": (ctypes.c_char_p, []),
 }
 

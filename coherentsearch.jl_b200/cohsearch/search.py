@@ -28,7 +28,7 @@ class SearchParams:
     """Tunable search parameters, defaults as src/search.jl:131-144.
 
     ``synth`` selects the device profile-synthesis arithmetic: ``"fp32"`` (the
-    plain FP32 GPU form), ``"bf16"`` or ``"bf16x3"`` (tensor-core forms).
+    plain FP32 GPU form), ``"bf16"`` or ``"fp16"`` (tensor-core forms).
     Equality is identity, as ``SearchCache`` keys on the object.
     """
     nharms: int = 32
@@ -271,6 +271,16 @@ class Engine:
         _lib.check(self.lib.cs_search_block_values(self._h, sig.ctypes.data, nv.ctypes.data, n.value,
                                                    ctypes.byref(n)), self._h)
         return sig, nv
+
+    def set_diagnostics(self, level: int):
+        _lib.check(self.lib.cs_set_diagnostics(self._h, int(level)), self._h, "cs_set_diagnostics")
+
+    def gate_values(self):
+        n = ctypes.c_int64()
+        self.lib.cs_search_gate_values(self._h, None, 0, ctypes.byref(n))
+        out = np.zeros(n.value, np.float32)
+        _lib.check(self.lib.cs_search_gate_values(self._h, out.ctypes.data, n.value, ctypes.byref(n)), self._h)
+        return out
 
     def trial_metrics(self):
         n = ctypes.c_int64()

@@ -160,6 +160,8 @@ void build_plans(const cs_params& p, double r_lo, HostPlans& out) {
         d.P = (int32_t)P;
         d.q = (int32_t)q;
         d.pnum = (int32_t)pnum;
+        d.s = (int32_t)s;
+        d.base_adv = (int32_t)(step / q);
         d.w_off = (int64_t)out.w.size();
         d.a_off = (int64_t)out.a.size();
         out.w.resize(out.w.size() + (size_t)m * P);
@@ -209,13 +211,18 @@ struct cs_handle {
     bool has_spec = false;
     int64_t spec_h2d_bytes = 0;   // bytes of the last host spectrum copy, charged to the next search
     // device buffers
-    DBuf d_levels, d_tw, d_harms, d_wtab, d_atab, d_ctab, d_nvalid, d_X, d_Q0, d_sub, d_sigma,
+    TcPlanHost tc;                      // tensor-core synthesis plan (synth != FP32)
+    DBuf d_tcB;
+    DBuf d_A, d_samp;
+    DBuf d_levels, d_tw, d_harms, d_wtab, d_atab, d_ctab, d_nvalid, d_X, d_Q0, d_sigma,
         d_tmetric, d_items, d_counts, d_cands;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     cs_stats stats{};
     std::vector<float> last_sigma;
     std::vector<int32_t> last_nvalid;
     std::vector<float> last_tmetric;
+    std::vector<float> last_gate;
+    int diag = 0;
     int last_nlev = 0;
     int last_Nprof = 0;
 };
@@ -255,7 +262,7 @@ cs_status validate(const cs_params* p) {
         if (p->decimations[i] < 1 || p->nharms / p->decimations[i] < 1) return CS_ERR_INVALID_ARGUMENT;
     if (p->precision != 0 && p->precision != 1) return CS_ERR_INVALID_ARGUMENT;
     if (!(p->boxcar_fsp > 0) || !(p->boxcar_maxfrac > 0)) return CS_ERR_INVALID_ARGUMENT;
-    if (p->synth != CS_SYNTH_FP32 && p->synth != CS_SYNTH_BF16 && p->synth != CS_SYNTH_BF16X3)
+    if (p->synth != CS_SYNTH_FP32 && p->synth != CS_SYNTH_BF16 && p->synth != CS_SYNTH_FP16)
         return CS_ERR_INVALID_ARGUMENT;
     return CS_OK;
 }
@@ -313,6 +320,14 @@ cs_status build_levels(cs_handle* H) {
     }
     CS_CUDA(upload(H->d_levels, H->dlev, H->stream), "upload levels");
     CS_CUDA(upload(H->d_tw, tw, H->stream), "upload twiddles");
+    if (p.synth != CS_SYNTH_FP32) {
+        const int rc = prepare_tc(H->dlev.data(), (int)H->dlev.size(), p.nharms, p.synth == CS_SYNTH_FP16,
+                                  &H->tc);
+        if (rc != 0)
+            return fail(H, CS_ERR_UNSUPPORTED,
+                        "tensor-core synthesis needs nharms <= 64, boxcar widths <= 32 and <= 512 TMEM columns");
+        CS_CUDA(upload(H->d_tcB, H->tc.B, H->stream), "upload tensor twiddles");
+    }
     return CS_OK;
 }
 
@@ -364,28 +379,47 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
 
     const int Nprof = R.Nprof;
     const int win_max = (int)std::ceil((double)(Nprof - 1 + 64) * p.hidr) + p.m + 4;
-    if ((size_t)win_max * sizeof(float2) > 200 * 1024)
-        return fail(H, CS_ERR_UNSUPPORTED, "blocksize*hidr too large for the shared-memory bin window");
+    if (interp_smem(win_max, Nprof) > 200 * 1024)
+        return fail(H, CS_ERR_UNSUPPORTED, "blocksize too large for the shared-memory interpolation row");
     int maxbins = 0, maxwmax = 0;
     for (int l = 0; l < R.nlev; ++l) {
         maxbins = std::max(maxbins, H->dlev[l].nbins);
         maxwmax = std::max(maxwmax, H->dlev[l].wmax);
     }
     const size_t smem_synth = synth_fp32_smem(p.nharms, maxbins, maxwmax);
-    if (smem_synth > 227 * 1024) return fail(H, CS_ERR_UNSUPPORTED, "profile tile exceeds shared memory");
+    int max_hk = 0, max_np = 0;
+    for (int l = 0; l < R.nlev; ++l) {
+        max_hk = std::max(max_hk, H->dlev[l].Hk);
+        max_np = std::max(max_np, H->dlev[l].np);
+    }
+    if (sigma_smem(max_hk, max_np) + 16 * 1024 > 227 * 1024)
+        return fail(H, CS_ERR_UNSUPPORTED, "sigma working set exceeds shared memory");
+    const bool tensor = p.synth != CS_SYNTH_FP32 && R.nlev == (int)H->dlev.size();
+    if (!tensor && smem_synth > 227 * 1024) return fail(H, CS_ERR_UNSUPPORTED, "profile tile exceeds shared memory");
 
     const int nlev = R.nlev;
-    const size_t per_blk = (size_t)p.nharms * Nprof * sizeof(float2) +
+    const int tiles_per_blk = (Nprof + 127) / 128;
+    const bool want_x = !tensor || R.interp_only;
+    const size_t per_blk = (want_x ? (size_t)p.nharms * Nprof * sizeof(float2) : 0) +
+                           (tensor ? (size_t)tiles_per_blk * kATileBytes : 0) +
+                           (size_t)nlev * kSampStride * sizeof(float2) +
                            (size_t)nlev * Nprof * sizeof(float) * (R.exact_all ? 2 : 1) +
-                           (size_t)nlev * kSigmaCap * sizeof(float) +
                            (size_t)nlev * Nprof * (sizeof(DevItem) + sizeof(DevCand)) + 64;
     const size_t budget = (size_t)3 << 30;
     const int64_t WB = std::max<int64_t>(1, std::min<int64_t>(R.nblocks, (int64_t)(budget / per_blk)));
 
-    CS_CUDA(H->d_X.ensure((size_t)WB * p.nharms * Nprof * sizeof(float2)), "alloc X");
+    if (want_x) CS_CUDA(H->d_X.ensure((size_t)WB * p.nharms * Nprof * sizeof(float2)), "alloc X");
+    if (tensor && !R.interp_only) {
+        const size_t abytes = (size_t)WB * tiles_per_blk * kATileBytes;
+        if (abytes > H->d_A.bytes) {
+            // zero once: the K columns past 2*nharms are never written
+            CS_CUDA(H->d_A.ensure(abytes), "alloc A tiles");
+            CS_CUDA(cudaMemsetAsync(H->d_A.p, 0, H->d_A.bytes, H->stream), "zero A tiles");
+        }
+    }
     if (!R.interp_only) {
+        CS_CUDA(H->d_samp.ensure((size_t)WB * nlev * kSampStride * sizeof(float2)), "alloc samples");
         CS_CUDA(H->d_Q0.ensure((size_t)WB * nlev * Nprof * sizeof(float)), "alloc Q0");
-        CS_CUDA(H->d_sub.ensure((size_t)WB * nlev * kSigmaCap * sizeof(float)), "alloc sub");
         CS_CUDA(H->d_sigma.ensure((size_t)WB * nlev * sizeof(float)), "alloc sigma");
         CS_CUDA(H->d_nvalid.ensure((size_t)WB * nlev * sizeof(int32_t)), "alloc nvalid");
         CS_CUDA(H->d_items.ensure((size_t)WB * nlev * Nprof * sizeof(DevItem)), "alloc items");
@@ -406,6 +440,8 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         H->last_nvalid.assign((size_t)R.nblocks * nlev, 0);
         if (R.exact_all) H->last_tmetric.assign((size_t)R.nblocks * nlev * Nprof, 0.0f);
         else H->last_tmetric.clear();
+        if (H->diag >= 2 && !R.exact_all) H->last_gate.assign((size_t)R.nblocks * nlev * Nprof, 0.0f);
+        else H->last_gate.clear();
         H->last_nlev = nlev;
         H->last_Nprof = Nprof;
     }
@@ -435,9 +471,12 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         a.levels = H->d_levels.as<DevLevel>();
         a.tw = H->d_tw.as<float>();
         a.nvalid = H->d_nvalid.as<int32_t>();
-        a.X = H->d_X.as<float2>();
+        a.X = want_x ? H->d_X.as<float2>() : nullptr;
+        a.Atile = (tensor && !R.interp_only) ? H->d_A.as<uint8_t>() : nullptr;
+        a.tiles_per_blk = tiles_per_blk;
+        a.fp16 = p.synth == CS_SYNTH_FP16 ? 1 : 0;
+        a.samp = R.interp_only ? nullptr : H->d_samp.as<float2>();
         a.Q0 = H->d_Q0.as<float>();
-        a.sub = H->d_sub.as<float>();
         a.sigma = H->d_sigma.as<float>();
         a.tmetric = R.exact_all ? H->d_tmetric.as<float>() : nullptr;
         a.items = H->d_items.as<DevItem>();
@@ -448,6 +487,17 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         a.cap_cands = a.cap_items;
         a.threshold = R.threshold;
         a.medcut = R.medcut;
+        a.medcut_gate = R.medcut;
+        a.verify_gate = 0;
+        if (tensor && !R.exact_all) {
+            // A 16-bit gate flags with slack below medcut; the rescan re-forms
+            // the FP32 gate and applies medcut itself, so the rescanned set --
+            // hence every candidate -- is the plain form's.
+            const float rel = p.synth == CS_SYNTH_BF16 ? 0.08f : 0.02f;
+            const float ab = p.synth == CS_SYNTH_BF16 ? 0.10f : 0.05f;
+            a.medcut_gate = R.medcut - (rel * std::fabs(R.medcut) + ab);
+            a.verify_gate = 1;
+        }
         a.exact_all = R.exact_all ? 1 : 0;
         int* d_err = H->d_counts.as<int32_t>() + 2;
 
@@ -464,17 +514,22 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             }
         }
         CS_CUDA(cudaMemsetAsync(H->d_counts.p, 0, 4 * sizeof(int32_t), H->stream), "reset counters");
+        if (!R.interp_only) {
+            CS_CUDA(upload(H->d_nvalid, nvalid, H->stream), "upload nvalid");
+            S.h2d_bytes += (int64_t)(nvalid.size() * sizeof(int32_t));
+            a.nvalid = H->d_nvalid.as<int32_t>();
+        }
         CS_CUDA(cudaEventRecord(H->ev[0], H->stream), "event");
         CS_CUDA(launch_interp(a, H->stream, win_max, d_err), "interp launch");
         CS_CUDA(cudaEventRecord(H->ev[1], H->stream), "event");
         S.launches += 1;
         if (!R.interp_only) {
-            CS_CUDA(upload(H->d_nvalid, nvalid, H->stream), "upload nvalid");
-            S.h2d_bytes += (int64_t)(nvalid.size() * sizeof(int32_t));
-            a.nvalid = H->d_nvalid.as<int32_t>();
-            CS_CUDA(launch_synth_fp32(a, H->stream, (int)smem_synth), "synth launch");
+            if (tensor)
+                CS_CUDA(launch_synth_tc(a, H->tc, H->d_tcB.p, d_err, H->stream, H->num_sms), "synth launch");
+            else
+                CS_CUDA(launch_synth_fp32(a, H->stream, (int)smem_synth), "synth launch");
             CS_CUDA(cudaEventRecord(H->ev[2], H->stream), "event");
-            CS_CUDA(launch_sigma(a, H->stream), "sigma launch");
+            CS_CUDA(launch_sigma(a, H->stream, max_hk, max_np), "sigma launch");
             CS_CUDA(cudaEventRecord(H->ev[3], H->stream), "event");
             if (!R.exact_all) {
                 CS_CUDA(launch_flag(a, H->stream), "flag launch");
@@ -489,7 +544,8 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
                 "read counters");
         CS_CUDA(cudaStreamSynchronize(H->stream), "wave");
         S.d2h_bytes += 4 * sizeof(int32_t);
-        if (counts[2] != 0) return fail(H, CS_ERR_CUDA, "interpolation window exceeded its bound");
+        if (counts[2] == 1) return fail(H, CS_ERR_CUDA, "interpolation window exceeded its bound");
+        if (counts[2] == 2) return fail(H, CS_ERR_TIMEOUT, "tensor-core completion wait ran out");
         float ms = 0.0f;
         CS_CUDA(cudaEventElapsedTime(&ms, H->ev[0], H->ev[1]), "timing");
         S.ms_interp += ms;
@@ -536,6 +592,20 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
                 CS_CUDA(cudaMemcpy(H->last_tmetric.data() + (size_t)c0 * nlev * Nprof, H->d_tmetric.p,
                                    (size_t)nb * nlev * Nprof * sizeof(float), cudaMemcpyDeviceToHost),
                         "read metrics");
+            if (!H->last_gate.empty()) {
+                float* g = H->last_gate.data() + (size_t)c0 * nlev * Nprof;
+                CS_CUDA(cudaMemcpy(g, H->d_Q0.p, (size_t)nb * nlev * Nprof * sizeof(float),
+                                   cudaMemcpyDeviceToHost),
+                        "read gate");
+                for (int b = 0; b < nb; ++b)
+                    for (int l = 0; l < nlev; ++l) {
+                        const float sg = H->last_sigma[(size_t)(c0 + b) * nlev + l];
+                        const float inv = sg > 0.0f ? 1.0f / sg : 0.0f;
+                        const int nv = nvalid[(size_t)b * nlev + l];
+                        float* row = g + ((size_t)b * nlev + l) * Nprof;
+                        for (int j = 0; j < Nprof; ++j) row[j] = j < nv ? row[j] * inv : 0.0f;
+                    }
+            }
         }
     }
     return CS_OK;
@@ -554,7 +624,6 @@ cs_status cs_create(cs_handle** out, const cs_params* params, int32_t device) {
     *out = nullptr;
     cs_status st = validate(params);
     if (st != CS_OK) return st;
-    if (params->synth != CS_SYNTH_FP32) return CS_ERR_UNSUPPORTED;
     cs_handle* H = new (std::nothrow) cs_handle();
     if (!H) return CS_ERR_OUT_OF_MEMORY;
     H->p = *params;
@@ -593,8 +662,8 @@ cs_status cs_destroy(cs_handle* H) {
     cudaSetDevice(H->device);
     if (H->stream) cudaStreamSynchronize(H->stream);
     if (H->own_stream) cudaStreamSynchronize(H->own_stream);
-    DBuf* bufs[] = {&H->amps_owned, &H->d_levels, &H->d_tw, &H->d_harms, &H->d_wtab, &H->d_atab,
-                    &H->d_ctab, &H->d_nvalid, &H->d_X, &H->d_Q0, &H->d_sub, &H->d_sigma,
+    DBuf* bufs[] = {&H->d_A, &H->d_samp, &H->d_tcB, &H->amps_owned, &H->d_levels, &H->d_tw, &H->d_harms, &H->d_wtab, &H->d_atab,
+                    &H->d_ctab, &H->d_nvalid, &H->d_X, &H->d_Q0, &H->d_sigma,
                     &H->d_tmetric, &H->d_items, &H->d_counts, &H->d_cands};
     for (DBuf* b : bufs) b->release();
     for (auto& ev : H->ev)
@@ -672,7 +741,7 @@ cs_status cs_search(cs_handle* H, double lofreq, double hifreq, int64_t lobin, i
     R.exact_all = exact_all != 0;
     R.threshold = (float)threshold;
     R.medcut = exact_all ? -INFINITY : (float)(threshold - p.boxcar_medmargin);
-    R.keep_diag = true;
+    R.keep_diag = H->diag >= 1;
     std::vector<DevCand> raw;
     cs_status st = run_blocks(H, R, &raw, nullptr);
     if (st != CS_OK) return st;
@@ -760,6 +829,21 @@ cs_status cs_search_block_values(const cs_handle* H, float* sigma, int32_t* nval
     if (cap < n) return CS_ERR_CAPACITY;
     if (sigma) std::copy(H->last_sigma.begin(), H->last_sigma.end(), sigma);
     if (nvalid) std::copy(H->last_nvalid.begin(), H->last_nvalid.end(), nvalid);
+    return CS_OK;
+}
+
+cs_status cs_set_diagnostics(cs_handle* H, int32_t level) {
+    if (!H || level < 0 || level > 2) return CS_ERR_INVALID_ARGUMENT;
+    H->diag = level;
+    return CS_OK;
+}
+
+cs_status cs_search_gate_values(const cs_handle* H, float* out, int64_t cap, int64_t* n_out) {
+    if (!H || !n_out) return CS_ERR_INVALID_ARGUMENT;
+    const int64_t n = (int64_t)H->last_gate.size();
+    *n_out = n;
+    if (cap < n) return CS_ERR_CAPACITY;
+    if (out) std::copy(H->last_gate.begin(), H->last_gate.end(), out);
     return CS_OK;
 }
 

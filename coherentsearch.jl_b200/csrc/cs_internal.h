@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace cs {
 
 constexpr int kMaxLevels = 16;     // decimation factors per search
@@ -12,6 +14,8 @@ constexpr int kMaxWidths = 64;     // boxcar widths per level
 constexpr int kMaxBins = 256;      // profile bins (nharms <= 128)
 constexpr int kSigmaCap = 8192;    // _BOXCAR_SIGMA_SAMPLES, src/search.jl:462
 constexpr int kTileTrials = 64;    // trials per CTA in the FP32 synthesis kernel
+constexpr int kATileBytes = 128 * 128 * 2;  // one 16-bit A tile: 128 trials x 128 K
+constexpr int kSampStride = kSigmaCap / 2;  // float2 per (block, level) in `samp`
 
 // One harmonic's rational trial-grid recipe (DirectPlan, src/directinterp.jl:179-204).
 // Global trial t of the search evaluates harmonic h at Fourier frequency
@@ -22,6 +26,8 @@ struct DevHarm {
     int32_t P;          // phase-cycle length q / gcd(h*pnum, q); 0 => per-trial FP64 path
     int32_t q;
     int32_t pnum;
+    int32_t s;          // (h*pnum) mod q
+    int32_t base_adv;   // (h*pnum) div q
     int64_t rfloor0;    // floor(h * r_lo)
     double dr0;         // h*r_lo - rfloor0
     double hr_lo;       // rfloor0 + dr0 (per-trial path)
@@ -79,9 +85,12 @@ struct WaveArgs {
     const DevLevel* levels;
     const float* tw;
     const int32_t* nvalid;  // [nblk][nlev]
-    float2* X;              // [nblk][nharms][Nprof]
+    float2* X;              // [nblk][nharms][Nprof] FP32 amplitudes (plain synthesis) or nullptr
+    uint8_t* Atile;         // [nblk][tiles_per_blk] 16-bit A tiles (tensor synthesis) or nullptr
+    int32_t tiles_per_blk;
+    int32_t fp16;           // A-tile format: 1 = FP16, 0 = BF16
+    float2* samp;           // [nblk][nlev][kSampStride]: pooled columns' amplitudes, [jh-1][slot]
     float* Q0;              // [nblk][nlev][Nprof] zero-baseline gate (unscaled by 1/sigma)
-    float* sub;             // [nblk][nlev][kSigmaCap] |profile| samples for sigma
     float* sigma;           // [nblk][nlev]
     float* tmetric;         // [nblk][nlev][Nprof] exact metrics (exact_all mode) or nullptr
     DevItem* items;         // rescue list
@@ -91,14 +100,64 @@ struct WaveArgs {
     int32_t* n_cands;
     int32_t cap_cands;
     float threshold;
-    float medcut;
+    float medcut;         // threshold - boxcar_medmargin (the reference's gate)
+    float medcut_gate;    // the flag kernel's cut: medcut, less a slack for 16-bit gates
+    int32_t verify_gate;  // rescan recomputes the FP32 gate and applies medcut itself
     int32_t exact_all;
 };
+
+// Tensor-core synthesis (cs_synth_tc.cu): per-level TMEM column layout.
+struct TcLevel {
+    int32_t nbins;
+    int32_t ncol;      // nbins + wmax columns with data (bins, then the wrapped first wmax bins)
+    int32_t pw;        // columns streamed: ncol padded with zero columns to a multiple of the ring
+    int32_t col;       // first TMEM column of the level
+    int32_t nunits;    // epilogue units the level's starts are split into
+    uint32_t wmask;    // bit w-1 set for each boxcar width w
+    float rsq[32];     // 1/sqrt(w) at index w-1
+};
+
+// One epilogue work unit: the boxcar starts [p0, p0+nstart) of one level,
+// scanned from TMEM column col (= level col + p0) over pw columns.
+struct TcUnit {
+    int16_t lev;
+    int16_t wg;        // epilogue warpgroup (0..3)
+    int16_t nstart;
+    int16_t pw;
+    int16_t col;
+    int16_t pad;
+};
+
+constexpr int kMaxUnits = 32;
+
+struct TcArgs {
+    TcLevel lev[kMaxLevels];
+    TcUnit unit[kMaxUnits];
+    int32_t nunit;
+    int32_t nlev;
+    int32_t hm;            // prefix-sum ring size: 8 or 32 (>= widest boxcar)
+    int32_t ncols_total;   // columns of the product (multiple of 16)
+    int32_t n1;            // N of the first MMA (<= 256); the rest is the second
+    int32_t fp16;          // operand format: 1 = FP16, 0 = BF16
+};
+
+struct TcPlanHost {
+    TcArgs args;
+    std::vector<uint16_t> B;   // ncols_total x 128 twiddles, core-matrix layout
+    size_t smem = 0;
+};
+
+// Returns 0, or < 0 when the configuration does not fit the tensor path.
+int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, TcPlanHost* out);
+cudaError_t launch_synth_tc(const WaveArgs& a, const TcPlanHost& tp, const void* dB, int* err,
+                            cudaStream_t st, int num_sms);
 
 // Kernel launchers (cs_kernels.cu).  Each returns the launch error.
 cudaError_t launch_interp(const WaveArgs& a, cudaStream_t st, int win_max, int* err);
 cudaError_t launch_synth_fp32(const WaveArgs& a, cudaStream_t st, int smem_bytes);
-cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st);
+size_t sigma_smem(int max_hk, int max_np);
+size_t interp_smem(int win_max, int Nprof);
+cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np);
 cudaError_t launch_flag(const WaveArgs& a, cudaStream_t st);
 cudaError_t launch_rescue(const WaveArgs& a, cudaStream_t st, int num_sms);
 size_t synth_fp32_smem(int nharms, int maxbins, int maxwmax);

@@ -13,6 +13,8 @@
 //                  and candidate emission (src/search.jl:1827-1838, :1695-1708).
 #include "cs_internal.h"
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <math.h>
 
 namespace cs {
@@ -28,170 +30,308 @@ namespace cs {
 // chain over the m taps, and the final complex product is unfused, which is the
 // arithmetic of the reference's Float32-weight group kernel
 // (src/directinterp.jl:584-605, whose zero-padded extra taps add exact zeros).
-template <int M>
-__device__ __forceinline__ float2 tap_sum(const float* __restrict__ w, int P, int p,
-                                          const float2* __restrict__ x, int m) {
-    float sre = 0.0f, sim = 0.0f;
-    if (M > 0) {
-#pragma unroll
-        for (int i = 0; i < M; ++i) {
-            const float wi = __ldg(w + i * P + p);
-            const float2 xi = x[i];
-            sre = fmaf(wi, xi.x, sre);
-            sim = fmaf(wi, xi.y, sim);
-        }
-    } else {
-        for (int i = 0; i < m; ++i) {
-            const float wi = __ldg(w + i * P + p);
-            const float2 xi = x[i];
-            sre = fmaf(wi, xi.x, sre);
-            sim = fmaf(wi, xi.y, sim);
-        }
-    }
-    return make_float2(sre, sim);
-}
-
 __device__ __forceinline__ float2 cmul_unfused(float2 a, float2 s) {
     // Complex{Float32} product a*s without contraction: (a.x*s.x - a.y*s.y, a.x*s.y + a.y*s.x).
     return make_float2(__fsub_rn(__fmul_rn(a.x, s.x), __fmul_rn(a.y, s.y)),
                        __fadd_rn(__fmul_rn(a.x, s.y), __fmul_rn(a.y, s.x)));
 }
 
-template <int M>
-__global__ void __launch_bounds__(256) k_interp(WaveArgs a, int win_max, int* err) {
-    extern __shared__ float2 win[];
-    __shared__ int s_ok, s_nw, s_p0, s_res0;
-    __shared__ long long s_lo, s_base;  // s_base = rfloor0 + qint0 - lo + 1 - m2
+// ---------------------------------------------------------------------------
+// Exact amplitudes on demand (block sigma samples and rescans)
+// ---------------------------------------------------------------------------
 
-    const int blk = blockIdx.x;
-    const int hidx = blockIdx.y;
-    const DevHarm hp = a.harms[hidx];
+// The range guard of k_interp for harmonic hp over the block's true trial
+// range [t0, t0+n) (src/directinterp.jl:490-496, :633-637).
+__device__ bool harm_guard(const WaveArgs& a, const DevHarm& hp, int64_t t0, int n) {
+    const int m2 = a.m / 2;
+    if (hp.P == 0) {
+        const double rfirst = __dadd_rn(hp.hr_lo, __dmul_rn((double)t0, hp.dh));
+        const double rlast = __dadd_rn(hp.hr_lo, __dmul_rn((double)(t0 + n - 1), hp.dh));
+        const int64_t lo = (int64_t)floor(__dadd_rn(rfirst, 1e-15)) + 2 - m2;
+        const int64_t hi = (int64_t)floor(__dadd_rn(rlast, 1e-15)) + 1 + m2;
+        return lo >= 1 && hi <= a.namps && (int64_t)floor(rlast) < a.Nhalf;
+    }
+    const int64_t hpn = (int64_t)hp.h * hp.pnum;
+    const int64_t qint0 = (t0 * hpn) / hp.q;
+    const int64_t tl = t0 + n - 1;
+    const int64_t qintl = (tl * hpn) / hp.q;
+    const uint8_t* ct = a.ctab + hp.a_off;
+    const int64_t fl0 = hp.rfloor0 + qint0 + ct[(int)(t0 % hp.P)];
+    const int64_t fll = hp.rfloor0 + qintl + ct[(int)(tl % hp.P)];
+    return (fl0 + 2 - m2 >= 1) && (fll + 1 + m2 <= a.namps) && (hp.rfloor0 + qintl < a.Nhalf);
+}
+
+// Amplitude of harmonic hp at global trial t (guard assumed passed), with the
+// arithmetic of k_interp: bit-identical to the value k_interp writes.
+// t_div_q / t_mod_q are t / q and t % q of the rational grid.
+__device__ float2 exact_amp(const WaveArgs& a, const DevHarm& hp, int64_t t, int64_t t_div_q, int t_mod_q) {
+    const int m = a.m, m2 = m / 2;
+    if (hp.P == 0) {
+        const double r = __dadd_rn(hp.hr_lo, __dmul_rn((double)t, hp.dh));
+        const int64_t rint = (int64_t)floor(__dadd_rn(r, 1e-15)) + 1;
+        const double dr = fmod(r, 1.0);
+        const int64_t base = rint - m2;
+        if (dr == 0.0) return a.amps[base + m2 - 1];
+        double sre = 0.0, sim = 0.0;
+        for (int i = 0; i < m; ++i) {
+            const double w = 1.0 / (dr - (double)(i + 1 - m2));
+            const float2 x = a.amps[base + i];
+            sre = fma(w, (double)x.x, sre);
+            sim = fma(w, (double)x.y, sim);
+        }
+        const double sn = sinpi(dr), c = cospi(dr);
+        const double ar = __ddiv_rn(__dmul_rn(sn, c), M_PI);
+        const double ai = -__ddiv_rn(__dmul_rn(sn, sn), M_PI);
+        return make_float2((float)__dsub_rn(__dmul_rn(ar, sre), __dmul_rn(ai, sim)),
+                           (float)__dadd_rn(__dmul_rn(ar, sim), __dmul_rn(ai, sre)));
+    }
+    // t*h*pnum = t*base_adv*q + t*s, and t*s = t_div_q*q*s + t_mod_q*s.
+    const uint32_t ts = (uint32_t)t_mod_q * (uint32_t)hp.s;
+    const int64_t qint = t * (int64_t)hp.base_adv + t_div_q * (int64_t)hp.s + (int64_t)(ts / (uint32_t)hp.q);
+    const int p = t_mod_q % hp.P;   // P divides q
+    const int64_t base = hp.rfloor0 + qint + a.ctab[hp.a_off + p] + 1 - m2;
+    const float* w = a.wtab + hp.w_off;
+    const float2* x = a.amps + base;
+    float sre = 0.0f, sim = 0.0f;
+    for (int i = 0; i < m; ++i) {
+        const float wi = __ldg(w + i * hp.P + p);
+        const float2 xi = __ldg(x + i);
+        sre = fmaf(wi, xi.x, sre);
+        sim = fmaf(wi, xi.y, sim);
+    }
+    return cmul_unfused(__ldg(a.atab + hp.a_off + p), make_float2(sre, sim));
+}
+
+__device__ __forceinline__ void tq_split(const DevHarm& hp, int64_t t, int64_t* t_div_q, int* t_mod_q) {
+    if (hp.P == 0) { *t_div_q = 0; *t_mod_q = 0; return; }
+    *t_div_q = t / hp.q;
+    *t_mod_q = (int)(t - *t_div_q * hp.q);
+}
+
+constexpr int kHG = 4;   // harmonics per interpolation CTA: one 16-byte K chunk of an A tile
+
+// Emit a block's staged rows for harmonics hidx0 .. hidx0+ng-1: FP32 rows
+// (plain synthesis) or one 16-byte K chunk per trial of the block's A tiles
+// (tensor synthesis), and the exact FP32 amplitudes of the columns each
+// level's block sigma pools.
+__device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, int Nst, int blk, int hidx0,
+                                          int ng, int n) {
+    if (a.X) {
+        for (int g = 0; g < ng; ++g) {
+            float2* xrow = a.X + ((int64_t)blk * a.nharms + hidx0 + g) * a.Nprof;
+            for (int j = threadIdx.x; j < n; j += blockDim.x) xrow[j] = xo[g * Nst + j];
+        }
+    }
+    if (a.Atile) {
+        // A tile (block, j/128), row r = j%128, K chunk hidx0/4 holds (Re, Im) of
+        // the 4 harmonics: SWIZZLE_NONE K-major core-matrix layout.
+        uint8_t* base = a.Atile + (int64_t)blk * a.tiles_per_blk * kATileBytes + (hidx0 >> 2) * 128;
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            uint32_t v[kHG];
+#pragma unroll
+            for (int g = 0; g < kHG; ++g) {
+                const float2 x = g < ng ? xo[g * Nst + j] : make_float2(0.0f, 0.0f);
+                if (a.fp16) {
+                    __half2 hv = __floats2half2_rn(x.x, x.y);
+                    v[g] = *reinterpret_cast<uint32_t*>(&hv);
+                } else {
+                    __nv_bfloat162 bv = __floats2bfloat162_rn(x.x, x.y);
+                    v[g] = *reinterpret_cast<uint32_t*>(&bv);
+                }
+            }
+            const int r = j & 127;
+            *reinterpret_cast<uint4*>(base + (int64_t)(j >> 7) * kATileBytes + (r >> 3) * 2048 + (r & 7) * 16) =
+                make_uint4(v[0], v[1], v[2], v[3]);
+        }
+    }
+    if (!a.samp) return;
+    for (int g = 0; g < ng; ++g) {
+        const int h = hidx0 + g + 1;
+        for (int l = 0; l < a.nlev; ++l) {
+            const DevLevel& L = a.levels[l];
+            if (h % L.k != 0 || h / L.k > L.Hk) continue;
+            const int jh = h / L.k;
+            const int nv = a.nvalid[blk * a.nlev + l];
+            if (nv <= 0) continue;
+            const bool all = (int64_t)L.nbins * nv <= kSigmaCap;
+            const int ncs = all ? nv : min(nv, max(1, kSigmaCap / L.nbins));
+            float2* dst = a.samp + ((int64_t)blk * a.nlev + l) * kSampStride + (int64_t)(jh - 1) * ncs;
+            // sl*nv < 8192*65536 fits 32 bits
+            for (int sl = threadIdx.x; sl < ncs; sl += blockDim.x)
+                dst[sl] = xo[g * Nst + (all ? sl : (int)(((uint32_t)sl * (uint32_t)nv) / (uint32_t)ncs))];
+        }
+    }
+}
+
+// Outputs of one phase class: trials j = jc + P*u, u in [u0, u1), whose phase
+// row p and window start b0 (+ u*Hs) are fixed, so the m weights and the
+// complex factor stay in registers.  Same sequential FMA chain and unfused
+// complex product per trial as the reference's Float32 kernel.
+template <int M>
+__device__ __forceinline__ void class_run(const float* __restrict__ wt, int P, int p, float2 A,
+                                          const float2* __restrict__ win, int b0, int Hs, int jc, int u0,
+                                          int u1, float2* xo, int m) {
+    if (M > 0) {
+        constexpr int MW = M > 0 ? M : 1;
+        float w[MW];
+#pragma unroll
+        for (int i = 0; i < M; ++i) w[i] = __ldg(wt + i * P + p);
+#pragma unroll 2
+        for (int u = u0; u < u1; ++u) {
+            const float2* x = win + b0 + u * Hs;
+            float sre = 0.0f, sim = 0.0f;
+#pragma unroll
+            for (int i = 0; i < M; ++i) {
+                const float2 xi = x[i];
+                sre = fmaf(w[i], xi.x, sre);
+                sim = fmaf(w[i], xi.y, sim);
+            }
+            xo[jc + P * u] = cmul_unfused(A, make_float2(sre, sim));
+        }
+    } else {
+        for (int u = u0; u < u1; ++u) {
+            const float2* x = win + b0 + u * Hs;
+            float sre = 0.0f, sim = 0.0f;
+            for (int i = 0; i < m; ++i) {
+                const float wi = __ldg(wt + i * P + p);
+                const float2 xi = x[i];
+                sre = fmaf(wi, xi.x, sre);
+                sim = fmaf(wi, xi.y, sim);
+            }
+            xo[jc + P * u] = cmul_unfused(A, make_float2(sre, sim));
+        }
+    }
+}
+
+// One CTA per (group of 4 harmonics, block).  Per harmonic: the range guard on
+// the block's TRUE trial range (src/directinterp.jl:490-496), the bin window
+// staged in shared memory, then every phase class of the block's trials --
+// trials t and t+P share the phase row (t mod P) and sit exactly
+// Hs = P*h*pnum/q bins apart -- split into runs over the threads.
+template <int M>
+__global__ void __launch_bounds__(256) k_interp(WaveArgs a, int win_max, int Nst, int* err) {
+    extern __shared__ float2 sm_i[];
+    float2* win = sm_i;
+    float2* xo = sm_i + win_max;            // [kHG][Nst] staged outputs
+    __shared__ int s_ok, s_nw, s_p0, s_res0, s_Ub, s_chunk, s_Tc, s_small;
+    __shared__ long long s_lo, s_base;      // s_base = rfloor0 + qint0 - lo + 1 - m2
+
+    const int hidx0 = blockIdx.x * kHG;
+    const int ng = min(kHG, a.nharms - hidx0);
+    const int blk = blockIdx.y;
     const int m = M > 0 ? M : a.m;
     const int m2 = m / 2;
     const int64_t t0 = a.t_first + (int64_t)blk * a.Nprof;
     const int n = (int)min((int64_t)a.Nprof, a.total - t0);
     if (n <= 0) return;
-    float2* __restrict__ xrow = a.X + ((int64_t)blk * a.nharms + hidx) * a.Nprof;
 
-    if (hp.P == 0) {
-        // Per-trial FP64 fallback for a non-rational trial step
-        // (_fill_row_direct_slow!, src/directinterp.jl:623-661).  Julia does not
-        // contract, so the FP64 expressions are evaluated with explicit rounding.
-        const double rfirst = __dadd_rn(hp.hr_lo, __dmul_rn((double)t0, hp.dh));
-        const double rlast = __dadd_rn(hp.hr_lo, __dmul_rn((double)(t0 + n - 1), hp.dh));
-        const int64_t lo = (int64_t)floor(__dadd_rn(rfirst, 1e-15)) + 2 - m2;
-        const int64_t hi = (int64_t)floor(__dadd_rn(rlast, 1e-15)) + 1 + m2;
-        const bool ok = lo >= 1 && hi <= a.namps && (int64_t)floor(rlast) < a.Nhalf;
-        for (int j = threadIdx.x; j < n; j += blockDim.x) {
-            float2 out = make_float2(0.0f, 0.0f);
-            if (ok) {
-                const double r = __dadd_rn(hp.hr_lo, __dmul_rn((double)(t0 + j), hp.dh));
-                const int64_t rint = (int64_t)floor(__dadd_rn(r, 1e-15)) + 1;
-                const double dr = fmod(r, 1.0);
-                const int64_t base = rint - m2;  // 0-based tap i at base + i
-                if (dr == 0.0) {
-                    out = a.amps[base + m2 - 1];
-                } else {
-                    double sre = 0.0, sim = 0.0;
-                    for (int i = 0; i < m; ++i) {
-                        const double w = 1.0 / (dr - (double)(i + 1 - m2));
-                        const float2 x = a.amps[base + i];
-                        sre = fma(w, (double)x.x, sre);
-                        sim = fma(w, (double)x.y, sim);
-                    }
-                    const double s = sinpi(dr), c = cospi(dr);
-                    const double ar = __ddiv_rn(__dmul_rn(s, c), M_PI);
-                    const double ai = -__ddiv_rn(__dmul_rn(s, s), M_PI);
-                    out.x = (float)__dsub_rn(__dmul_rn(ar, sre), __dmul_rn(ai, sim));
-                    out.y = (float)__dadd_rn(__dmul_rn(ar, sim), __dmul_rn(ai, sre));
-                }
-            }
-            xrow[j] = out;
+    for (int g = 0; g < ng; ++g) {
+        const DevHarm hp = a.harms[hidx0 + g];
+        float2* xg = xo + g * Nst;
+        if (hp.P == 0) {
+            // Per-trial FP64 fallback for a non-rational trial step
+            // (_fill_row_direct_slow!, src/directinterp.jl:623-661).
+            const bool ok = harm_guard(a, hp, t0, n);
+            for (int j = threadIdx.x; j < n; j += blockDim.x)
+                xg[j] = ok ? exact_amp(a, hp, t0 + j, 0, 0) : make_float2(0.0f, 0.0f);
+            __syncthreads();
+            continue;
         }
-        return;
+        const float* __restrict__ wt = a.wtab + hp.w_off;
+        const float2* __restrict__ at = a.atab + hp.a_off;
+        const uint8_t* __restrict__ ct = a.ctab + hp.a_off;
+        const int64_t hpn = (int64_t)hp.h * hp.pnum;
+        if (threadIdx.x == 0) {
+            const int64_t T0 = t0 * hpn;
+            const int64_t qint0 = T0 / hp.q;
+            const int p0 = (int)(t0 % hp.P);
+            const int64_t tl = t0 + n - 1;
+            const int64_t qintl = (tl * hpn) / hp.q;
+            const int pl = (int)(tl % hp.P);
+            const int64_t fl0 = hp.rfloor0 + qint0 + ct[p0];
+            const int64_t fll = hp.rfloor0 + qintl + ct[pl];
+            const bool ok = (fl0 + 2 - m2 >= 1) && (fll + 1 + m2 <= a.namps) &&
+                            (hp.rfloor0 + qintl < a.Nhalf);
+            const int64_t lo = fl0 + 1 - m2;
+            const int64_t nw = fll + m2 - lo + 1;
+            s_ok = ok && nw <= win_max;
+            if (ok && nw > win_max) atomicExch(err, 1);
+            s_lo = lo;
+            s_nw = (int)min(nw, (int64_t)win_max);
+            s_p0 = p0;
+            s_res0 = (int)(T0 % hp.q);
+            s_base = hp.rfloor0 + qint0 - lo + 1 - m2;
+            // task split of the phase classes (see below), once per harmonic
+            const int P = hp.P;
+            const int Tc = P >= (int)blockDim.x ? 1 : (int)blockDim.x / P;
+            const int Ub = n / P;                       // classes jc < n - Ub*P get Ub+1 trials
+            s_Ub = Ub;
+            s_Tc = Tc;
+            s_chunk = (Ub + 1 + Tc - 1) / Tc;
+            // res0 + jc*h*pnum < 2^32 for every class: the window start fits 32-bit math
+            s_small = ((uint64_t)hp.q + (uint64_t)P * (uint64_t)hpn) < 0xFFFFFFFFull;
+        }
+        __syncthreads();
+        if (!s_ok) {
+            for (int j = threadIdx.x; j < n; j += blockDim.x) xg[j] = make_float2(0.0f, 0.0f);
+            __syncthreads();
+            continue;
+        }
+        const int nw = s_nw;
+        const float2* __restrict__ src = a.amps + s_lo;
+        for (int i = threadIdx.x; i < nw; i += blockDim.x) win[i] = src[i];
+        __syncthreads();
+        const int P = hp.P, q = hp.q;
+        const int Hs = (int)(((int64_t)P * hpn) / q);   // bins between trials t and t+P
+        // Runs: class jc (first trial j = jc, phase (p0 + jc) mod P), part `part`
+        // of its u range; classes below n - Ub*P have Ub+1 trials, the rest Ub.
+        const int Tc = s_Tc, Ub = s_Ub, chunk = s_chunk, p0 = s_p0, res0 = s_res0;
+        const int ntask = P >= (int)blockDim.x ? P : P * Tc;
+        const int nlong = n - Ub * P;
+        const float invP = 1.0f / (float)P;
+        for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
+            // task < 256 when Tc > 1: (task + 0.5)/P is >= 0.5/P from an integer,
+            // far above the float error, so the quotient is exact.
+            const int part = Tc > 1 ? (int)(((float)task + 0.5f) * invP) : 0;
+            const int jc = task - part * P;
+            if (jc >= n) continue;
+            const int U = Ub + (jc < nlong ? 1 : 0);
+            const int u0 = part * chunk, u1 = min(U, u0 + chunk);
+            if (u0 >= u1) continue;
+            int p = p0 + jc;
+            if (p >= P) p -= P;
+            const int64_t qv = s_small ? (int64_t)(((uint32_t)res0 + (uint32_t)jc * (uint32_t)hpn) / (uint32_t)q)
+                                       : ((int64_t)res0 + (int64_t)jc * hpn) / q;
+            const int b0 = (int)(s_base + qv + ct[p]);
+            class_run<M>(wt, P, p, __ldg(at + p), win, b0, Hs, jc, u0, u1, xg, m);
+        }
+        __syncthreads();
     }
-
-    const float* __restrict__ wt = a.wtab + hp.w_off;
-    const float2* __restrict__ at = a.atab + hp.a_off;
-    const uint8_t* __restrict__ ct = a.ctab + hp.a_off;
-    const int64_t hpn = (int64_t)hp.h * hp.pnum;
-    if (threadIdx.x == 0) {
-        // Range guard on the TRUE trial range (src/directinterp.jl:490-496),
-        // with the Julia 1-based bounds translated to 0-based windows.
-        const int64_t T0 = t0 * hpn;
-        const int64_t qint0 = T0 / hp.q;
-        const int p0 = (int)(t0 % hp.P);
-        const int64_t tl = t0 + n - 1;
-        const int64_t qintl = (tl * hpn) / hp.q;
-        const int pl = (int)(tl % hp.P);
-        const int64_t fl0 = hp.rfloor0 + qint0 + ct[p0];
-        const int64_t fll = hp.rfloor0 + qintl + ct[pl];
-        const bool ok = (fl0 + 2 - m2 >= 1) && (fll + 1 + m2 <= a.namps) &&
-                        (hp.rfloor0 + qintl < a.Nhalf);
-        const int64_t lo = fl0 + 1 - m2;
-        const int64_t nw = fll + m2 - lo + 1;
-        s_ok = ok && nw <= win_max;
-        if (ok && nw > win_max) atomicExch(err, 1);
-        s_lo = lo;
-        s_nw = (int)min(nw, (int64_t)win_max);
-        s_p0 = p0;
-        s_res0 = (int)(T0 % hp.q);
-        s_base = hp.rfloor0 + qint0 - lo + 1 - m2;
-    }
-    __syncthreads();
-    if (!s_ok) {
-        for (int j = threadIdx.x; j < n; j += blockDim.x) xrow[j] = make_float2(0.0f, 0.0f);
-        return;
-    }
-    const int nw = s_nw;
-    const float2* __restrict__ src = a.amps + s_lo;
-    for (int i = threadIdx.x; i < nw; i += blockDim.x) win[i] = src[i];
-    __syncthreads();
-
-    const int P = hp.P, q = hp.q;
-    const int step = blockDim.x;
-    // Trial j: p = (p0 + j) mod P;  (res0 + j*hpn) = qv*q + rv.
-    int j = threadIdx.x;
-    int p = (int)((s_p0 + (int64_t)j) % P);
-    const int pstep = step % P;
-    int64_t v = (int64_t)s_res0 + (int64_t)j * hpn;
-    int64_t qv = v / q;
-    int rv = (int)(v % q);
-    const int64_t dv = (int64_t)step * hpn;
-    const int64_t dq = dv / q;
-    const int drr = (int)(dv % q);
-    const int64_t base0 = s_base;
-    for (; j < n; j += step) {
-        const int b = (int)(base0 + qv + ct[p]);   // window index of tap 0
-        const float2 s = tap_sum<M>(wt, P, p, win + b, m);
-        xrow[j] = cmul_unfused(at[p], s);
-        p += pstep;
-        if (p >= P) p -= P;
-        qv += dq;
-        rv += drr;
-        if (rv >= q) { rv -= q; qv += 1; }
-    }
+    emit_rows(a, xo, Nst, blk, hidx0, ng, n);
 }
 
+size_t interp_smem(int win_max, int Nprof) { return (size_t)(win_max + kHG * Nprof) * sizeof(float2); }
+
 cudaError_t launch_interp(const WaveArgs& a, cudaStream_t st, int win_max, int* err) {
-    dim3 grid(a.nblk, a.nharms);
-    const size_t smem = (size_t)win_max * sizeof(float2);
+    dim3 grid((a.nharms + kHG - 1) / kHG, a.nblk);
+    const size_t smem = interp_smem(win_max, a.Nprof);
+    const int Nst = a.Nprof;
     switch (a.m) {
         case 16:
             cudaFuncSetAttribute(k_interp<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            k_interp<16><<<grid, 256, smem, st>>>(a, win_max, err);
+            k_interp<16><<<grid, 256, smem, st>>>(a, win_max, Nst, err);
             break;
         case 32:
             cudaFuncSetAttribute(k_interp<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            k_interp<32><<<grid, 256, smem, st>>>(a, win_max, err);
+            k_interp<32><<<grid, 256, smem, st>>>(a, win_max, Nst, err);
             break;
         case 8:
             cudaFuncSetAttribute(k_interp<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            k_interp<8><<<grid, 256, smem, st>>>(a, win_max, err);
+            k_interp<8><<<grid, 256, smem, st>>>(a, win_max, Nst, err);
             break;
         default:
             cudaFuncSetAttribute(k_interp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            k_interp<0><<<grid, 256, smem, st>>>(a, win_max, err);
+            k_interp<0><<<grid, 256, smem, st>>>(a, win_max, Nst, err);
             break;
     }
     return cudaGetLastError();
@@ -215,6 +355,7 @@ __device__ __forceinline__ void synth_chunk8(const float2* __restrict__ xs, int 
                                              int n0, float E[8], float O[8]) {
 #pragma unroll
     for (int u = 0; u < 8; ++u) { E[u] = 0.0f; O[u] = 0.0f; }
+#pragma unroll 4
     for (int jh = 1; jh < Hk; ++jh) {
         const float2 x = xs[(jh * k - 1) * xstride];
         const float4 c0 = *reinterpret_cast<const float4*>(C2 + jh * np + n0);
@@ -233,16 +374,6 @@ __device__ __forceinline__ void synth_chunk8(const float2* __restrict__ xs, int 
     const float ny = xs[(Hk * k - 1) * xstride].x;
 #pragma unroll
     for (int u = 0; u < 8; ++u) E[u] = E[u] + (((n0 + u) & 1) ? -ny : ny);
-}
-
-// Slot of profile column j among the columns _block_sigma pools for a
-// (block, level) with nv valid columns (src/search.jl:528-537), or -1.
-__device__ __forceinline__ int sigma_slot(int j, int nv, int nbins) {
-    if ((int64_t)nbins * nv <= kSigmaCap) return j < nv ? j : -1;
-    const int ncol = min(nv, max(1, kSigmaCap / nbins));
-    const int c = (int)(((int64_t)j * ncol + nv - 1) / nv);  // ceil(j*ncol/nv)
-    if (c < ncol && (int)(((int64_t)c * nv) / ncol) == j) return c;
-    return -1;
 }
 
 __global__ void __launch_bounds__(2 * kTileTrials) k_synth_fp32(WaveArgs a) {
@@ -286,14 +417,6 @@ __global__ void __launch_bounds__(2 * kTileTrials) k_synth_fp32(WaveArgs a) {
             }
         }
         __syncthreads();
-        if (j < nv) {
-            const int slot = sigma_slot(j, nv, nbins);
-            if (slot >= 0) {
-                float* dst = a.sub + ((int64_t)blk * a.nlev + l) * kSigmaCap + (int64_t)slot * nbins;
-                for (int i = half; i < nbins; i += 2) dst[i] = fabsf(buf[(OFF + i) * TT + t]);
-            }
-        }
-        __syncthreads();
         if (half == 0) {
             // Wrapped prefix sums in place: ps[i] lands in row i, reading prof
             // from row OFF+i >= i+1 before it is overwritten.
@@ -334,74 +457,169 @@ cudaError_t launch_synth_fp32(const WaveArgs& a, cudaStream_t st, int smem_bytes
 }
 
 // ---------------------------------------------------------------------------
-// Block sigma: exact median of the pooled |x| samples (radix select)
+// Block sigma: exact FP32 profiles of the pooled columns, then the exact median
 // ---------------------------------------------------------------------------
 
-// k-th smallest (0-based) of ns non-negative floats given as bit patterns;
-// non-negative IEEE floats order like their unsigned bit patterns.
-__device__ uint32_t radix_select(const uint32_t* vals, int ns, int kth, uint32_t* hist, int* sh) {
+// Block-wide exclusive prefix sum of one int per thread (blockDim.x == 256).
+__device__ __forceinline__ int block_excl_scan(int v, int* warp_tot, int* total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int w = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+        int incl = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane < (int)(blockDim.x >> 5)) warp_tot[lane] = incl - w;
+        if (lane == 31) *total = incl;
+    }
+    __syncthreads();
+    const int r = warp_tot[wid] + x - v;
+    __syncthreads();
+    return r;
+}
+
+// k-th smallest (0-based) of ns non-negative floats given as bit patterns
+// (non-negative IEEE floats order like their unsigned bits): three radix
+// passes of 11/11/10 bits with a parallel bucket search.
+__device__ uint32_t radix_select(const uint32_t* vals, int ns, int kth, uint32_t* hist, int* sh, int* wtot) {
     uint32_t prefix = 0, mask = 0;
     int kk = kth;
-    for (int shift = 24; shift >= 0; shift -= 8) {
-        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+    const int shifts[3] = {21, 10, 0};
+    const int bits[3] = {11, 11, 10};
+    for (int pass = 0; pass < 3; ++pass) {
+        const int shift = shifts[pass], nb = 1 << bits[pass];
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) hist[i] = 0;
         __syncthreads();
         for (int i = threadIdx.x; i < ns; i += blockDim.x) {
             const uint32_t v = vals[i];
-            if ((v & mask) == prefix) atomicAdd(&hist[(v >> shift) & 255u], 1u);
+            if ((v & mask) == prefix) atomicAdd(&hist[(v >> shift) & (uint32_t)(nb - 1)], 1u);
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            int cum = 0, d = 0;
-            for (; d < 255; ++d) {
-                const int c = (int)hist[d];
-                if (cum + c > kk) break;
-                cum += c;
+        const int per = nb / (int)blockDim.x;
+        int local = 0;
+        for (int b = 0; b < per; ++b) local += (int)hist[threadIdx.x * per + b];
+        const int excl = block_excl_scan(local, wtot, sh + 2);
+        if (excl <= kk && kk < excl + local) {
+            int c = excl;
+            for (int b = 0; b < per; ++b) {
+                const int hb = (int)hist[threadIdx.x * per + b];
+                if (c + hb > kk) {
+                    sh[0] = threadIdx.x * per + b;
+                    sh[1] = kk - c;
+                    break;
+                }
+                c += hb;
             }
-            sh[0] = d;
-            sh[1] = kk - cum;
         }
         __syncthreads();
         prefix |= (uint32_t)sh[0] << shift;
-        mask |= 255u << shift;
+        mask |= (uint32_t)(nb - 1) << shift;
         kk = sh[1];
         __syncthreads();
     }
     return prefix;
 }
 
+// One CTA per (block, level).  The columns _block_sigma pools
+// (src/search.jl:528-537): every valid column when nbins*nv <= 8192, else ncol
+// whole columns spaced evenly.  k_interp leaves their exact FP32 amplitudes in
+// `samp`; their profiles are built here with synth_chunk8 -- the arithmetic of
+// the FP32 synthesis and of the rescan -- so sigma is identical in every
+// synthesis mode.  sigma = 1.4826 * median(|x|), _median! semantics.
 __global__ void __launch_bounds__(256) k_sigma(WaveArgs a) {
-    __shared__ uint32_t vals[kSigmaCap];
-    __shared__ uint32_t hist[256];
-    __shared__ int sh[2];
+    extern __shared__ float4 ss4[];
+    __shared__ uint32_t hist[2048];
+    __shared__ int sh[4];
+    __shared__ int wtot[32];
+    __shared__ uint32_t red[8];
     const int bl = blockIdx.x;
     const int l = bl % a.nlev;
-    const int nbins = a.levels[l].nbins;
+    const DevLevel& L = a.levels[l];
+    const int Hk = L.Hk, nbins = L.nbins, np = L.np;
     const int nv = a.nvalid[bl];
-    const int64_t N = (int64_t)nbins * nv;
-    int ns;
-    if (N <= kSigmaCap) ns = (int)N;
-    else ns = min(nv, max(1, kSigmaCap / nbins)) * nbins;
-    if (ns == 0) {
+    if (nv <= 0) {
         if (threadIdx.x == 0) a.sigma[bl] = 0.0f;
         return;
     }
-    const float* src = a.sub + (int64_t)bl * kSigmaCap;
-    for (int i = threadIdx.x; i < ns; i += blockDim.x) vals[i] = __float_as_uint(src[i]);
+    const bool all = (int64_t)nbins * nv <= kSigmaCap;
+    const int ncs = all ? nv : min(nv, max(1, kSigmaCap / nbins));
+    const int ns = ncs * nbins;
+    float* tws = reinterpret_cast<float*>(ss4);                 // C2 then S2: 2*Hk*np
+    float2* Xs = reinterpret_cast<float2*>(tws + 2 * Hk * np);  // [Hk][ncs]
+    uint32_t* vals = reinterpret_cast<uint32_t*>(Xs + kSigmaCap / 2);  // [ns]
+    const float4* tsrc = reinterpret_cast<const float4*>(a.tw + L.tw_off);
+    for (int i = threadIdx.x; i < 2 * Hk * np / 4; i += blockDim.x) ss4[i] = tsrc[i];
+    const float2* samp = a.samp + (int64_t)bl * kSampStride;
+    for (int idx = threadIdx.x; idx < Hk * ncs; idx += blockDim.x) Xs[idx] = samp[idx];
+    __syncthreads();
+    const int nch = (Hk + 1 + 7) / 8;
+    for (int idx = threadIdx.x; idx < ncs * nch; idx += blockDim.x) {
+        const int sl = idx % ncs, ch = idx / ncs;
+        const int n0 = ch * 8;
+        float E[8], O[8];
+        synth_chunk8(Xs + sl, ncs, tws, tws + Hk * np, np, 1, Hk, n0, E, O);
+        uint32_t* dst = vals + sl * nbins;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int nn = n0 + u;
+            if (nn <= Hk) dst[nn] = __float_as_uint(fabsf(E[u] + O[u]));
+            if (nn >= 1 && nn < Hk) dst[2 * Hk - nn] = __float_as_uint(fabsf(E[u] - O[u]));
+        }
+    }
     __syncthreads();
     const int half = ns >> 1;
     float med;
     if (ns & 1) {
-        med = __uint_as_float(radix_select(vals, ns, half, hist, sh));
+        med = __uint_as_float(radix_select(vals, ns, half, hist, sh, wtot));
     } else {
-        const float lo = __uint_as_float(radix_select(vals, ns, half - 1, hist, sh));
-        const float hi = __uint_as_float(radix_select(vals, ns, half, hist, sh));
-        med = 0.5f * (lo + hi);
+        // _median! (src/search.jl:295-305): mean of the two central order statistics.
+        const uint32_t lo = radix_select(vals, ns, half - 1, hist, sh, wtot);
+        int le = 0;
+        uint32_t above = 0xFFFFFFFFu;
+        for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+            const uint32_t v = vals[i];
+            le += v <= lo;
+            if (v > lo && v < above) above = v;
+        }
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            le += __shfl_xor_sync(0xffffffffu, le, o);
+            above = min(above, __shfl_xor_sync(0xffffffffu, above, o));
+        }
+        if (lane == 0) { wtot[wid] = le; red[wid] = above; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int tle = 0;
+            uint32_t tab = 0xFFFFFFFFu;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tle += wtot[w]; tab = min(tab, red[w]); }
+            sh[3] = (int)(tle >= half + 1 ? lo : tab);
+        }
+        __syncthreads();
+        med = 0.5f * (__uint_as_float(lo) + __uint_as_float((uint32_t)sh[3]));
     }
     if (threadIdx.x == 0) a.sigma[bl] = 1.4826f * med;
 }
 
-cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st) {
-    k_sigma<<<a.nblk * a.nlev, 256, 0, st>>>(a);
+size_t sigma_smem(int max_hk, int max_np) {
+    return (size_t)2 * max_hk * max_np * sizeof(float) + (size_t)(kSigmaCap / 2) * sizeof(float2) +
+           (size_t)kSigmaCap * sizeof(uint32_t);
+}
+
+cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np) {
+    const size_t smem = sigma_smem(max_hk, max_np);
+    cudaFuncSetAttribute(k_sigma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_sigma<<<a.nblk * a.nlev, 256, smem, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -423,6 +641,7 @@ __device__ __forceinline__ void push_cand(const WaveArgs& a, int blk, int l, int
 
 __device__ __forceinline__ float inv_sigma(float sig) { return sig > 0.0f ? 1.0f / sig : 0.0f; }
 
+// medcut test of the gate (boxcar_metrics!, src/search.jl:825-843).
 __global__ void __launch_bounds__(256) k_flag(WaveArgs a) {
     const int64_t n_all = (int64_t)a.nblk * a.nlev * a.Nprof;
     for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n_all;
@@ -437,7 +656,7 @@ __global__ void __launch_bounds__(256) k_flag(WaveArgs a) {
             continue;
         }
         const float m0 = a.Q0[idx] * invsig;
-        if (m0 >= a.medcut) {
+        if (m0 >= a.medcut_gate) {
             const int pos = atomicAdd(a.n_items, 1);
             if (pos < a.cap_items) {
                 DevItem it;
@@ -460,63 +679,35 @@ cudaError_t launch_flag(const WaveArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-// Exact metric of one (block, level, trial): the profile recomputed with the
-// tile kernel's arithmetic, its median as baseline, sequential wrapped prefix
-// sums, and the width/phase scan (src/search.jl:571-598, :893-904).
-__device__ float exact_metric(const WaveArgs& a, int blk, int l, int j, float invsig) {
-    const DevLevel& L = a.levels[l];
-    const int k = L.k, Hk = L.Hk, nbins = L.nbins, wmax = L.wmax, np = L.np;
-    float prof[kMaxBins];
-    float srt[kMaxBins];
-    float ps[kMaxBins + kMaxBins + 1];
-    const float2* xs = a.X + (int64_t)blk * a.nharms * a.Nprof + j;
-    const float* C2 = a.tw + L.tw_off;
-    const float* S2 = C2 + (int64_t)Hk * np;
-    for (int n0 = 0; n0 <= Hk; n0 += 8) {
-        float E[8], O[8];
-        synth_chunk8(xs, a.Nprof, C2, S2, np, k, Hk, n0, E, O);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int nn = n0 + u;
-            if (nn <= Hk) prof[nn] = E[u] + O[u];
-            if (nn >= 1 && nn < Hk) prof[2 * Hk - nn] = E[u] - O[u];
-        }
-    }
-    for (int i = 0; i < nbins; ++i) {
-        const float x = prof[i];
-        int q = i - 1;
-        while (q >= 0 && srt[q] > x) { srt[q + 1] = srt[q]; --q; }
-        srt[q + 1] = x;
-    }
-    const int half = nbins >> 1;
-    const float med = (nbins & 1) ? srt[half] : 0.5f * (srt[half - 1] + srt[half]);
-    ps[0] = 0.0f;
-    for (int i = 0; i < nbins + wmax; ++i) {
-        const int idx = i >= nbins ? i - nbins : i;
-        ps[i + 1] = ps[i] + (prof[idx] - med);
-    }
-    float best = -INFINITY;
-    for (int wi = 0; wi < L.nw; ++wi) {
-        const int w = L.widths[wi];
-        const float invsw = invsig / sqrtf((float)w);
-        float mm = ps[w] - ps[0];
-        for (int p = 1; p < nbins; ++p) mm = fmaxf(mm, ps[p + w] - ps[p]);
-        const float cand = mm * invsw;
-        if (cand > best) best = cand;
-    }
-    return best;
-}
+constexpr int kRescueWarps = 4;
 
-__global__ void __launch_bounds__(128) k_rescue(WaveArgs a) {
+// One warp per (block, level, trial).  Lanes recompute the exact amplitudes of
+// the level's harmonics, then the FP32 profile chunks (synth_chunk8, the
+// arithmetic of the FP32 synthesis), then:
+//  * when the gate was a 16-bit one, the FP32 zero-baseline gate exactly as
+//    k_synth_fp32 forms it, against medcut -- so the rescanned set is the
+//    plain form's;
+//  * the exact metric: median baseline (order statistics by rank counting),
+//    sequential wrapped prefix sums, max over phase and width
+//    (src/search.jl:571-598, :893-904).
+__global__ void __launch_bounds__(32 * kRescueWarps) k_rescue(WaveArgs a) {
+    __shared__ float2 xs_all[kRescueWarps][kMaxBins / 2 + 8];
+    __shared__ float prof_all[kRescueWarps][kMaxBins];
+    __shared__ float ps_all[kRescueWarps][2 * kMaxBins + 2];
+    __shared__ float med_all[kRescueWarps][2];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float2* xs = xs_all[wid];
+    float* prof = prof_all[wid];
+    float* ps = ps_all[wid];
     const int64_t count = a.exact_all ? (int64_t)a.nblk * a.nlev * a.Nprof
                                       : (int64_t)min(*a.n_items, a.cap_items);
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < count;
-         idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t gwarps = (int64_t)gridDim.x * kRescueWarps;
+    for (int64_t idx = blockIdx.x * (int64_t)kRescueWarps + wid; idx < count; idx += gwarps) {
         int blk, l, j;
         if (a.exact_all) {
             j = (int)(idx % a.Nprof);
             const int bl = (int)(idx / a.Nprof);
-            if (j >= a.nvalid[bl]) continue;
+            if (j >= a.nvalid[bl]) continue;   // warp-uniform
             l = bl % a.nlev;
             blk = bl / a.nlev;
         } else {
@@ -526,14 +717,118 @@ __global__ void __launch_bounds__(128) k_rescue(WaveArgs a) {
             j = it.j;
         }
         const float invsig = inv_sigma(a.sigma[blk * a.nlev + l]);
-        const float metric = invsig > 0.0f ? exact_metric(a, blk, l, j, invsig) : 0.0f;
-        if (a.tmetric) a.tmetric[((int64_t)blk * a.nlev + l) * a.Nprof + j] = metric;
-        if (metric > a.threshold) push_cand(a, blk, l, j, metric);
+        const DevLevel& L = a.levels[l];
+        const int k = L.k, Hk = L.Hk, nbins = L.nbins, np = L.np, nw = L.nw, wmax = L.wmax;
+        float metric = 0.0f;
+        if (invsig > 0.0f) {
+            const int64_t t0 = a.t_first + (int64_t)blk * a.Nprof;
+            const int n = (int)min((int64_t)a.Nprof, a.total - t0);
+            const int64_t t = t0 + j;
+            for (int jh = 1 + lane; jh <= Hk; jh += 32) {
+                const DevHarm& hp = a.harms[jh * k - 1];
+                float2 v = make_float2(0.0f, 0.0f);
+                if (harm_guard(a, hp, t0, n)) {
+                    int64_t tdq;
+                    int tmq;
+                    tq_split(hp, t, &tdq, &tmq);
+                    v = exact_amp(a, hp, t, tdq, tmq);
+                }
+                xs[jh - 1] = v;
+            }
+            __syncwarp();
+            const float* C2 = a.tw + L.tw_off;
+            const float* S2 = C2 + (int64_t)Hk * np;
+            const int nch = (Hk + 1 + 7) / 8;
+            if (lane < nch) {
+                const int n0 = lane * 8;
+                float E[8], O[8];
+                synth_chunk8(xs, 1, C2, S2, np, 1, Hk, n0, E, O);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int nn = n0 + u;
+                    if (nn <= Hk) prof[nn] = E[u] + O[u];
+                    if (nn >= 1 && nn < Hk) prof[2 * Hk - nn] = E[u] - O[u];
+                }
+            }
+            __syncwarp();
+            bool exact = true;
+            if (a.verify_gate) {
+                // k_synth_fp32's gate: sequential prefix, wrap as ps[nbins] + ps[u].
+                if (lane == 0) {
+                    float s = 0.0f;
+                    ps[0] = 0.0f;
+                    for (int i = 0; i < nbins; ++i) { s += prof[i]; ps[i + 1] = s; }
+                    for (int u = 1; u <= wmax; ++u) ps[nbins + u] = s + ps[u];
+                }
+                __syncwarp();
+                float best = -INFINITY;
+                for (int wi = 0; wi < nw; ++wi) {
+                    const int w = L.widths[wi];
+                    float mm = -INFINITY;
+                    for (int p = lane; p < nbins; p += 32) mm = fmaxf(mm, ps[p + w] - ps[p]);
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) mm = fmaxf(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+                    best = fmaxf(best, mm * L.rsqrtw[wi]);
+                }
+                const float m0 = best * invsig;
+                if (!(m0 >= a.medcut)) {
+                    metric = m0;
+                    exact = false;
+                }
+                __syncwarp();
+            }
+            if (exact) {
+                // Median: the values of rank half-1 and half by counting.
+                const int half = nbins >> 1;
+                for (int i = lane; i < nbins; i += 32) {
+                    const float v = prof[i];
+                    int lt = 0, le = 0;
+                    for (int q2 = 0; q2 < nbins; ++q2) {
+                        const float u = prof[q2];
+                        lt += u < v;
+                        le += u <= v;
+                    }
+                    if (nbins & 1) {
+                        if (lt <= half && half < le) med_all[wid][0] = v;
+                    } else {
+                        if (lt <= half - 1 && half - 1 < le) med_all[wid][0] = v;
+                        if (lt <= half && half < le) med_all[wid][1] = v;
+                    }
+                }
+                __syncwarp();
+                const float med = (nbins & 1) ? med_all[wid][0] : 0.5f * (med_all[wid][0] + med_all[wid][1]);
+                if (lane == 0) {
+                    ps[0] = 0.0f;
+                    for (int i = 0; i < nbins + wmax; ++i) {
+                        const int id = i >= nbins ? i - nbins : i;
+                        ps[i + 1] = ps[i] + (prof[id] - med);
+                    }
+                }
+                __syncwarp();
+                float best = -INFINITY;
+                for (int wi = 0; wi < nw; ++wi) {
+                    const int w = L.widths[wi];
+                    const float invsw = invsig / sqrtf((float)w);
+                    float mm = -INFINITY;
+                    for (int p = lane; p < nbins; p += 32) mm = fmaxf(mm, ps[p + w] - ps[p]);
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) mm = fmaxf(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+                    const float cand = mm * invsw;
+                    if (cand > best) best = cand;
+                }
+                metric = best;
+            }
+        }
+        if (lane == 0) {
+            if (a.tmetric) a.tmetric[((int64_t)blk * a.nlev + l) * a.Nprof + j] = metric;
+            if (metric > a.threshold) push_cand(a, blk, l, j, metric);
+        }
+        __syncwarp();
     }
 }
 
 cudaError_t launch_rescue(const WaveArgs& a, cudaStream_t st, int num_sms) {
-    k_rescue<<<num_sms * 8, 128, 0, st>>>(a);
+    k_rescue<<<num_sms * 8, 32 * kRescueWarps, 0, st>>>(a);
     return cudaGetLastError();
 }
 

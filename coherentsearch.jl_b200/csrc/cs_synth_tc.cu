@@ -1,0 +1,477 @@
+// cs_synth_tc.cu -- tensor-core profile synthesis + zero-baseline boxcar gate
+// (the mixed-precision form of k_synth_fp32).
+//
+// The c2r transform of every decimation level is linear in the amplitude
+// stack, so all levels come out of ONE product per 128-trial tile:
+//   D[trial][col] = sum_k A[trial][k] * B[col][k]
+// with A = (Re X_1, Im X_1, Re X_2, ..., Im X_60) in BF16/FP16 and B the
+// host-built FP64 twiddles rounded once, one column per profile bin of every
+// level followed by that level's first wmax bins again (the wrapped tail of
+// the boxcar prefix sums, src/search.jl:571-578).  tcgen05.mma (M=128, K=16
+// per instruction, FP32 accumulation in TMEM) computes D; each epilogue thread
+// owns one trial's TMEM row and streams its bins through a register ring of
+// prefix sums to the zero-baseline gate value (src/search.jl:743-779) and the
+// block-sigma samples.  The gate only selects the trials that take the exact
+// FP32 rescan, so the reported S/N never depends on the reduced precision.
+//
+// Layout: SWIZZLE_NONE K-major canonical UMMA layout -- 8-row x 16-byte core
+// matrices, K-adjacent core matrices 128 B apart (LBO), 8-row groups 2048 B
+// apart (SBO).  One persistent CTA per SM (it holds all 512 TMEM columns).
+#include "cs_internal.h"
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <math.h>
+
+#include <cmath>
+#include <vector>
+
+namespace cs {
+
+namespace {
+
+constexpr int kTM = 128;            // trials per tile (MMA M)
+constexpr int kK = 128;             // padded K: 2*nharms <= 128
+constexpr int kSBO = (kK / 8) * 128;  // bytes between 8-row groups
+constexpr int kABytes = kTM * kK * 2;
+constexpr uint32_t kWaitLimit = 1u << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);                 // start address
+    d |= (uint64_t)((128 >> 4) & 0x3FFF) << 16;             // LBO: K-adjacent core matrices
+    d |= (uint64_t)((kSBO >> 4) & 0x3FFF) << 32;            // SBO: 8-row groups
+    d |= (uint64_t)1 << 46;                                 // descriptor version (sm_100)
+    return d;                                               // base offset 0, SWIZZLE_NONE
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait on an mbarrier phase: gives up after kWaitLimit polls or one
+// second of wall time, whichever comes first.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((it & 1023u) == 1023u && global_ns() - t0 > 1000000000ull) return false;
+    }
+    return false;
+}
+
+// Plain (non-multicast) 1-D bulk copy global -> this CTA's shared memory,
+// completing `bytes` of transaction on mbarrier `bar` (armed here).
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float v[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                   "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float v[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+          "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+          "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+          "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Zero-baseline gate of one level streamed out of TMEM: wrapped prefix sums
+// ps[e] over the level's columns (nbins bins, then its first wmax bins again,
+// then zero padding to a multiple of HM), ring[e mod HM] holding the prefix at
+// each start position (+inf once the start would lie past the profile, so
+// windows that would start there -- including every window through the zero
+// padding -- never count), and per width w the max of ps[e] - ps[e-w].
+// MASK (bit w-1 per width) is a compile-time width set; MASK == 0 reads the
+// runtime mask instead.
+template <int HM, uint32_t MASK>
+struct GateScan {
+    float ring[HM];
+    float mw[HM];
+    float ps;
+    uint32_t wm;
+
+    __device__ __forceinline__ void init(uint32_t runtime_mask) {
+#pragma unroll
+        for (int d = 0; d < HM; ++d) { ring[d] = INFINITY; mw[d] = -INFINITY; }
+        ring[0] = 0.0f;
+        ps = 0.0f;
+        wm = MASK ? MASK : runtime_mask;
+    }
+    // One bin at column e_bin, whose ring slot of position e_bin+1 is SLOT.
+    template <int SLOT>
+    __device__ __forceinline__ void step(float x, int e_bin, int nbins) {
+        ps += x;
+#pragma unroll
+        for (int w = 1; w <= HM; ++w) {
+            const bool on = MASK ? ((MASK >> (w - 1)) & 1u) : ((wm >> (w - 1)) & 1u);
+            if (on) mw[w - 1] = fmaxf(mw[w - 1], ps - ring[(SLOT - w + HM) % HM]);
+        }
+        ring[SLOT % HM] = (e_bin + 1 < nbins) ? ps : INFINITY;
+    }
+    __device__ __forceinline__ float finish(const float* __restrict__ rsq) const {
+        float best = -INFINITY;
+#pragma unroll
+        for (int w = 1; w <= HM; ++w) {
+            const bool on = MASK ? ((MASK >> (w - 1)) & 1u) : ((wm >> (w - 1)) & 1u);
+            if (on) best = fmaxf(best, mw[w - 1] * rsq[w - 1]);
+        }
+        return best;
+    }
+};
+
+template <int U, int N, class G>
+struct Unroll {
+    __device__ __forceinline__ static void run(G& g, const float* x, int base, int nbins) {
+        g.template step<U + 1>(x[U], base + U, nbins);
+        Unroll<U + 1, N, G>::run(g, x, base, nbins);
+    }
+};
+template <int N, class G>
+struct Unroll<N, N, G> {
+    __device__ __forceinline__ static void run(G&, const float*, int, int) {}
+};
+
+// pw (the level's padded column count) is a multiple of HM.
+template <int HM, uint32_t MASK>
+__device__ __noinline__ float gate_level(uint32_t tcol, int nbins, int pw, uint32_t wmask,
+                                         const float* __restrict__ rsq) {
+    GateScan<HM, MASK> g;
+    g.init(wmask);
+    for (int c0 = 0; c0 < pw; c0 += 32) {
+        if (c0 + 32 <= pw) {
+            float x[32];
+            tmem_ld32(tcol + c0, x);
+            Unroll<0, 32, GateScan<HM, MASK>>::run(g, x, c0, nbins);
+        } else {
+            for (int c1 = c0; c1 < pw; c1 += 8) {   // HM == 8 here: pw is a multiple of 8
+                float x[8];
+                tmem_ld8(tcol + c1, x);
+                Unroll<0, 8, GateScan<HM, MASK>>::run(g, x, c1, nbins);
+            }
+        }
+    }
+    return g.finish(rsq);
+}
+
+// Width sets of the decimation ladder and of the plain geometric bank.
+constexpr uint32_t kMaskLadderBase = 0x2Fu;   // {1,2,3,4,6}
+constexpr uint32_t kMaskLadderDeep = 0x2Eu;   // {2,3,4,6}
+
+template <int HM>
+__device__ __forceinline__ float gate_dispatch(uint32_t tcol, int nbins, int pw, uint32_t wmask,
+                                               const float* __restrict__ rsq) {
+    if (HM == 8) {
+        if (wmask == kMaskLadderBase) return gate_level<8, kMaskLadderBase>(tcol, nbins, pw, wmask, rsq);
+        if (wmask == kMaskLadderDeep) return gate_level<8, kMaskLadderDeep>(tcol, nbins, pw, wmask, rsq);
+        return gate_level<8, 0u>(tcol, nbins, pw, wmask, rsq);
+    }
+    if (wmask == 0x4112Fu) return gate_level<32, 0x4112Fu>(tcol, nbins, pw, wmask, rsq);  // {1,..,13,19}
+    if (wmask == 0x804112Fu) return gate_level<32, 0x804112Fu>(tcol, nbins, pw, wmask, rsq);
+    return gate_level<32, 0u>(tcol, nbins, pw, wmask, rsq);
+}
+
+}  // namespace
+
+constexpr int kEpiThreads = 512;   // 4 warpgroups share the epilogue
+
+template <int HM>
+__global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs t, const uint4* __restrict__ Bg,
+                                                      int* err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* As0 = smem;                      // two A buffers, kABytes each
+    uint8_t* Bs = smem + 2 * kABytes;         // ncols_total * kK * 2
+    __shared__ uint64_t mbar;                 // MMA completion
+    __shared__ uint64_t lbar[2];              // A-tile arrival, one per buffer
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ TcLevel lev_sh[kMaxLevels];
+    __shared__ TcUnit unit_sh[kMaxUnits];
+    __shared__ float part_sh[kMaxUnits][kTM];   // per-unit gate partials of the tile
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int tiles_per_blk = a.tiles_per_blk;
+    const int ntiles = a.nblk * tiles_per_blk;
+
+    // B once per CTA.
+    const int bwords = t.ncols_total * kK * 2 / 16;
+    for (int i = tid; i < bwords; i += blockDim.x) reinterpret_cast<uint4*>(Bs)[i] = Bg[i];
+    if (tid < t.nlev) lev_sh[tid] = t.lev[tid];
+    if (tid < t.nunit) unit_sh[tid] = t.unit[tid];
+    if (tid == 0) {
+        mbar_init(&mbar, 1);
+        mbar_init(&lbar[0], 1);
+        mbar_init(&lbar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_base_sh)), "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_sh;
+
+    const uint32_t idesc_base = (1u << 4) | ((uint32_t)(t.fp16 ? 0 : 1) << 7) |
+                                ((uint32_t)(t.fp16 ? 0 : 1) << 10) | ((uint32_t)(kTM >> 4) << 24);
+    const uint32_t b_addr = smem_u32(Bs);
+    uint32_t phase = 0;
+    bool ok = true;
+    if (tid == 0 && (int)blockIdx.x < ntiles)
+        bulk_load(smem_u32(As0), a.Atile + (int64_t)blockIdx.x * kABytes, kABytes, &lbar[0]);
+
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
+        const int buf = it & 1;
+        const int blk = tile / tiles_per_blk;
+        const int j0 = (tile % tiles_per_blk) * kTM;
+        // Prefetch the next tile into the other buffer: its previous reader (the
+        // MMA of the last iteration) has completed.
+        if (tid == 0 && tile + (int)gridDim.x < ntiles)
+            bulk_load(smem_u32(As0 + (buf ^ 1) * kABytes), a.Atile + (int64_t)(tile + gridDim.x) * kABytes,
+                      kABytes, &lbar[buf ^ 1]);
+        ok = __syncthreads_and(mbar_wait(&lbar[buf], (uint32_t)((it >> 1) & 1))) != 0;
+        if (!ok) {
+            if (tid == 0) atomicExch(err, 2);
+            break;
+        }
+        const uint32_t a_addr = smem_u32(As0 + buf * kABytes);
+
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int nparts = t.ncols_total > t.n1 ? 2 : 1;
+            for (int part = 0; part < nparts; ++part) {
+                const int ncol0 = part ? t.n1 : 0;
+                const int nn = part ? t.ncols_total - t.n1 : t.n1;
+                const uint32_t idesc = idesc_base | ((uint32_t)(nn >> 3) << 17);
+                for (int ks = 0; ks < kK / 16; ++ks) {
+                    const uint64_t da = umma_desc(a_addr + ks * 256);
+                    const uint64_t db = umma_desc(b_addr + (ncol0 / 8) * kSBO + ks * 256);
+                    const uint32_t acc = ks > 0;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                        ::"r"(tmem + (uint32_t)ncol0), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(smem_u32(&mbar)) : "memory");
+        }
+        ok = __syncthreads_and(mbar_wait(&mbar, phase)) != 0;
+        if (!ok && tid == 0) atomicExch(err, 2);
+        if (ok) phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+        if (ok) {
+            // Epilogue: warpgroup g scans its units; thread owns TMEM row (warp%4)*32 + lane.
+            const int wg = warp >> 2;
+            const int row = (warp & 3) * 32 + (tid & 31);
+            const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+            for (int u = 0; u < t.nunit; ++u) {
+                const TcUnit& U = unit_sh[u];
+                if (U.wg != wg) continue;                               // warp-uniform
+                if (j0 >= a.nvalid[blk * a.nlev + U.lev]) continue;     // warp-uniform
+                const TcLevel& L = lev_sh[U.lev];
+                part_sh[u][row] = gate_dispatch<HM>(lane_base + (uint32_t)U.col, U.nstart, U.pw, L.wmask, L.rsq);
+            }
+            __syncthreads();
+            // Q0 = max over the level's units.
+            for (int idx = tid; idx < t.nlev * kTM; idx += blockDim.x) {
+                const int l = idx / kTM, r = idx % kTM;
+                const int j = j0 + r;
+                if (j >= a.nvalid[blk * a.nlev + l]) continue;
+                float g = -INFINITY;
+                for (int u = 0; u < t.nunit; ++u)
+                    if (unit_sh[u].lev == l) g = fmaxf(g, part_sh[u][r]);
+                a.Q0[((int64_t)blk * a.nlev + l) * a.Nprof + j] = g;
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+    }
+    if (!ok) {
+        // bounded: let an in-flight MMA and prefetch land before TMEM and smem go away
+        mbar_wait(&mbar, phase);
+        mbar_wait(&lbar[0], 0);
+        mbar_wait(&lbar[1], 0);
+    }
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side: the twiddle matrix, the level layout and the launch.
+// ---------------------------------------------------------------------------
+
+static uint16_t to_half_bits(float v, int fp16) {
+    if (fp16) {
+        __half h = __float2half_rn(v);
+        return *reinterpret_cast<uint16_t*>(&h);
+    }
+    __nv_bfloat16 b = __float2bfloat16_rn(v);
+    return *reinterpret_cast<uint16_t*>(&b);
+}
+
+int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, TcPlanHost* out) {
+    if (2 * nharms > kK) return -1;
+    TcArgs& t = out->args;
+    t = TcArgs{};
+    t.nlev = nlev;
+    t.fp16 = fp16;
+    int wmax = 0;
+    for (int l = 0; l < nlev; ++l) wmax = wmax > dl[l].wmax ? wmax : dl[l].wmax;
+    t.hm = wmax <= 8 ? 8 : (wmax <= 32 ? 32 : 0);
+    if (!t.hm) return -2;
+    int col = 0;
+    for (int l = 0; l < nlev; ++l) {
+        TcLevel& L = t.lev[l];
+        L.nbins = dl[l].nbins;
+        L.ncol = dl[l].nbins + dl[l].wmax;
+        L.pw = (L.ncol + t.hm - 1) / t.hm * t.hm;
+        L.col = col;
+        L.wmask = 0;
+        for (int i = 0; i < 32; ++i) L.rsq[i] = 0.0f;
+        for (int i = 0; i < dl[l].nw; ++i) {
+            const int w = dl[l].widths[i];
+            L.wmask |= 1u << (w - 1);
+            L.rsq[w - 1] = dl[l].rsqrtw[i];
+        }
+        col += L.pw;
+    }
+    const int total = (col + 15) / 16 * 16;
+    if (total > 512) return -3;
+    // Epilogue units: split each level's boxcar starts into segments of about
+    // equal scan cost (every segment re-reads wmax columns), then place them on
+    // the 4 warpgroups, heaviest first onto the lightest.
+    double tot_cost = 0.0;
+    for (int l = 0; l < nlev; ++l) tot_cost += (double)(dl[l].nbins + dl[l].wmax) * (1 + 2 * dl[l].nw);
+    const double target = tot_cost / 8.0;
+    int nu = 0;
+    struct UC { int lev, p0, nst; double c; } uc[kMaxUnits];
+    for (int l = 0; l < nlev; ++l) {
+        const double c = (double)(dl[l].nbins + dl[l].wmax) * (1 + 2 * dl[l].nw);
+        int nseg = (int)(c / target + 0.5);
+        nseg = nseg < 1 ? 1 : nseg;
+        while (nseg > 1 && dl[l].nbins / nseg < 8) --nseg;
+        if (nu + nseg > kMaxUnits) nseg = 1;
+        if (nu + nseg > kMaxUnits) return -4;
+        t.lev[l].nunits = nseg;
+        for (int sgi = 0; sgi < nseg; ++sgi) {
+            // segment boundaries on multiples of 8 columns
+            const int p0 = (int)(((int64_t)dl[l].nbins * sgi / nseg) / 8 * 8);
+            const int p1 = sgi + 1 == nseg ? dl[l].nbins : (int)(((int64_t)dl[l].nbins * (sgi + 1) / nseg) / 8 * 8);
+            uc[nu++] = {l, p0, p1 - p0, (double)(p1 - p0 + dl[l].wmax) * (1 + 2 * dl[l].nw)};
+        }
+    }
+    double load[4] = {0.0, 0.0, 0.0, 0.0};
+    bool used[kMaxUnits] = {false};
+    t.nunit = nu;
+    for (int k = 0; k < nu; ++k) {
+        int best = -1;
+        for (int i = 0; i < nu; ++i)
+            if (!used[i] && (best < 0 || uc[i].c > uc[best].c)) best = i;
+        used[best] = true;
+        int g = 0;
+        for (int q = 1; q < 4; ++q) if (load[q] < load[g]) g = q;
+        load[g] += uc[best].c;
+        TcUnit& U = t.unit[best];
+        U.lev = (int16_t)uc[best].lev;
+        U.wg = (int16_t)g;
+        U.nstart = (int16_t)uc[best].nst;
+        U.pw = (int16_t)((uc[best].nst + dl[uc[best].lev].wmax + t.hm - 1) / t.hm * t.hm);
+        U.col = (int16_t)(t.lev[uc[best].lev].col + uc[best].p0);
+        U.pad = 0;
+        if (U.col + U.pw > 512) return -3;
+    }
+    t.ncols_total = total;
+    t.n1 = total > 256 ? 256 : total;
+    out->B.assign((size_t)total * kK, 0);
+    for (int l = 0; l < nlev; ++l) {
+        const DevLevel& d = dl[l];
+        const TcLevel& L = t.lev[l];
+        for (int c = 0; c < L.ncol; ++c) {
+            const int nbin = c % d.nbins;
+            const int n = L.col + c;
+            for (int jh = 1; jh <= d.Hk; ++jh) {
+                const int h = jh * d.k;          // base harmonic
+                double cre, cim;
+                if (jh < d.Hk) {
+                    const double ang = 2.0 * M_PI * (double)(((int64_t)jh * nbin) % d.nbins) / (double)d.nbins;
+                    cre = 2.0 * std::cos(ang);
+                    cim = -2.0 * std::sin(ang);
+                } else {
+                    cre = (nbin & 1) ? -1.0 : 1.0;   // Nyquist term: real part only
+                    cim = 0.0;
+                }
+                for (int part = 0; part < 2; ++part) {
+                    const int k = 2 * (h - 1) + part;
+                    const size_t off = ((size_t)(n >> 3) * kSBO + (size_t)(k >> 3) * 128 + (n & 7) * 16 +
+                                        (k & 7) * 2) / 2;
+                    out->B[off] = to_half_bits((float)(part ? cim : cre), fp16);
+                }
+            }
+        }
+    }
+    out->smem = (size_t)2 * kABytes + (size_t)total * kK * 2;
+    return 0;
+}
+
+cudaError_t launch_synth_tc(const WaveArgs& a, const TcPlanHost& tp, const void* dB, int* err, cudaStream_t st,
+                            int num_sms) {
+    const int tiles = a.nblk * ((a.Nprof + kTM - 1) / kTM);
+    const int grid = tiles < num_sms ? tiles : num_sms;
+    if (tp.args.hm == 8) {
+        cudaFuncSetAttribute(k_synth_tc<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tp.smem);
+        k_synth_tc<8><<<grid, kEpiThreads, tp.smem, st>>>(a, tp.args, static_cast<const uint4*>(dB), err);
+    } else {
+        cudaFuncSetAttribute(k_synth_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tp.smem);
+        k_synth_tc<32><<<grid, kEpiThreads, tp.smem, st>>>(a, tp.args, static_cast<const uint4*>(dB), err);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace cs

@@ -40,11 +40,13 @@ typedef enum cs_status {
 
 enum { CS_MAX_DECIM = 16 };
 
-/* Profile-synthesis arithmetic on the device. */
+/* Profile-synthesis arithmetic on the device.  It feeds only the
+ * zero-baseline gate; every trial that can reach the threshold is rescored by
+ * the exact FP32 path, so candidates and their S/N are the same in all modes. */
 typedef enum cs_synth {
     CS_SYNTH_FP32 = 0,   /* plain FP32 SIMT synthesis ("plain FP32 GPU form") */
-    CS_SYNTH_BF16 = 1,   /* tcgen05 tensor-core GEMM, BF16 operands, FP32 accumulate */
-    CS_SYNTH_BF16X3 = 2  /* tcgen05 GEMM with split hi+lo BF16 operands (3 products) */
+    CS_SYNTH_BF16 = 1,   /* tcgen05 tensor-core product, BF16 operands, FP32 accumulate */
+    CS_SYNTH_FP16 = 2    /* tcgen05 tensor-core product, FP16 operands, FP32 accumulate */
 } cs_synth;
 
 /* Mirrors SearchParams (src/search.jl:131-144). */
@@ -154,6 +156,18 @@ cs_status cs_interp_chunk(cs_handle* h, double r_lo, int64_t t0, int64_t n, floa
  * counts entries; nlev = number of decimation factors, l in params order. */
 cs_status cs_search_block_values(const cs_handle* h, float* sigma, int32_t* nvalid, int64_t cap,
                                  int64_t* n_out);
+
+/* Diagnostics kept on the host after each cs_search: 0 = none (default),
+ * 1 = per-(block, k) sigma and valid counts, 2 = also every trial's gate
+ * value.  Level 2 copies nblocks*nlev*blocksize floats back per search. */
+cs_status cs_set_diagnostics(cs_handle* h, int32_t level);
+
+/* Zero-baseline gate value of every (block, k, trial) of the last cs_search
+ * run with diagnostics level 2: the `mvals` the reference's batched gate
+ * leaves before the exact rescan (_boxcar_gate!, src/search.jl:784-807),
+ * out[(b * nlev + l) * blocksize + j]; entries past a block's valid trials
+ * are 0. */
+cs_status cs_search_gate_values(const cs_handle* h, float* out, int64_t cap, int64_t* n_out);
 
 /* Per-trial metrics of the last cs_search run with exact_all = 1:
  * out[(b * nlev + l) * blocksize + j]. */

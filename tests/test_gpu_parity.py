@@ -22,6 +22,10 @@ pytestmark = pytest.mark.gpu
 
 SNR_RTOL = 1e-3
 SIGMA_RTOL = 1e-3
+# Tensor-core synthesis feeds only the gate and the sigma samples; its
+# operands carry 8 (BF16) or 11 (FP16) significant bits.
+TC_SIGMA_RTOL = {"bf16": 1e-2, "fp16": 2e-3}
+TC_GATE_TOL = {"bf16": (2e-2, 0.05), "fp16": (4e-3, 0.01)}   # (relative, absolute) on the gate S/N
 
 
 def _cs():
@@ -29,9 +33,10 @@ def _cs():
     return cohsearch
 
 
-def _engine(params, amps, N, dt):
+def _engine(params, amps, N, dt, diag=1):
     cs = _cs()
     eng = cs.Engine(params)
+    eng.set_diagnostics(diag)
     eng.set_spectrum(cs.FFTFile.from_array(amps, N, dt))
     return eng
 
@@ -99,16 +104,18 @@ def _oracle_run(amps, N, dt, op, band, thr, medcut, blocksize=2048):
     return o.search_region(amps, N, T, op, r_lo, r_hi, total, Nprof, thr, medcut, keep_blocks=True)
 
 
+@pytest.mark.parametrize("synth", ["fp32", "bf16", "fp16"])
 @pytest.mark.parametrize("maxdecim,band,blocksize", [(4, (1.0, 60.0), 2048), (6, (20.0, 900.0), 1000)])
-def test_search_vs_oracle(maxdecim, band, blocksize):
+def test_search_vs_oracle(maxdecim, band, blocksize, synth):
     """The hot loop end to end (src/search.jl:1768-1894): nvalid exact, sigma
-    and S/N within tolerance, candidate (trial, k) sets equal outside the band."""
+    and S/N within tolerance, candidate (trial, k) sets equal outside the band,
+    for the plain FP32 and both tensor-core synthesis forms."""
     amps, N, dt = multi_spectrum()
     cs = _cs()
     nh = 32
     thr = 7.0
     dec = cs.decimation_set(nh, maxdecim)
-    eng = _engine(cs.SearchParams(nharms=nh, m=16, decimations=dec, threshold=thr), amps, N, dt)
+    eng = _engine(cs.SearchParams(nharms=nh, m=16, decimations=dec, threshold=thr, synth=synth), amps, N, dt)
     dev = eng.search_raw(band[0], band[1], 100, blocksize, thr)
     sig, nv = eng.block_values()
     op = o.SearchParams(nharms=nh, m=16, decimations=dec, threshold=thr)
@@ -122,7 +129,8 @@ def test_search_vs_oracle(maxdecim, band, blocksize):
         ref_sig[b.block * nlev + levk.index(b.k)] = b.sigma
     assert np.array_equal(nv, ref_nv)
     ok = ref_sig > 0
-    assert np.all(np.abs(sig[ok] - ref_sig[ok]) <= SIGMA_RTOL * ref_sig[ok])
+    srtol = SIGMA_RTOL if synth == "fp32" else TC_SIGMA_RTOL[synth]
+    assert np.all(np.abs(sig[ok] - ref_sig[ok]) <= srtol * ref_sig[ok])
     assert np.all(sig[~ok] == 0)
     dmap = {(int(c["trial"]), int(c["k"])): c for c in dev}
     rmap = {(blk * blocksize + j, k): c for (blk, k, j, c) in ref}
@@ -214,3 +222,38 @@ def test_error_behaviour():
     assert len(eng.search_raw(5.0, 4.0)) == 0          # empty band: no trials
     with pytest.raises(ValueError):
         eng.chunk_metrics(100.0, 0)
+
+
+@pytest.mark.parametrize("synth", ["bf16", "fp16"])
+def test_tensor_gate_tracks_fp32_gate(synth):
+    """The tcgen05 product reproduces the FP32 synthesis' gate values to its
+    operand precision, for every level of a full decimation ladder."""
+    amps, N, dt = multi_spectrum()
+    cs = _cs()
+    dec = cs.decimation_set(60, 6)
+    band = (0.5, 40.0)
+    res = {}
+    for mode in ("fp32", synth):
+        eng = _engine(cs.SearchParams(nharms=60, m=16, decimations=dec, synth=mode), amps, N, dt, diag=2)
+        eng.search_raw(band[0], band[1], 100, 2048, 8.0)
+        res[mode] = (eng.gate_values(), eng.block_values())
+    g32, gtc = res["fp32"][0], res[synth][0]
+    rel, ab = TC_GATE_TOL[synth]
+    assert g32.shape == gtc.shape and np.any(g32 != 0)
+    assert np.all(np.abs(gtc - g32) <= rel * np.abs(g32) + ab)
+
+
+@pytest.mark.parametrize("synth", ["bf16", "fp16"])
+def test_tensor_candidates_identical_to_plain(synth):
+    """Every trial near the threshold is rescored by the same exact FP32 path,
+    so the mixed form reports exactly the plain form's candidates."""
+    amps, N, dt = multi_spectrum()
+    cs = _cs()
+    dec = cs.decimation_set(60, 6)
+    out = {}
+    for mode in ("fp32", synth):
+        eng = _engine(cs.SearchParams(nharms=60, m=16, decimations=dec, synth=mode), amps, N, dt, diag=0)
+        out[mode] = eng.search_raw(0.2, 180.0, 100, 2048, 8.0)
+    a, b = out["fp32"], out[synth]
+    assert len(a) > 0
+    assert np.array_equal(a, b)

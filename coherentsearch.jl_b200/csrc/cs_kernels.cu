@@ -145,21 +145,51 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
         }
     }
     if (!a.samp) return;
-    for (int g = 0; g < ng; ++g) {
+    // Every (harmonic, level) pair whose level folds this harmonic, with its
+    // pooled columns, then all their slots as one flat index space.
+    __shared__ int e_off[kHG * kMaxLevels + 1];
+    __shared__ int e_ncs[kHG * kMaxLevels], e_nv[kHG * kMaxLevels], e_all[kHG * kMaxLevels];
+    __shared__ int e_g[kHG * kMaxLevels];
+    __shared__ long long e_dst[kHG * kMaxLevels];
+    __shared__ int e_cnt;
+    const int npair = ng * a.nlev;
+    if (threadIdx.x < npair) {
+        const int g = threadIdx.x / a.nlev, l = threadIdx.x % a.nlev;
         const int h = hidx0 + g + 1;
-        for (int l = 0; l < a.nlev; ++l) {
-            const DevLevel& L = a.levels[l];
-            if (h % L.k != 0 || h / L.k > L.Hk) continue;
-            const int jh = h / L.k;
-            const int nv = a.nvalid[blk * a.nlev + l];
-            if (nv <= 0) continue;
-            const bool all = (int64_t)L.nbins * nv <= kSigmaCap;
-            const int ncs = all ? nv : min(nv, max(1, kSigmaCap / L.nbins));
-            float2* dst = a.samp + ((int64_t)blk * a.nlev + l) * kSampStride + (int64_t)(jh - 1) * ncs;
-            // sl*nv < 8192*65536 fits 32 bits
-            for (int sl = threadIdx.x; sl < ncs; sl += blockDim.x)
-                dst[sl] = xo[g * Nst + (all ? sl : (int)(((uint32_t)sl * (uint32_t)nv) / (uint32_t)ncs))];
+        const DevLevel& L = a.levels[l];
+        int ncs = 0, nv = 0, all = 0;
+        long long dst = 0;
+        if (h % L.k == 0 && h / L.k <= L.Hk) {
+            nv = a.nvalid[blk * a.nlev + l];
+            if (nv > 0) {
+                all = (int64_t)L.nbins * nv <= kSigmaCap;
+                ncs = all ? nv : min(nv, max(1, kSigmaCap / L.nbins));
+                dst = ((int64_t)blk * a.nlev + l) * kSampStride + (int64_t)(h / L.k - 1) * ncs;
+            }
         }
+        e_ncs[threadIdx.x] = ncs;
+        e_nv[threadIdx.x] = nv;
+        e_all[threadIdx.x] = all;
+        e_g[threadIdx.x] = g;
+        e_dst[threadIdx.x] = dst;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int c = 0;
+        for (int i = 0; i < npair; ++i) { e_off[i] = c; c += e_ncs[i]; }
+        e_off[npair] = c;
+        e_cnt = c;
+    }
+    __syncthreads();
+    const int total = e_cnt;
+    int e = 0;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        while (idx >= e_off[e + 1]) ++e;   // idx only grows, so e only grows
+        const int sl = idx - e_off[e];
+        const int nv = e_nv[e], ncs = e_ncs[e];
+        // sl*nv < 8192*65536 fits 32 bits
+        const int j = e_all[e] ? sl : (int)(((uint32_t)sl * (uint32_t)nv) / (uint32_t)ncs);
+        a.samp[e_dst[e] + sl] = xo[e_g[e] * Nst + j];
     }
 }
 
@@ -213,8 +243,10 @@ __global__ void __launch_bounds__(256) k_interp(WaveArgs a, int win_max, int Nst
     extern __shared__ float2 sm_i[];
     float2* win = sm_i;
     float2* xo = sm_i + win_max;            // [kHG][Nst] staged outputs
-    __shared__ int s_ok, s_nw, s_p0, s_res0, s_Ub, s_chunk, s_Tc, s_small;
-    __shared__ long long s_lo, s_base;      // s_base = rfloor0 + qint0 - lo + 1 - m2
+    // Per-harmonic state of the group, computed by one thread per harmonic.
+    __shared__ int s_ok[kHG], s_nw[kHG], s_p0[kHG], s_res0[kHG], s_Ub[kHG], s_chunk[kHG], s_Tc[kHG],
+        s_small[kHG], s_Hs[kHG];
+    __shared__ long long s_lo[kHG], s_base[kHG];   // s_base = rfloor0 + qint0 - lo + 1 - m2
 
     const int hidx0 = blockIdx.x * kHG;
     const int ng = min(kHG, a.nharms - hidx0);
@@ -225,23 +257,16 @@ __global__ void __launch_bounds__(256) k_interp(WaveArgs a, int win_max, int Nst
     const int n = (int)min((int64_t)a.Nprof, a.total - t0);
     if (n <= 0) return;
 
-    for (int g = 0; g < ng; ++g) {
+    if (threadIdx.x < ng) {
+        // Range guard on the TRUE trial range (src/directinterp.jl:490-496),
+        // with the Julia 1-based bounds translated to 0-based windows.
+        const int g = threadIdx.x;
         const DevHarm hp = a.harms[hidx0 + g];
-        float2* xg = xo + g * Nst;
         if (hp.P == 0) {
-            // Per-trial FP64 fallback for a non-rational trial step
-            // (_fill_row_direct_slow!, src/directinterp.jl:623-661).
-            const bool ok = harm_guard(a, hp, t0, n);
-            for (int j = threadIdx.x; j < n; j += blockDim.x)
-                xg[j] = ok ? exact_amp(a, hp, t0 + j, 0, 0) : make_float2(0.0f, 0.0f);
-            __syncthreads();
-            continue;
-        }
-        const float* __restrict__ wt = a.wtab + hp.w_off;
-        const float2* __restrict__ at = a.atab + hp.a_off;
-        const uint8_t* __restrict__ ct = a.ctab + hp.a_off;
-        const int64_t hpn = (int64_t)hp.h * hp.pnum;
-        if (threadIdx.x == 0) {
+            s_ok[g] = harm_guard(a, hp, t0, n) ? 2 : 0;   // 2: per-trial FP64 path
+        } else {
+            const uint8_t* ct = a.ctab + hp.a_off;
+            const int64_t hpn = (int64_t)hp.h * hp.pnum;
             const int64_t T0 = t0 * hpn;
             const int64_t qint0 = T0 / hp.q;
             const int p0 = (int)(t0 % hp.P);
@@ -254,38 +279,53 @@ __global__ void __launch_bounds__(256) k_interp(WaveArgs a, int win_max, int Nst
                             (hp.rfloor0 + qintl < a.Nhalf);
             const int64_t lo = fl0 + 1 - m2;
             const int64_t nw = fll + m2 - lo + 1;
-            s_ok = ok && nw <= win_max;
+            s_ok[g] = ok && nw <= win_max ? 1 : 0;
             if (ok && nw > win_max) atomicExch(err, 1);
-            s_lo = lo;
-            s_nw = (int)min(nw, (int64_t)win_max);
-            s_p0 = p0;
-            s_res0 = (int)(T0 % hp.q);
-            s_base = hp.rfloor0 + qint0 - lo + 1 - m2;
-            // task split of the phase classes (see below), once per harmonic
+            s_lo[g] = lo;
+            s_nw[g] = (int)min(nw, (int64_t)win_max);
+            s_p0[g] = p0;
+            s_res0[g] = (int)(T0 % hp.q);
+            s_base[g] = hp.rfloor0 + qint0 - lo + 1 - m2;
+            // task split of the phase classes (see below)
             const int P = hp.P;
             const int Tc = P >= (int)blockDim.x ? 1 : (int)blockDim.x / P;
             const int Ub = n / P;                       // classes jc < n - Ub*P get Ub+1 trials
-            s_Ub = Ub;
-            s_Tc = Tc;
-            s_chunk = (Ub + 1 + Tc - 1) / Tc;
+            s_Ub[g] = Ub;
+            s_Tc[g] = Tc;
+            s_chunk[g] = (Ub + 1 + Tc - 1) / Tc;
             // res0 + jc*h*pnum < 2^32 for every class: the window start fits 32-bit math
-            s_small = ((uint64_t)hp.q + (uint64_t)P * (uint64_t)hpn) < 0xFFFFFFFFull;
+            s_small[g] = ((uint64_t)hp.q + (uint64_t)P * (uint64_t)hpn) < 0xFFFFFFFFull;
+            s_Hs[g] = (int)(((int64_t)P * hpn) / hp.q);   // bins between trials t and t+P
         }
-        __syncthreads();
-        if (!s_ok) {
-            for (int j = threadIdx.x; j < n; j += blockDim.x) xg[j] = make_float2(0.0f, 0.0f);
-            __syncthreads();
+    }
+    __syncthreads();
+
+    for (int g = 0; g < ng; ++g) {
+        const DevHarm& hp = a.harms[hidx0 + g];
+        float2* xg = xo + g * Nst;
+        if (s_ok[g] != 1) {
+            // guarded-off row, or the per-trial FP64 fallback for a non-rational
+            // trial step (_fill_row_direct_slow!, src/directinterp.jl:623-661)
+            const bool slow = s_ok[g] == 2;
+            for (int j = threadIdx.x; j < n; j += blockDim.x)
+                xg[j] = slow ? exact_amp(a, hp, t0 + j, 0, 0) : make_float2(0.0f, 0.0f);
             continue;
         }
-        const int nw = s_nw;
-        const float2* __restrict__ src = a.amps + s_lo;
+        const float* __restrict__ wt = a.wtab + hp.w_off;
+        const float2* __restrict__ at = a.atab + hp.a_off;
+        const uint8_t* __restrict__ ct = a.ctab + hp.a_off;
+        const int64_t hpn = (int64_t)hp.h * hp.pnum;
+        const int nw = s_nw[g];
+        const float2* __restrict__ src = a.amps + s_lo[g];
+        __syncthreads();   // the previous harmonic's window reads are done
         for (int i = threadIdx.x; i < nw; i += blockDim.x) win[i] = src[i];
         __syncthreads();
-        const int P = hp.P, q = hp.q;
-        const int Hs = (int)(((int64_t)P * hpn) / q);   // bins between trials t and t+P
+        const int P = hp.P, q = hp.q, Hs = s_Hs[g];
         // Runs: class jc (first trial j = jc, phase (p0 + jc) mod P), part `part`
         // of its u range; classes below n - Ub*P have Ub+1 trials, the rest Ub.
-        const int Tc = s_Tc, Ub = s_Ub, chunk = s_chunk, p0 = s_p0, res0 = s_res0;
+        const int Tc = s_Tc[g], Ub = s_Ub[g], chunk = s_chunk[g], p0 = s_p0[g], res0 = s_res0[g];
+        const int small = s_small[g];
+        const long long base = s_base[g];
         const int ntask = P >= (int)blockDim.x ? P : P * Tc;
         const int nlong = n - Ub * P;
         const float invP = 1.0f / (float)P;
@@ -300,13 +340,13 @@ __global__ void __launch_bounds__(256) k_interp(WaveArgs a, int win_max, int Nst
             if (u0 >= u1) continue;
             int p = p0 + jc;
             if (p >= P) p -= P;
-            const int64_t qv = s_small ? (int64_t)(((uint32_t)res0 + (uint32_t)jc * (uint32_t)hpn) / (uint32_t)q)
-                                       : ((int64_t)res0 + (int64_t)jc * hpn) / q;
-            const int b0 = (int)(s_base + qv + ct[p]);
+            const int64_t qv = small ? (int64_t)(((uint32_t)res0 + (uint32_t)jc * (uint32_t)hpn) / (uint32_t)q)
+                                     : ((int64_t)res0 + (int64_t)jc * hpn) / q;
+            const int b0 = (int)(base + qv + ct[p]);
             class_run<M>(wt, P, p, __ldg(at + p), win, b0, Hs, jc, u0, u1, xg, m);
         }
-        __syncthreads();
     }
+    __syncthreads();
     emit_rows(a, xo, Nst, blk, hidx0, ng, n);
 }
 

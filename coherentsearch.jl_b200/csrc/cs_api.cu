@@ -11,7 +11,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdarg>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -857,3 +859,207 @@ cs_status cs_search_trial_metrics(const cs_handle* H, float* out, int64_t cap, i
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Chunk metrics without device allocation (cs_chunk_metrics_static).
+//
+// Some callers are not allowed to call cudaMalloc or cudaFree: a plugin loaded
+// into a host pipeline that reserved the device memory for itself at start-up
+// and hands out only fixed buffers, or a runtime whose own pooling allocator
+// must see every allocation.  cudaFree also synchronises the device, which a
+// latency-bound caller cannot afford.  For them the chunk-metrics path keeps
+// its scratch -- counters, the level and plan tables and the sigma samples --
+// in one file-scope device array of fixed size.
+// The caller passes its spectrum and the output as device pointers.
+
+namespace {
+constexpr size_t kStaticScratchBytes = (size_t)4 << 20;  // 4 MiB on every device
+constexpr int kStaticMaxDevices = 64;
+}  // namespace
+
+// Loaded with the library on every GPU it is used on and held until the
+// process exits.  In host code this name is a stand-in for the symbol, not a
+// device address: the address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+namespace {
+
+std::mutex g_static_mu[kStaticMaxDevices];
+void* g_static_base[kStaticMaxDevices];  // device address of g_static_scratch, per device
+
+cs_status static_fail(char* err, int64_t cap, cs_status st, const char* fmt, ...) {
+    if (err && cap > 0) {
+        va_list ap;
+        va_start(ap, fmt);
+        std::vsnprintf(err, (size_t)cap, fmt, ap);
+        va_end(ap);
+    }
+    return st;
+}
+
+size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" cs_status cs_chunk_metrics_static(const cs_params* params, const float* d_amps, int64_t namps,
+                                             int64_t N, double rstart, int64_t n, float* d_out, void* stream,
+                                             char* err, int64_t err_cap) {
+    if (err && err_cap > 0) err[0] = '\0';
+    if (validate(params) != CS_OK)
+        return static_fail(err, err_cap, CS_ERR_INVALID_ARGUMENT, "invalid search parameters");
+    if (!d_amps || !d_out || namps < 1 || N < 2 || n < 1 || n > (1 << 16))
+        return static_fail(err, err_cap, CS_ERR_INVALID_ARGUMENT,
+                           "needs device spectrum and output, namps >= 1, N >= 2 and 1 <= n <= 65536");
+    if ((reinterpret_cast<uintptr_t>(d_amps) & 7u) != 0 || (reinterpret_cast<uintptr_t>(d_out) & 3u) != 0)
+        return static_fail(err, err_cap, CS_ERR_INVALID_ARGUMENT,
+                           "spectrum must be 8-byte and output 4-byte aligned");
+    const cs_params& p = *params;
+
+    // The base fold (k = 1) only, as cs_chunk_metrics evaluates it.
+    DevLevel L{};
+    L.k = 1;
+    L.Hk = p.nharms;
+    L.nbins = 2 * p.nharms;
+    const std::vector<int> widths = ladder_widths(L.nbins, 1, p);
+    if (L.nbins > kMaxBins || (int)widths.size() > kMaxWidths || widths.back() > kMaxBins)
+        return static_fail(err, err_cap, CS_ERR_UNSUPPORTED,
+                           "needs nharms <= 128, <= 64 boxcar widths, widths <= 256 bins");
+    L.nw = (int)widths.size();
+    L.wmax = widths.back();
+    L.np = ((L.Hk + 1) + 7) / 8 * 8;
+    L.tw_off = 0;
+    for (int i = 0; i < L.nw; ++i) {
+        L.widths[i] = widths[i];
+        L.rsqrtw[i] = (float)(1.0 / std::sqrt((double)widths[i]));
+    }
+    std::vector<float> tw(2 * (size_t)L.Hk * L.np, 0.0f);
+    for (int j = 1; j < L.Hk; ++j)
+        for (int k = 0; k <= L.Hk; ++k) {
+            const double ang = 2.0 * M_PI * (double)(((int64_t)j * k) % L.nbins) / (double)L.nbins;
+            tw[(size_t)j * L.np + k] = (float)(2.0 * std::cos(ang));
+            tw[((size_t)L.Hk + j) * L.np + k] = (float)(-2.0 * std::sin(ang));
+        }
+    HostPlans plans;
+    build_plans(p, rstart, plans);
+    for (const DevHarm& d : plans.harms)
+        if ((double)n * (double)d.h * (double)d.pnum > 4.6e18)
+            return static_fail(err, err_cap, CS_ERR_UNSUPPORTED,
+                               "trial index times harmonic overflows 64-bit phase state");
+    const int Nprof = (int)n;
+    const int win_max = (int)std::ceil((double)(Nprof - 1 + 64) * p.hidr) + p.m + 4;
+    if (interp_smem(win_max, Nprof) > 200 * 1024)
+        return static_fail(err, err_cap, CS_ERR_UNSUPPORTED,
+                           "chunk too long for the shared-memory interpolation row");
+    if (sigma_smem(L.Hk, L.np) + 16 * 1024 > 227 * 1024)
+        return static_fail(err, err_cap, CS_ERR_UNSUPPORTED, "sigma working set exceeds shared memory");
+
+    // Scratch layout, every piece on a 256-byte boundary.
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = up256(off + bytes);
+        return o;
+    };
+    const size_t o_cnt = take(4 * sizeof(int32_t));
+    const size_t o_lev = take(sizeof(DevLevel));
+    const size_t o_tw = take(tw.size() * sizeof(float));
+    const size_t o_harms = take(plans.harms.size() * sizeof(DevHarm));
+    const size_t o_w = take(plans.w.size() * sizeof(float));
+    const size_t o_a = take(plans.a.size() * sizeof(float2));
+    const size_t o_c = take(plans.c.size());
+    const size_t o_nv = take(sizeof(int32_t));
+    const size_t o_sig = take(sizeof(float));
+    const size_t o_samp = take((size_t)kSampStride * sizeof(float2));
+    if (off > kStaticScratchBytes)
+        return static_fail(err, err_cap, CS_ERR_CAPACITY,
+                           "plan tables need %zu bytes of scratch; the static scratch holds %zu (4 MiB): "
+                           "lower nharms or m, or use a trial grid with a smaller denominator",
+                           off, kStaticScratchBytes);
+
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return static_fail(err, err_cap, CS_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kStaticMaxDevices)
+        return static_fail(err, err_cap, CS_ERR_UNSUPPORTED, "device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_static_mu[dev]);
+    if (!g_static_base[dev]) {
+        // Once per device, with that device current.
+        void* ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (e != cudaSuccess || !ptr)
+            return static_fail(err, err_cap, CS_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        g_static_base[dev] = ptr;
+    }
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
+    uint8_t* base = static_cast<uint8_t*>(g_static_base[dev]);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int32_t nvalid = Nprof;
+#define CS_STATIC_CUDA(call, where)                                                                  \
+    do {                                                                                             \
+        const cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                       \
+            return static_fail(err, err_cap, CS_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e_)); \
+    } while (0)
+    auto put = [&](size_t o, const void* src, size_t bytes) {
+        return bytes ? cudaMemcpyAsync(base + o, src, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
+    };
+    // The counters must start at zero; every other region is fully rewritten.
+    CS_STATIC_CUDA(cudaMemsetAsync(base + o_cnt, 0, 4 * sizeof(int32_t), st), "clear counters");
+    CS_STATIC_CUDA(put(o_lev, &L, sizeof(DevLevel)), "copy level");
+    CS_STATIC_CUDA(put(o_tw, tw.data(), tw.size() * sizeof(float)), "copy twiddles");
+    CS_STATIC_CUDA(put(o_harms, plans.harms.data(), plans.harms.size() * sizeof(DevHarm)), "copy plans");
+    CS_STATIC_CUDA(put(o_w, plans.w.data(), plans.w.size() * sizeof(float)), "copy weights");
+    CS_STATIC_CUDA(put(o_a, plans.a.data(), plans.a.size() * sizeof(float2)), "copy phases");
+    CS_STATIC_CUDA(put(o_c, plans.c.data(), plans.c.size()), "copy carries");
+    CS_STATIC_CUDA(put(o_nv, &nvalid, sizeof(int32_t)), "copy valid count");
+
+    int32_t* cnt = reinterpret_cast<int32_t*>(base + o_cnt);
+    WaveArgs a{};
+    a.amps = reinterpret_cast<const float2*>(d_amps);
+    a.namps = namps;
+    a.Nhalf = N / 2;
+    a.nharms = p.nharms;
+    a.m = p.m;
+    a.nlev = 1;
+    a.Nprof = Nprof;
+    a.t_first = 0;
+    a.total = n;
+    a.nblk = 1;
+    a.blk_base = 0;
+    a.harms = reinterpret_cast<const DevHarm*>(base + o_harms);
+    a.wtab = reinterpret_cast<const float*>(base + o_w);
+    a.atab = reinterpret_cast<const float2*>(base + o_a);
+    a.ctab = base + o_c;
+    a.levels = reinterpret_cast<const DevLevel*>(base + o_lev);
+    a.tw = reinterpret_cast<const float*>(base + o_tw);
+    a.nvalid = reinterpret_cast<int32_t*>(base + o_nv);
+    a.X = nullptr;  // the amplitude rows are not kept: sigma reads the samples,
+    a.Atile = nullptr;  // the metric kernel recomputes each trial's amplitudes
+    a.tiles_per_blk = (Nprof + 127) / 128;
+    a.fp16 = 0;
+    a.samp = reinterpret_cast<float2*>(base + o_samp);
+    a.Q0 = nullptr;  // no gate: every trial gets the exact metric
+    a.sigma = reinterpret_cast<float*>(base + o_sig);
+    a.tmetric = d_out;
+    a.items = nullptr;
+    a.n_items = cnt;
+    a.cap_items = 0;
+    a.cands = nullptr;
+    a.n_cands = cnt + 1;
+    a.cap_cands = 0;
+    a.threshold = INFINITY;
+    a.medcut = -INFINITY;
+    a.medcut_gate = -INFINITY;
+    a.verify_gate = 0;
+    a.exact_all = 1;
+    CS_STATIC_CUDA(launch_interp(a, st, win_max, cnt + 2), "interp launch");
+    CS_STATIC_CUDA(launch_sigma(a, st, L.Hk, L.np), "sigma launch");
+    CS_STATIC_CUDA(launch_rescue(a, st, sms), "metric launch");
+    int32_t counts[4] = {0, 0, 0, 0};
+    CS_STATIC_CUDA(cudaMemcpyAsync(counts, cnt, sizeof(counts), cudaMemcpyDeviceToHost, st), "read counters");
+    CS_STATIC_CUDA(cudaStreamSynchronize(st), "chunk");
+#undef CS_STATIC_CUDA
+    if (counts[2] == 1) return static_fail(err, err_cap, CS_ERR_CUDA, "interpolation window exceeded its bound");
+    return CS_OK;
+}

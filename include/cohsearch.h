@@ -144,6 +144,34 @@ cs_status cs_search_stats(const cs_handle* h, cs_stats* out);
  * at rstart, base fold only), written to out[0..n). */
 cs_status cs_chunk_metrics(cs_handle* h, double rstart, int64_t n, double* out);
 
+/* cs_chunk_metrics for callers that may not allocate device memory.  It has
+ * no counterpart in the reference: it exists for code that runs inside a host
+ * that owns the device memory budget (a pipeline that reserved HBM at start-up
+ * and hands out fixed buffers, a runtime whose pool allocator must see every
+ * allocation) or that cannot pay the device-wide synchronisation of cudaFree.
+ * It creates no handle and calls no cudaMalloc, cudaFree or allocating
+ * library routine.  Its scratch (counters, plan tables, sigma samples) lives
+ * in a 4 MiB array inside the library that every GPU using the library holds
+ * until the process exits; a request whose plan tables need more returns
+ * CS_ERR_CAPACITY with the sizes in `err`.
+ *
+ * Inputs and output are device memory on the current device: d_amps holds
+ * namps complex64 amplitudes of an N-sample series (8-byte aligned), d_out
+ * receives the n float32 metrics that cs_chunk_metrics returns as doubles
+ * (trials rstart + j*lodr, base fold), 1 <= n <= 65536.  Work runs on
+ * `stream` (NULL = legacy default stream) and the call returns once it has
+ * finished.  `err` (may be NULL) receives a message of at most err_cap bytes.
+ *
+ * The first call on a device looks up the array's device address there
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls on a device share the array and it keeps the last call's
+ * contents; the counters are cleared on every call.  Calls whose GPU work
+ * overlapped would race on it: the library serialises its own calls per
+ * device with a lock and returns only after its work is done. */
+cs_status cs_chunk_metrics_static(const cs_params* params, const float* d_amps, int64_t namps, int64_t N,
+                                  double rstart, int64_t n, float* d_out, void* stream, char* err,
+                                  int64_t err_cap);
+
 /* Interpolated amplitude stack of a chunk (the `ftprofs` rows of
  * fill_chunk_profiles!, src/search.jl:1280-1290, and fill_harmonic_row_direct!,
  * src/directinterp.jl:470-572): trials t0 .. t0+n-1 of a search whose global

@@ -416,6 +416,41 @@ __device__ __forceinline__ void synth_chunk8(const float2* __restrict__ xs, int 
     for (int u = 0; u < 8; ++u) E[u] = E[u] + (((n0 + u) & 1) ? -ny : ny);
 }
 
+// synth_chunk8 for two columns sharing each twiddle load; per output the same
+// sequential FMA chain, hence the same values.
+__device__ __forceinline__ void synth_chunk8x2(const float2* __restrict__ xa, const float2* __restrict__ xb,
+                                               int xstride, const float* __restrict__ C2,
+                                               const float* __restrict__ S2, int np, int Hk, int n0,
+                                               float Ea[8], float Oa[8], float Eb[8], float Ob[8]) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) { Ea[u] = 0.0f; Oa[u] = 0.0f; Eb[u] = 0.0f; Ob[u] = 0.0f; }
+#pragma unroll 2
+    for (int jh = 1; jh < Hk; ++jh) {
+        const float2 x = xa[(jh - 1) * xstride];
+        const float2 y = xb[(jh - 1) * xstride];
+        const float4 c0 = __ldg(reinterpret_cast<const float4*>(C2 + jh * np + n0));
+        const float4 c1 = __ldg(reinterpret_cast<const float4*>(C2 + jh * np + n0 + 4));
+        const float4 s0 = __ldg(reinterpret_cast<const float4*>(S2 + jh * np + n0));
+        const float4 s1 = __ldg(reinterpret_cast<const float4*>(S2 + jh * np + n0 + 4));
+        const float c[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+        const float sv[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            Ea[u] = fmaf(x.x, c[u], Ea[u]);
+            Oa[u] = fmaf(x.y, sv[u], Oa[u]);
+            Eb[u] = fmaf(y.x, c[u], Eb[u]);
+            Ob[u] = fmaf(y.y, sv[u], Ob[u]);
+        }
+    }
+    const float nya = xa[(Hk - 1) * xstride].x;
+    const float nyb = xb[(Hk - 1) * xstride].x;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        Ea[u] = Ea[u] + (((n0 + u) & 1) ? -nya : nya);
+        Eb[u] = Eb[u] + (((n0 + u) & 1) ? -nyb : nyb);
+    }
+}
+
 __global__ void __launch_bounds__(2 * kTileTrials) k_synth_fp32(WaveArgs a) {
     constexpr int TT = kTileTrials;
     extern __shared__ float4 smem4[];
@@ -578,7 +613,6 @@ __device__ uint32_t radix_select(const uint32_t* vals, int ns, int kth, uint32_t
 // synthesis mode.  sigma = 1.4826 * median(|x|), _median! semantics.
 __global__ void __launch_bounds__(256) k_sigma(WaveArgs a) {
     extern __shared__ float4 ss4[];
-    __shared__ uint32_t hist[2048];
     __shared__ int sh[4];
     __shared__ int wtot[32];
     __shared__ uint32_t red[8];
@@ -594,26 +628,36 @@ __global__ void __launch_bounds__(256) k_sigma(WaveArgs a) {
     const bool all = (int64_t)nbins * nv <= kSigmaCap;
     const int ncs = all ? nv : min(nv, max(1, kSigmaCap / nbins));
     const int ns = ncs * nbins;
-    float* tws = reinterpret_cast<float*>(ss4);                 // C2 then S2: 2*Hk*np
-    float2* Xs = reinterpret_cast<float2*>(tws + 2 * Hk * np);  // [Hk][ncs]
-    uint32_t* vals = reinterpret_cast<uint32_t*>(Xs + kSigmaCap / 2);  // [ns]
-    const float4* tsrc = reinterpret_cast<const float4*>(a.tw + L.tw_off);
-    for (int i = threadIdx.x; i < 2 * Hk * np / 4; i += blockDim.x) ss4[i] = tsrc[i];
+    float2* Xs = reinterpret_cast<float2*>(ss4);                    // [Hk][ncs], <= kSampStride
+    uint32_t* hist = reinterpret_cast<uint32_t*>(ss4);              // reuses Xs once profiles exist
+    uint32_t* vals = reinterpret_cast<uint32_t*>(Xs + kSampStride);  // [ns]
+    const float* C2 = a.tw + L.tw_off;
+    const float* S2 = C2 + (int64_t)Hk * np;
     const float2* samp = a.samp + (int64_t)bl * kSampStride;
     for (int idx = threadIdx.x; idx < Hk * ncs; idx += blockDim.x) Xs[idx] = samp[idx];
     __syncthreads();
+    // Two columns per thread share each twiddle load (read through L1).
     const int nch = (Hk + 1 + 7) / 8;
-    for (int idx = threadIdx.x; idx < ncs * nch; idx += blockDim.x) {
-        const int sl = idx % ncs, ch = idx / ncs;
+    const int npairs = (ncs + 1) / 2;
+    for (int idx = threadIdx.x; idx < npairs * nch; idx += blockDim.x) {
+        const int pr = idx % npairs, ch = idx / npairs;
+        const int sa = 2 * pr, sb = min(2 * pr + 1, ncs - 1);
         const int n0 = ch * 8;
-        float E[8], O[8];
-        synth_chunk8(Xs + sl, ncs, tws, tws + Hk * np, np, 1, Hk, n0, E, O);
-        uint32_t* dst = vals + sl * nbins;
+        float Ea[8], Oa[8], Eb[8], Ob[8];
+        synth_chunk8x2(Xs + sa, Xs + sb, ncs, C2, S2, np, Hk, n0, Ea, Oa, Eb, Ob);
+        uint32_t* da = vals + sa * nbins;
+        uint32_t* db = vals + sb * nbins;
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const int nn = n0 + u;
-            if (nn <= Hk) dst[nn] = __float_as_uint(fabsf(E[u] + O[u]));
-            if (nn >= 1 && nn < Hk) dst[2 * Hk - nn] = __float_as_uint(fabsf(E[u] - O[u]));
+            if (nn <= Hk) {
+                da[nn] = __float_as_uint(fabsf(Ea[u] + Oa[u]));
+                db[nn] = __float_as_uint(fabsf(Eb[u] + Ob[u]));
+            }
+            if (nn >= 1 && nn < Hk) {
+                da[2 * Hk - nn] = __float_as_uint(fabsf(Ea[u] - Oa[u]));
+                db[2 * Hk - nn] = __float_as_uint(fabsf(Eb[u] - Ob[u]));
+            }
         }
     }
     __syncthreads();
@@ -652,8 +696,9 @@ __global__ void __launch_bounds__(256) k_sigma(WaveArgs a) {
 }
 
 size_t sigma_smem(int max_hk, int max_np) {
-    return (size_t)2 * max_hk * max_np * sizeof(float) + (size_t)(kSigmaCap / 2) * sizeof(float2) +
-           (size_t)kSigmaCap * sizeof(uint32_t);
+    (void)max_hk;
+    (void)max_np;
+    return (size_t)kSampStride * sizeof(float2) + (size_t)kSigmaCap * sizeof(uint32_t);
 }
 
 cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np) {

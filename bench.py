@@ -22,10 +22,10 @@ reference's search (the C port, all host threads) on a bounded sample of the
 same workload.
 """
 import argparse
+import gc
 import json
 import math
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -51,58 +51,71 @@ def workload_config(synth_mode):
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    """SM clock, power and clock-event reasons of this process's GPU, polled
+    through NVML every 5 ms while the timed region runs (nvidia-smi's 100 ms
+    loop would see a few samples of a sub-second region at most)."""
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, cuda_index):
+        self.cuda_index = cuda_index
+        self.samples = []
+        self.stop = threading.Event()
+        self.thread = None
+        self.max_mhz = None
+        self.nvml = None
+
+    def _handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            pr = torch.cuda.get_device_properties(self.cuda_index)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
+
+    def _poll(self, nv, h):
+        masks = [(n, getattr(nv, c)) for n, c in self.REASONS]
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), [n for n, m in masks if rs & m]))
+            except Exception:
+                pass
+            time.sleep(0.005)
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            nv, h = self._handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.nvml = nv
+            self.thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
             self.thread.start()
         except Exception:
-            self.proc = None
+            self.thread = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
+        self.stop.set()
+        if self.thread:
+            self.thread.join(timeout=5)
+        if self.nvml:
             try:
-                self.proc.wait(timeout=5)
+                self.nvml.nvmlShutdown()
             except Exception:
-                self.proc.kill()
+                pass
 
     def summary(self):
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 7:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx.append(float(parts[1]))
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[3:7]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0, "source": "nvml"}
+        reasons = sorted({r for _, rs in self.samples for r in rs})
+        return {"sm_mhz": float(np.median([s for s, _ in self.samples])), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples), "source": "nvml, 5 ms poll"}
 
 
 # ---------------------------------------------------------------------------
@@ -193,11 +206,13 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
+    gc.disable()   # no collector pauses inside the timed regions
     with ClockSampler(local_rank) as clk:
         ms, stage, launches, _, _, ncand = timed(step_device, args.steps)
         torch.cuda.synchronize()
     ms_e2e, _, _, h2d, d2h, _ = timed(step_e2e, args.steps)
     torch.cuda.synchronize()
+    gc.enable()
     plain = None
     if args.synth != "fp32" and not args.no_plain:
         # the plain FP32 GPU form on the same data, for the mixed-vs-plain comparison

@@ -218,6 +218,11 @@ struct cs_handle {
     DBuf d_A, d_samp;
     DBuf d_levels, d_tw, d_harms, d_wtab, d_atab, d_ctab, d_nvalid, d_X, d_Q0, d_sigma,
         d_tmetric, d_items, d_counts, d_cands;
+    // FP64 plan tables of the last anchor r_lo, already on the device
+    bool plan_valid = false;
+    double plan_rlo = 0.0;
+    HostPlans plans;
+    int64_t plan_bytes = 0;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     cs_stats stats{};
     std::vector<float> last_sigma;
@@ -365,19 +370,28 @@ struct RunSpec {
 
 cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands, float2* x_out) {
     const cs_params& p = H->p;
-    HostPlans plans;
-    build_plans(p, R.r_lo, plans);
-    for (const DevHarm& d : plans.harms) {
+    // The tables depend on r_lo only (params are fixed per handle): a search
+    // repeated on the same band, the common case of a pipeline over many
+    // spectra, reuses the device copies.
+    int64_t plan_bytes = 0;
+    if (!H->plan_valid || H->plan_rlo != R.r_lo) {
+        H->plan_valid = false;
+        build_plans(p, R.r_lo, H->plans);
+        const HostPlans& plans = H->plans;
+        CS_CUDA(upload(H->d_harms, plans.harms, H->stream), "upload plans");
+        CS_CUDA(upload(H->d_wtab, plans.w, H->stream), "upload weights");
+        CS_CUDA(upload(H->d_atab, plans.a, H->stream), "upload phases");
+        CS_CUDA(upload(H->d_ctab, plans.c, H->stream), "upload carries");
+        plan_bytes = (int64_t)(plans.harms.size() * sizeof(DevHarm) + plans.w.size() * sizeof(float) +
+                               plans.a.size() * sizeof(float2) + plans.c.size());
+        H->plan_valid = true;
+        H->plan_rlo = R.r_lo;
+    }
+    for (const DevHarm& d : H->plans.harms) {
         const double lim = 4.6e18;
         if ((double)R.t_end * (double)d.h * (double)d.pnum > lim)
             return fail(H, CS_ERR_UNSUPPORTED, "trial index times harmonic overflows 64-bit phase state");
     }
-    CS_CUDA(upload(H->d_harms, plans.harms, H->stream), "upload plans");
-    CS_CUDA(upload(H->d_wtab, plans.w, H->stream), "upload weights");
-    CS_CUDA(upload(H->d_atab, plans.a, H->stream), "upload phases");
-    CS_CUDA(upload(H->d_ctab, plans.c, H->stream), "upload carries");
-    const int64_t plan_bytes = (int64_t)(plans.harms.size() * sizeof(DevHarm) + plans.w.size() * sizeof(float) +
-                                         plans.a.size() * sizeof(float2) + plans.c.size());
 
     const int Nprof = R.Nprof;
     const int win_max = (int)std::ceil((double)(Nprof - 1 + 64) * p.hidr) + p.m + 4;
@@ -407,7 +421,18 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
                            (size_t)nlev * kSampStride * sizeof(float2) +
                            (size_t)nlev * Nprof * sizeof(float) * (R.exact_all ? 2 : 1) +
                            (size_t)nlev * Nprof * (sizeof(DevItem) + sizeof(DevCand)) + 64;
-    const size_t budget = (size_t)3 << 30;
+    // Working set of one wave: up to 8 GiB, and at most half of the free
+    // device memory (a full survey band is one wave on a 180 GB part).
+    size_t budget = (size_t)8 << 30;
+    {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+            // memory this handle already holds for waves counts as free
+            const size_t held = H->d_X.bytes + H->d_A.bytes + H->d_samp.bytes + H->d_Q0.bytes +
+                                H->d_items.bytes + H->d_cands.bytes + H->d_tmetric.bytes;
+            budget = std::min(budget, std::max<size_t>((size_t)512 << 20, (free_b + held) / 2));
+        }
+    }
     const int64_t WB = std::max<int64_t>(1, std::min<int64_t>(R.nblocks, (int64_t)(budget / per_blk)));
 
     if (want_x) CS_CUDA(H->d_X.ensure((size_t)WB * p.nharms * Nprof * sizeof(float2)), "alloc X");

@@ -126,70 +126,59 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
         // A tile (block, j/128), row r = j%128, K chunk hidx0/4 holds (Re, Im) of
         // the 4 harmonics: SWIZZLE_NONE K-major core-matrix layout.
         uint8_t* base = a.Atile + (int64_t)blk * a.tiles_per_blk * kATileBytes + (hidx0 >> 2) * 128;
+        const float2* x1 = xo + Nst;
+        const float2* x2 = xo + 2 * Nst;
+        const float2* x3 = xo + 3 * Nst;
+        const float2 z = make_float2(0.0f, 0.0f);
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
-            uint32_t v[kHG];
-#pragma unroll
-            for (int g = 0; g < kHG; ++g) {
-                const float2 x = g < ng ? xo[g * Nst + j] : make_float2(0.0f, 0.0f);
-                if (a.fp16) {
-                    __half2 hv = __floats2half2_rn(x.x, x.y);
-                    v[g] = *reinterpret_cast<uint32_t*>(&hv);
-                } else {
-                    __nv_bfloat162 bv = __floats2bfloat162_rn(x.x, x.y);
-                    v[g] = *reinterpret_cast<uint32_t*>(&bv);
-                }
+            const float2 v0 = xo[j];
+            const float2 v1 = ng > 1 ? x1[j] : z;
+            const float2 v2 = ng > 2 ? x2[j] : z;
+            const float2 v3 = ng > 3 ? x3[j] : z;
+            uint4 pk;
+            if (a.fp16) {
+                __half2 h0 = __floats2half2_rn(v0.x, v0.y), h1 = __floats2half2_rn(v1.x, v1.y);
+                __half2 h2 = __floats2half2_rn(v2.x, v2.y), h3 = __floats2half2_rn(v3.x, v3.y);
+                pk = make_uint4(*reinterpret_cast<uint32_t*>(&h0), *reinterpret_cast<uint32_t*>(&h1),
+                                *reinterpret_cast<uint32_t*>(&h2), *reinterpret_cast<uint32_t*>(&h3));
+            } else {
+                __nv_bfloat162 h0 = __floats2bfloat162_rn(v0.x, v0.y), h1 = __floats2bfloat162_rn(v1.x, v1.y);
+                __nv_bfloat162 h2 = __floats2bfloat162_rn(v2.x, v2.y), h3 = __floats2bfloat162_rn(v3.x, v3.y);
+                pk = make_uint4(*reinterpret_cast<uint32_t*>(&h0), *reinterpret_cast<uint32_t*>(&h1),
+                                *reinterpret_cast<uint32_t*>(&h2), *reinterpret_cast<uint32_t*>(&h3));
             }
-            const int r = j & 127;
-            *reinterpret_cast<uint4*>(base + (int64_t)(j >> 7) * kATileBytes + (r >> 3) * 2048 + (r & 7) * 16) =
-                make_uint4(v[0], v[1], v[2], v[3]);
+            const uint32_t off = (uint32_t)(j >> 7) * (uint32_t)kATileBytes + ((uint32_t)(j & 127) >> 3) * 2048u +
+                                 (uint32_t)(j & 7) * 16u;
+            *reinterpret_cast<uint4*>(base + off) = pk;
         }
     }
     if (!a.samp) return;
-    // Every (harmonic, level) pair whose level folds this harmonic, with its
-    // pooled columns, then all their slots as one flat index space.
-    __shared__ int e_off[kHG * kMaxLevels + 1];
-    __shared__ int e_ncs[kHG * kMaxLevels], e_nv[kHG * kMaxLevels], e_all[kHG * kMaxLevels];
-    __shared__ int e_g[kHG * kMaxLevels];
-    __shared__ long long e_dst[kHG * kMaxLevels];
-    __shared__ int e_cnt;
-    const int npair = ng * a.nlev;
-    if (threadIdx.x < npair) {
-        const int g = threadIdx.x / a.nlev, l = threadIdx.x % a.nlev;
+    // One warp per (harmonic, level) pair whose level folds this harmonic;
+    // lanes over its pooled columns j_c = (c*nv) div ncs (src/search.jl:528-537),
+    // the division by ncs done as a multiply-high by ceil(2^64/ncs), exact for
+    // every 32-bit dividend.
+    const int lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    for (int e = threadIdx.x >> 5; e < ng * a.nlev; e += nwarps) {
+        const int g = e / a.nlev, l = e - g * a.nlev;
         const int h = hidx0 + g + 1;
         const DevLevel& L = a.levels[l];
-        int ncs = 0, nv = 0, all = 0;
-        long long dst = 0;
-        if (h % L.k == 0 && h / L.k <= L.Hk) {
-            nv = a.nvalid[blk * a.nlev + l];
-            if (nv > 0) {
-                all = (int64_t)L.nbins * nv <= kSigmaCap;
-                ncs = all ? nv : min(nv, max(1, kSigmaCap / L.nbins));
-                dst = ((int64_t)blk * a.nlev + l) * kSampStride + (int64_t)(h / L.k - 1) * ncs;
+        if (h % L.k != 0 || h / L.k > L.Hk) continue;
+        const int nv = a.nvalid[blk * a.nlev + l];
+        if (nv <= 0) continue;
+        const bool all = (int64_t)L.nbins * nv <= kSigmaCap;
+        const int ncs = all ? nv : min(nv, max(1, kSigmaCap / L.nbins));
+        float2* dst = a.samp + ((int64_t)blk * a.nlev + l) * kSampStride + (int64_t)(h / L.k - 1) * ncs;
+        const float2* src = xo + g * Nst;
+        if (all || ncs == 1) {
+            for (int c = lane; c < ncs; c += 32) dst[c] = src[all ? c : 0];
+        } else {
+            const uint64_t mg = 0xFFFFFFFFFFFFFFFFull / (uint64_t)ncs + 1ull;
+            for (int c = lane; c < ncs; c += 32) {
+                const uint32_t x = (uint32_t)c * (uint32_t)nv;   // < 4096 * 65536
+                dst[c] = src[(int)__umul64hi((uint64_t)x, mg)];
             }
         }
-        e_ncs[threadIdx.x] = ncs;
-        e_nv[threadIdx.x] = nv;
-        e_all[threadIdx.x] = all;
-        e_g[threadIdx.x] = g;
-        e_dst[threadIdx.x] = dst;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int c = 0;
-        for (int i = 0; i < npair; ++i) { e_off[i] = c; c += e_ncs[i]; }
-        e_off[npair] = c;
-        e_cnt = c;
-    }
-    __syncthreads();
-    const int total = e_cnt;
-    int e = 0;
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        while (idx >= e_off[e + 1]) ++e;   // idx only grows, so e only grows
-        const int sl = idx - e_off[e];
-        const int nv = e_nv[e], ncs = e_ncs[e];
-        // sl*nv < 8192*65536 fits 32 bits
-        const int j = e_all[e] ? sl : (int)(((uint32_t)sl * (uint32_t)nv) / (uint32_t)ncs);
-        a.samp[e_dst[e] + sl] = xo[e_g[e] * Nst + j];
     }
 }
 
@@ -206,9 +195,10 @@ __device__ __forceinline__ void class_run(const float* __restrict__ wt, int P, i
         float w[MW];
 #pragma unroll
         for (int i = 0; i < M; ++i) w[i] = __ldg(wt + i * P + p);
+        const float2* x = win + b0 + u0 * Hs;
+        float2* o = xo + jc + P * u0;
 #pragma unroll 2
         for (int u = u0; u < u1; ++u) {
-            const float2* x = win + b0 + u * Hs;
             float sre = 0.0f, sim = 0.0f;
 #pragma unroll
             for (int i = 0; i < M; ++i) {
@@ -216,7 +206,9 @@ __device__ __forceinline__ void class_run(const float* __restrict__ wt, int P, i
                 sre = fmaf(w[i], xi.x, sre);
                 sim = fmaf(w[i], xi.y, sim);
             }
-            xo[jc + P * u] = cmul_unfused(A, make_float2(sre, sim));
+            *o = cmul_unfused(A, make_float2(sre, sim));
+            x += Hs;
+            o += P;
         }
     } else {
         for (int u = u0; u < u1; ++u) {

@@ -182,6 +182,25 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
     }
 }
 
+// Packed FP32 pairs (sm_100): fma.rn.f32x2 is two IEEE fmaf, lane by lane, so
+// a (re, im) tap pair costs one instruction and rounds exactly like fmaf.
+__device__ __forceinline__ unsigned long long f2_pack(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float2 f2_unpack(unsigned long long v) {
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+    return make_float2(lo, hi);
+}
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
 // Outputs of one phase class: trials j = jc + P*u, u in [u0, u1), whose phase
 // row p and window start b0 (+ u*Hs) are fixed, so the m weights and the
 // complex factor stay in registers.  Same sequential FMA chain and unfused
@@ -192,21 +211,20 @@ __device__ __forceinline__ void class_run(const float* __restrict__ wt, int P, i
                                           int u1, float2* xo, int m) {
     if (M > 0) {
         constexpr int MW = M > 0 ? M : 1;
-        float w[MW];
+        unsigned long long w2[MW];
 #pragma unroll
-        for (int i = 0; i < M; ++i) w[i] = __ldg(wt + i * P + p);
-        const float2* x = win + b0 + u0 * Hs;
+        for (int i = 0; i < M; ++i) {
+            const float wi = __ldg(wt + i * P + p);
+            w2[i] = f2_pack(wi, wi);
+        }
+        const unsigned long long* x = reinterpret_cast<const unsigned long long*>(win + b0 + u0 * Hs);
         float2* o = xo + jc + P * u0;
 #pragma unroll 2
         for (int u = u0; u < u1; ++u) {
-            float sre = 0.0f, sim = 0.0f;
+            unsigned long long acc = 0ull;   // (+0, +0)
 #pragma unroll
-            for (int i = 0; i < M; ++i) {
-                const float2 xi = x[i];
-                sre = fmaf(w[i], xi.x, sre);
-                sim = fmaf(w[i], xi.y, sim);
-            }
-            *o = cmul_unfused(A, make_float2(sre, sim));
+            for (int i = 0; i < M; ++i) acc = f2_fma(w2[i], x[i], acc);
+            *o = cmul_unfused(A, f2_unpack(acc));
             x += Hs;
             o += P;
         }
@@ -225,13 +243,76 @@ __device__ __forceinline__ void class_run(const float* __restrict__ wt, int P, i
     }
 }
 
+// class_run for 16 taps when consecutive trials of the class sit HS < 16 bins
+// apart: the 16 window values live in a register ring and each trial loads
+// only its HS new ones.  Element i of trial it (counted from u0) sits in slot
+// (i + it*HS) mod 16; after a trial the HS oldest slots take the next values.
+// The ring offsets repeat after 16/gcd(16, HS) trials, the unrolled period.
+// Same chain, same order of taps as class_run.
+template <int HS>
+__device__ __forceinline__ void slide_run(const float* __restrict__ wt, int P, int p, float2 A,
+                                          const float2* __restrict__ win, int b0, int jc, int u0, int u1,
+                                          float2* xo) {
+    constexpr int M = 16;
+    constexpr int G = (HS % 16 == 0) ? 16 : (HS % 8 == 0) ? 8 : (HS % 4 == 0) ? 4 : (HS % 2 == 0) ? 2 : 1;
+    constexpr int PERIOD = M / G;
+    unsigned long long w2[M], r[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        const float wi = __ldg(wt + i * P + p);
+        w2[i] = f2_pack(wi, wi);
+    }
+    const unsigned long long* xn = reinterpret_cast<const unsigned long long*>(win + b0 + u0 * HS);
+#pragma unroll
+    for (int i = 0; i < M; ++i) r[i] = xn[i];
+    xn += M;
+    float2* o = xo + jc + P * u0;
+    int u = u0;
+    while (true) {
+#pragma unroll
+        for (int it = 0; it < PERIOD; ++it) {
+            unsigned long long acc = 0ull;   // (+0, +0)
+#pragma unroll
+            for (int i = 0; i < M; ++i) acc = f2_fma(w2[i], r[(i + it * HS) % M], acc);
+            *o = cmul_unfused(A, f2_unpack(acc));
+            o += P;
+            if (++u >= u1) return;
+#pragma unroll
+            for (int j = 0; j < HS; ++j) r[(it * HS + j) % M] = xn[j];
+            xn += HS;
+        }
+    }
+}
+
+__device__ __forceinline__ bool slide_dispatch(int Hs, const float* __restrict__ wt, int P, int p, float2 A,
+                                               const float2* __restrict__ win, int b0, int jc, int u0, int u1,
+                                               float2* xo) {
+    switch (Hs) {
+        case 1: slide_run<1>(wt, P, p, A, win, b0, jc, u0, u1, xo); return true;
+        case 2: slide_run<2>(wt, P, p, A, win, b0, jc, u0, u1, xo); return true;
+        case 3: slide_run<3>(wt, P, p, A, win, b0, jc, u0, u1, xo); return true;
+        case 4: slide_run<4>(wt, P, p, A, win, b0, jc, u0, u1, xo); return true;
+        case 5: slide_run<5>(wt, P, p, A, win, b0, jc, u0, u1, xo); return true;
+        case 6: slide_run<6>(wt, P, p, A, win, b0, jc, u0, u1, xo); return true;
+        case 7: slide_run<7>(wt, P, p, A, win, b0, jc, u0, u1, xo); return true;
+        case 8: slide_run<8>(wt, P, p, A, win, b0, jc, u0, u1, xo); return true;
+        case 9: slide_run<9>(wt, P, p, A, win, b0, jc, u0, u1, xo); return true;
+        case 10: slide_run<10>(wt, P, p, A, win, b0, jc, u0, u1, xo); return true;
+        case 11: slide_run<11>(wt, P, p, A, win, b0, jc, u0, u1, xo); return true;
+        case 12: slide_run<12>(wt, P, p, A, win, b0, jc, u0, u1, xo); return true;
+        default: return false;
+    }
+}
+
 // One CTA per (group of 4 harmonics, block).  Per harmonic: the range guard on
 // the block's TRUE trial range (src/directinterp.jl:490-496), the bin window
 // staged in shared memory, then every phase class of the block's trials --
 // trials t and t+P share the phase row (t mod P) and sit exactly
-// Hs = P*h*pnum/q bins apart -- split into runs over the threads.
+// Hs = P*h*pnum/q bins apart -- split into runs over the threads.  Three CTAs
+// per SM (74 KB of shared memory each, registers capped to match) hide the
+// shared-memory latency of the tap loads.
 template <int M>
-__global__ void __launch_bounds__(256) k_interp(WaveArgs a, int win_max, int Nst, int* err) {
+__global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int Nst, int* err) {
     extern __shared__ float2 sm_i[];
     float2* win = sm_i;
     float2* xo = sm_i + win_max;            // [kHG][Nst] staged outputs
@@ -335,7 +416,9 @@ __global__ void __launch_bounds__(256) k_interp(WaveArgs a, int win_max, int Nst
             const int64_t qv = small ? (int64_t)(((uint32_t)res0 + (uint32_t)jc * (uint32_t)hpn) / (uint32_t)q)
                                      : ((int64_t)res0 + (int64_t)jc * hpn) / q;
             const int b0 = (int)(base + qv + ct[p]);
-            class_run<M>(wt, P, p, __ldg(at + p), win, b0, Hs, jc, u0, u1, xg, m);
+            const float2 A = __ldg(at + p);
+            if (M == 16 && u1 - u0 >= 2 && slide_dispatch(Hs, wt, P, p, A, win, b0, jc, u0, u1, xg)) continue;
+            class_run<M>(wt, P, p, A, win, b0, Hs, jc, u0, u1, xg, m);
         }
     }
     __syncthreads();

@@ -556,7 +556,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             else
                 CS_CUDA(launch_synth_fp32(a, H->stream, (int)smem_synth), "synth launch");
             CS_CUDA(cudaEventRecord(H->ev[2], H->stream), "event");
-            CS_CUDA(launch_sigma(a, H->stream, max_hk, max_np), "sigma launch");
+            CS_CUDA(launch_sigma(a, H->stream, max_hk, max_np, d_err), "sigma launch");
             CS_CUDA(cudaEventRecord(H->ev[3], H->stream), "event");
             if (!R.exact_all) {
                 CS_CUDA(launch_flag(a, H->stream), "flag launch");
@@ -573,6 +573,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         S.d2h_bytes += 4 * sizeof(int32_t);
         if (counts[2] == 1) return fail(H, CS_ERR_CUDA, "interpolation window exceeded its bound");
         if (counts[2] == 2) return fail(H, CS_ERR_TIMEOUT, "tensor-core completion wait ran out");
+        if (counts[2] == 3) return fail(H, CS_ERR_TIMEOUT, "sigma sample copy wait ran out");
         float ms = 0.0f;
         CS_CUDA(cudaEventElapsedTime(&ms, H->ev[0], H->ev[1]), "timing");
         S.ms_interp += ms;
@@ -1079,12 +1080,13 @@ extern "C" cs_status cs_chunk_metrics_static(const cs_params* params, const floa
     a.verify_gate = 0;
     a.exact_all = 1;
     CS_STATIC_CUDA(launch_interp(a, st, win_max, cnt + 2), "interp launch");
-    CS_STATIC_CUDA(launch_sigma(a, st, L.Hk, L.np), "sigma launch");
+    CS_STATIC_CUDA(launch_sigma(a, st, L.Hk, L.np, cnt + 2), "sigma launch");
     CS_STATIC_CUDA(launch_rescue(a, st, sms), "metric launch");
     int32_t counts[4] = {0, 0, 0, 0};
     CS_STATIC_CUDA(cudaMemcpyAsync(counts, cnt, sizeof(counts), cudaMemcpyDeviceToHost, st), "read counters");
     CS_STATIC_CUDA(cudaStreamSynchronize(st), "chunk");
 #undef CS_STATIC_CUDA
     if (counts[2] == 1) return static_fail(err, err_cap, CS_ERR_CUDA, "interpolation window exceeded its bound");
+    if (counts[2] == 3) return static_fail(err, err_cap, CS_ERR_TIMEOUT, "sigma sample copy wait ran out");
     return CS_OK;
 }

@@ -16,6 +16,7 @@ constexpr int kSigmaCap = 8192;    // _BOXCAR_SIGMA_SAMPLES, src/search.jl:462
 constexpr int kTileTrials = 64;    // trials per CTA in the FP32 synthesis kernel
 constexpr int kATileBytes = 128 * 128 * 2;  // one 16-bit A tile: 128 trials x 128 K
 constexpr int kSampStride = kSigmaCap / 2;  // float2 per (block, level) in `samp`
+constexpr int kSigmaThreads = 384;          // k_sigma CTA: one pass over a level's synthesis tasks
 
 // One harmonic's rational trial-grid recipe (DirectPlan, src/directinterp.jl:179-204).
 // Global trial t of the search evaluates harmonic h at Fourier frequency
@@ -153,11 +154,63 @@ cudaError_t launch_synth_tc(const WaveArgs& a, const TcPlanHost& tp, const void*
                             cudaStream_t st, int num_sms);
 
 // Kernel launchers (cs_kernels.cu).  Each returns the launch error.
+#ifdef __CUDACC__
+// ---------------------------------------------------------------------------
+// Shared-memory barriers and plain (non-multicast) bulk copies, used by the
+// tensor-core synthesis and the block sigma.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kWaitLimit = 1u << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait on an mbarrier phase: gives up after kWaitLimit polls or one
+// second of wall time, whichever comes first.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((it & 1023u) == 1023u && global_ns() - t0 > 1000000000ull) return false;
+    }
+    return false;
+}
+
+// Plain (non-multicast) 1-D bulk copy global -> this CTA's shared memory,
+// completing `bytes` of transaction on mbarrier `bar` (armed here).
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+#endif  // __CUDACC__
+
 cudaError_t launch_interp(const WaveArgs& a, cudaStream_t st, int win_max, int* err);
 cudaError_t launch_synth_fp32(const WaveArgs& a, cudaStream_t st, int smem_bytes);
 size_t sigma_smem(int max_hk, int max_np);
 size_t interp_smem(int win_max, int Nprof);
-cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np);
+cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np, int* err);
 cudaError_t launch_flag(const WaveArgs& a, cudaStream_t st);
 cudaError_t launch_rescue(const WaveArgs& a, cudaStream_t st, int num_sms);
 size_t synth_fp32_smem(int nharms, int maxbins, int maxwmax);

@@ -610,7 +610,7 @@ cudaError_t launch_synth_fp32(const WaveArgs& a, cudaStream_t st, int smem_bytes
 // Block sigma: exact FP32 profiles of the pooled columns, then the exact median
 // ---------------------------------------------------------------------------
 
-// Block-wide exclusive prefix sum of one int per thread (blockDim.x == 256).
+// Block-wide exclusive prefix sum of one int per thread (blockDim.x <= 1024).
 __device__ __forceinline__ int block_excl_scan(int v, int* warp_tot, int* total) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int x = v;
@@ -655,16 +655,17 @@ __device__ uint32_t radix_select(const uint32_t* vals, int ns, int kth, uint32_t
             if ((v & mask) == prefix) atomicAdd(&hist[(v >> shift) & (uint32_t)(nb - 1)], 1u);
         }
         __syncthreads();
-        const int per = nb / (int)blockDim.x;
+        const int per = (nb + (int)blockDim.x - 1) / (int)blockDim.x;
+        const int b0 = min(nb, (int)threadIdx.x * per), b1 = min(nb, b0 + per);
         int local = 0;
-        for (int b = 0; b < per; ++b) local += (int)hist[threadIdx.x * per + b];
+        for (int b = b0; b < b1; ++b) local += (int)hist[b];
         const int excl = block_excl_scan(local, wtot, sh + 2);
         if (excl <= kk && kk < excl + local) {
             int c = excl;
-            for (int b = 0; b < per; ++b) {
-                const int hb = (int)hist[threadIdx.x * per + b];
+            for (int b = b0; b < b1; ++b) {
+                const int hb = (int)hist[b];
                 if (c + hb > kk) {
-                    sh[0] = threadIdx.x * per + b;
+                    sh[0] = b;
                     sh[1] = kk - c;
                     break;
                 }
@@ -686,11 +687,12 @@ __device__ uint32_t radix_select(const uint32_t* vals, int ns, int kth, uint32_t
 // `samp`; their profiles are built here with synth_chunk8 -- the arithmetic of
 // the FP32 synthesis and of the rescan -- so sigma is identical in every
 // synthesis mode.  sigma = 1.4826 * median(|x|), _median! semantics.
-__global__ void __launch_bounds__(256) k_sigma(WaveArgs a) {
+__global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err) {
     extern __shared__ float4 ss4[];
     __shared__ int sh[4];
     __shared__ int wtot[32];
-    __shared__ uint32_t red[8];
+    __shared__ uint32_t red[32];
+    __shared__ __align__(8) uint64_t sbar;
     const int bl = blockIdx.x;
     const int l = bl % a.nlev;
     const DevLevel& L = a.levels[l];
@@ -709,12 +711,45 @@ __global__ void __launch_bounds__(256) k_sigma(WaveArgs a) {
     const float* C2 = a.tw + L.tw_off;
     const float* S2 = C2 + (int64_t)Hk * np;
     const float2* samp = a.samp + (int64_t)bl * kSampStride;
-    for (int idx = threadIdx.x; idx < Hk * ncs; idx += blockDim.x) Xs[idx] = samp[idx];
+    // The samples arrive by one bulk copy (rounded up to 16 bytes, still inside
+    // this (block, level)'s kSampStride slot) instead of dependent loads.
+    if (threadIdx.x == 0) {
+        mbar_init(&sbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     __syncthreads();
-    // Two columns per thread share each twiddle load (read through L1).
+    if (threadIdx.x == 0)
+        bulk_load(smem_u32(Xs), samp, (uint32_t)((Hk * ncs * (int)sizeof(float2) + 15) & ~15), &sbar);
+    if (__syncthreads_or(!mbar_wait(&sbar, 0))) {
+        // give up (every thread alike) with an error status, after the copy in
+        // flight (bounded again)
+        mbar_wait(&sbar, 0);
+        if (threadIdx.x == 0) {
+            atomicExch(err, 3);
+            a.sigma[bl] = 0.0f;
+        }
+        return;
+    }
+    // Two columns per thread share each twiddle load (read through L1) when
+    // the pairs fit one pass of the CTA; otherwise one column per thread, so
+    // that the pass count, not a thin second pass, sets the time.
     const int nch = (Hk + 1 + 7) / 8;
     const int npairs = (ncs + 1) / 2;
-    for (int idx = threadIdx.x; idx < npairs * nch; idx += blockDim.x) {
+    if (npairs * nch > (int)blockDim.x) {
+        for (int idx = threadIdx.x; idx < ncs * nch; idx += blockDim.x) {
+            const int sl = idx % ncs, ch = idx / ncs;
+            const int n0 = ch * 8;
+            float E[8], O[8];
+            synth_chunk8(Xs + sl, ncs, C2, S2, np, 1, Hk, n0, E, O);
+            uint32_t* d = vals + sl * nbins;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int nn = n0 + u;
+                if (nn <= Hk) d[nn] = __float_as_uint(fabsf(E[u] + O[u]));
+                if (nn >= 1 && nn < Hk) d[2 * Hk - nn] = __float_as_uint(fabsf(E[u] - O[u]));
+            }
+        }
+    } else for (int idx = threadIdx.x; idx < npairs * nch; idx += blockDim.x) {
         const int pr = idx % npairs, ch = idx / npairs;
         const int sa = 2 * pr, sb = min(2 * pr + 1, ncs - 1);
         const int n0 = ch * 8;
@@ -776,10 +811,10 @@ size_t sigma_smem(int max_hk, int max_np) {
     return (size_t)kSampStride * sizeof(float2) + (size_t)kSigmaCap * sizeof(uint32_t);
 }
 
-cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np) {
+cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np, int* err) {
     const size_t smem = sigma_smem(max_hk, max_np);
     cudaFuncSetAttribute(k_sigma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_sigma<<<a.nblk * a.nlev, 256, smem, st>>>(a);
+    k_sigma<<<a.nblk * a.nlev, kSigmaThreads, smem, st>>>(a, err);
     return cudaGetLastError();
 }
 

@@ -34,11 +34,6 @@ constexpr int kTM = 128;            // trials per tile (MMA M)
 constexpr int kK = 128;             // padded K: 2*nharms <= 128
 constexpr int kSBO = (kK / 8) * 128;  // bytes between 8-row groups
 constexpr int kABytes = kTM * kK * 2;
-constexpr uint32_t kWaitLimit = 1u << 24;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
     uint64_t d = 0;
@@ -47,45 +42,6 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
     d |= (uint64_t)((kSBO >> 4) & 0x3FFF) << 32;            // SBO: 8-row groups
     d |= (uint64_t)1 << 46;                                 // descriptor version (sm_100)
     return d;                                               // base offset 0, SWIZZLE_NONE
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ uint64_t global_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Bounded wait on an mbarrier phase: gives up after kWaitLimit polls or one
-// second of wall time, whichever comes first.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    const uint64_t t0 = global_ns();
-    for (uint32_t it = 0; it < kWaitLimit; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(smem_u32(bar)), "r"(parity)
-            : "memory");
-        if (done) return true;
-        if ((it & 1023u) == 1023u && global_ns() - t0 > 1000000000ull) return false;
-    }
-    return false;
-}
-
-// Plain (non-multicast) 1-D bulk copy global -> this CTA's shared memory,
-// completing `bytes` of transaction on mbarrier `bar` (armed here).
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(dst), "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
 }
 
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float v[8]) {

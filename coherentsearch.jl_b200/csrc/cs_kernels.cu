@@ -503,10 +503,10 @@ __device__ __forceinline__ void synth_chunk8x2(const float2* __restrict__ xa, co
     for (int jh = 1; jh < Hk; ++jh) {
         const float2 x = xa[(jh - 1) * xstride];
         const float2 y = xb[(jh - 1) * xstride];
-        const float4 c0 = __ldg(reinterpret_cast<const float4*>(C2 + jh * np + n0));
-        const float4 c1 = __ldg(reinterpret_cast<const float4*>(C2 + jh * np + n0 + 4));
-        const float4 s0 = __ldg(reinterpret_cast<const float4*>(S2 + jh * np + n0));
-        const float4 s1 = __ldg(reinterpret_cast<const float4*>(S2 + jh * np + n0 + 4));
+        const float4 c0 = *reinterpret_cast<const float4*>(C2 + jh * np + n0);
+        const float4 c1 = *reinterpret_cast<const float4*>(C2 + jh * np + n0 + 4);
+        const float4 s0 = *reinterpret_cast<const float4*>(S2 + jh * np + n0);
+        const float4 s1 = *reinterpret_cast<const float4*>(S2 + jh * np + n0 + 4);
         const float c[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
         const float sv[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
 #pragma unroll
@@ -708,8 +708,9 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
     float2* Xs = reinterpret_cast<float2*>(ss4);                    // [Hk][ncs], <= kSampStride
     uint32_t* hist = reinterpret_cast<uint32_t*>(ss4);              // reuses Xs once profiles exist
     uint32_t* vals = reinterpret_cast<uint32_t*>(Xs + kSampStride);  // [ns]
-    const float* C2 = a.tw + L.tw_off;
-    const float* S2 = C2 + (int64_t)Hk * np;
+    float* tws = reinterpret_cast<float*>(vals + kSigmaCap);        // the level's C2 then S2 rows
+    const float* C2 = tws;
+    const float* S2 = tws + Hk * np;
     const float2* samp = a.samp + (int64_t)bl * kSampStride;
     // The samples arrive by one bulk copy (rounded up to 16 bytes, still inside
     // this (block, level)'s kSampStride slot) instead of dependent loads.
@@ -718,8 +719,14 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (threadIdx.x == 0)
-        bulk_load(smem_u32(Xs), samp, (uint32_t)((Hk * ncs * (int)sizeof(float2) + 15) & ~15), &sbar);
+    if (threadIdx.x == 0) {
+        // the level's twiddle rows come along (2*Hk*np floats, a multiple of 64 bytes)
+        const uint32_t xb = (uint32_t)((Hk * ncs * (int)sizeof(float2) + 15) & ~15);
+        const uint32_t tb = (uint32_t)(2 * Hk * np * (int)sizeof(float));
+        mbar_expect_tx(&sbar, xb + tb);
+        bulk_copy(smem_u32(Xs), samp, xb, &sbar);
+        bulk_copy(smem_u32(tws), a.tw + L.tw_off, tb, &sbar);
+    }
     if (__syncthreads_or(!mbar_wait(&sbar, 0))) {
         // give up (every thread alike) with an error status, after the copy in
         // flight (bounded again)
@@ -806,9 +813,8 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
 }
 
 size_t sigma_smem(int max_hk, int max_np) {
-    (void)max_hk;
-    (void)max_np;
-    return (size_t)kSampStride * sizeof(float2) + (size_t)kSigmaCap * sizeof(uint32_t);
+    return (size_t)kSampStride * sizeof(float2) + (size_t)kSigmaCap * sizeof(uint32_t) +
+           (size_t)2 * max_hk * max_np * sizeof(float);
 }
 
 cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np, int* err) {

@@ -137,6 +137,16 @@ def interp_flops_per_trial(m=16):
     return NHARMS * (4 * m + 6)   # m real-times-complex FMAs + one complex product
 
 
+# DRAM bytes (read + write) per trial of one launch, from the ncu captures
+# summarised under profiles/ (small survey case, 1,282,048 trials; the traffic
+# of these kernels grows in proportion to the trial count).
+NCU_BYTES_PER_TRIAL = {"k_interp": 295.3, "k_synth_tc": 277.3, "k_sigma": 98.9, "k_flag+k_rescue": 24.5}
+# Algorithmic DRAM bytes per trial: k_interp writes 240 B of FP16 A-tile chunks
+# and 96 B of sigma samples and reads ~4 B of spectrum; k_sigma reads the 96 B
+# of samples; the flag pass reads 6 levels x 4 B of gate values.
+ALG_BYTES_PER_TRIAL = {"k_interp": 340.0, "k_sigma": 96.0, "k_flag+k_rescue": 24.0}
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -333,34 +343,37 @@ def main():
     prof_per_trial = st["profiles"] / max(1, trials)
     # roofline of the dominant kernel
     dom = max(stage, key=stage.get)
-    sm_mhz = res["clocks"].get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
     fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12   # TFLOP/s, nominal
-    x_bytes = trials * NHARMS * 8.0
     tc_flops = trials * 2.0 * 128 * 352     # dense product per trial: 2 * K(128) * N(352 columns)
-    if dom == "ms_synth" and args.synth != "fp32":
+    kname = {"ms_interp": "k_interp", "ms_synth": "k_synth_tc" if args.synth != "fp32" else "k_synth_fp32",
+             "ms_sigma": "k_sigma", "ms_rescue": "k_flag+k_rescue"}[dom]
+    traffic = NCU_BYTES_PER_TRIAL.get(kname)
+    traffic = traffic * trials if traffic is not None else None
+    if kname == "k_synth_tc":
         achieved = tc_flops / (stage[dom] / 1000.0) / 1e12
-        roof = {"kernel": "k_synth_tc", "bound": "tensor", "achieved": achieved,
-                "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"],
-                "traffic": None, "work": "2*128*352 flops per trial (dense 16-bit product, all levels)"}
-    elif dom == "ms_synth" and args.synth == "fp32":
-        fl = trials * (synth_flops_per_trial(frac_valid))
+        roof = {"kernel": kname, "bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
+                "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"], "traffic": traffic,
+                "work": "2*128*352 flops per trial (dense 16-bit product, all levels)"}
+    elif kname == "k_synth_fp32":
+        fl = trials * synth_flops_per_trial({1: 1.0})
         achieved = fl / (stage[dom] / 1000.0) / 1e12
-        roof = {"kernel": "k_synth_fp32", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+        roof = {"kernel": kname, "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
                 "peak_source": "nominal FP32 FMA rate 148 SM x 128 lanes x 2 x max SM clock "
                                "(no measured FP32 peak exists)",
                 "work": "4(Hk+1)(Hk-1) flops per trial per level"}
-    elif dom == "ms_interp":
-        fl = trials * interp_flops_per_trial()
-        achieved = fl / (stage[dom] / 1000.0) / 1e12
-        roof = {"kernel": "k_interp", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
-                "peak_source": "nominal FP32 FMA rate (no measured FP32 peak exists)",
-                "work": "nharms*(4m+6) flops per trial"}
     else:
-        achieved = x_bytes / (stage[dom] / 1000.0) / 1e9
-        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None}
+        alg = ALG_BYTES_PER_TRIAL[kname] * trials
+        achieved = alg / (stage[dom] / 1000.0) / 1e9
+        roof = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                "work": f"{ALG_BYTES_PER_TRIAL[kname]:.0f} algorithmic DRAM bytes per trial"}
+        if kname == "k_interp":
+            fl = trials * interp_flops_per_trial()
+            roof["fp32"] = {"achieved_tflops": fl / (stage[dom] / 1000.0) / 1e12, "peak_tflops": fp32_peak,
+                            "work": "nharms*(4m+6) flops per trial",
+                            "note": "limited by shared-memory tap loads, not DRAM or FMA"}
+    roof["peak_source"] = roof.get("peak_source", f"MEASURED_PEAKS.json ({psrc})")
     roof["stage_ms"] = stage
     cpu = None
     try:

@@ -247,7 +247,10 @@ class Engine:
                    exact_all=False, cap=1 << 16) -> np.ndarray:
         thr = self.params.threshold if threshold is None else threshold
         while True:
-            out = np.zeros(cap, dtype=_lib.CAND_DTYPE)
+            # one reusable output array per engine: no per-call zero fill
+            if getattr(self, "_cand_buf", None) is None or len(self._cand_buf) < cap:
+                self._cand_buf = np.empty(cap, dtype=_lib.CAND_DTYPE)
+            out = self._cand_buf
             n = ctypes.c_int64()
             st = self.lib.cs_search(self._h, float(lofreq), float(hifreq), int(lobin), int(blocksize),
                                     float(thr), int(bool(exact_all)), out.ctypes.data, cap,
@@ -256,7 +259,7 @@ class Engine:
                 cap = int(n.value)
                 continue
             _lib.check(st, self._h, "cs_search")
-            return out[:n.value]
+            return out[:n.value].copy()
 
     def stats(self) -> dict:
         s = _lib.cs_stats()

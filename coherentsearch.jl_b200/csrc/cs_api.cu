@@ -46,6 +46,31 @@ struct DBuf {
     T* as() const { return static_cast<T*>(p); }
 };
 
+// Pinned host staging (grown on demand): copies from and to it are truly
+// asynchronous, so a search enqueues its work without host-side stalls.
+struct HBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t need) {
+        if (need == 0) need = 16;
+        if (need <= bytes) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaHostAlloc(&p, need, cudaHostAllocDefault);
+        if (e == cudaSuccess) bytes = need;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+
 struct LevelHost {
     int k, Hk, nbins;
     std::vector<int> widths;
@@ -216,6 +241,7 @@ struct cs_handle {
     TcPlanHost tc;                      // tensor-core synthesis plan (synth != FP32)
     DBuf d_tcB;
     DBuf d_A, d_samp;
+    HBuf h_nvalid, h_io;                // pinned: valid counts up; counters + candidate prefix down
     DBuf d_levels, d_tw, d_harms, d_wtab, d_atab, d_ctab, d_nvalid, d_X, d_Q0, d_sigma,
         d_tmetric, d_items, d_counts, d_cands;
     // FP64 plan tables of the last anchor r_lo, already on the device
@@ -446,7 +472,8 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
     }
     if (!R.interp_only) {
         CS_CUDA(H->d_samp.ensure((size_t)WB * nlev * kSampStride * sizeof(float2)), "alloc samples");
-        CS_CUDA(H->d_Q0.ensure((size_t)WB * nlev * Nprof * sizeof(float)), "alloc Q0");
+        if (H->diag >= 2 && !R.exact_all)
+            CS_CUDA(H->d_Q0.ensure((size_t)WB * nlev * Nprof * sizeof(float)), "alloc gate values");
         CS_CUDA(H->d_sigma.ensure((size_t)WB * nlev * sizeof(float)), "alloc sigma");
         CS_CUDA(H->d_nvalid.ensure((size_t)WB * nlev * sizeof(int32_t)), "alloc nvalid");
         CS_CUDA(H->d_items.ensure((size_t)WB * nlev * Nprof * sizeof(DevItem)), "alloc items");
@@ -473,9 +500,11 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         H->last_Nprof = Nprof;
     }
     const double nyq = (double)H->N / 2.0;
-    std::vector<int32_t> nvalid;
-    std::vector<DevCand> wave_c;
-    int32_t counts[4];
+    // counters, then the first kCandPrefix candidates, come back in one pinned read
+    constexpr int kCandPrefix = 4096;
+    CS_CUDA(H->h_io.ensure(64 + (size_t)kCandPrefix * sizeof(DevCand)), "pinned readback");
+    int32_t* counts = H->h_io.as<int32_t>();
+    DevCand* cand_pre = reinterpret_cast<DevCand*>(H->h_io.as<uint8_t>() + 64);
 
     for (int64_t c0 = 0; c0 < R.nblocks; c0 += WB) {
         const int nb = (int)std::min<int64_t>(WB, R.nblocks - c0);
@@ -503,7 +532,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         a.tiles_per_blk = tiles_per_blk;
         a.fp16 = p.synth == CS_SYNTH_FP16 ? 1 : 0;
         a.samp = R.interp_only ? nullptr : H->d_samp.as<float2>();
-        a.Q0 = H->d_Q0.as<float>();
+        a.Q0 = (H->diag >= 2 && !R.exact_all) ? H->d_Q0.as<float>() : nullptr;   // gate values: diagnostics only
         a.sigma = H->d_sigma.as<float>();
         a.tmetric = R.exact_all ? H->d_tmetric.as<float>() : nullptr;
         a.items = H->d_items.as<DevItem>();
@@ -528,7 +557,8 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         a.exact_all = R.exact_all ? 1 : 0;
         int* d_err = H->d_counts.as<int32_t>() + 2;
 
-        nvalid.assign((size_t)nb * nlev, 0);
+        CS_CUDA(H->h_nvalid.ensure((size_t)nb * nlev * sizeof(int32_t)), "pinned valid counts");
+        int32_t* nvalid = H->h_nvalid.as<int32_t>();
         for (int b = 0; b < nb; ++b) {
             const int64_t c = c0 + b;
             const int64_t i0 = c * (int64_t)Nprof;  // trial offset of the block
@@ -542,8 +572,10 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         }
         CS_CUDA(cudaMemsetAsync(H->d_counts.p, 0, 4 * sizeof(int32_t), H->stream), "reset counters");
         if (!R.interp_only) {
-            CS_CUDA(upload(H->d_nvalid, nvalid, H->stream), "upload nvalid");
-            S.h2d_bytes += (int64_t)(nvalid.size() * sizeof(int32_t));
+            CS_CUDA(cudaMemcpyAsync(H->d_nvalid.p, nvalid, (size_t)nb * nlev * sizeof(int32_t),
+                                    cudaMemcpyHostToDevice, H->stream),
+                    "upload nvalid");
+            S.h2d_bytes += (int64_t)nb * nlev * (int64_t)sizeof(int32_t);
             a.nvalid = H->d_nvalid.as<int32_t>();
         }
         CS_CUDA(cudaEventRecord(H->ev[0], H->stream), "event");
@@ -551,24 +583,32 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         CS_CUDA(cudaEventRecord(H->ev[1], H->stream), "event");
         S.launches += 1;
         if (!R.interp_only) {
-            if (tensor)
-                CS_CUDA(launch_synth_tc(a, H->tc, H->d_tcB.p, d_err, H->stream, H->num_sms), "synth launch");
-            else
-                CS_CUDA(launch_synth_fp32(a, H->stream, (int)smem_synth), "synth launch");
-            CS_CUDA(cudaEventRecord(H->ev[2], H->stream), "event");
+            // sigma needs only the samples, so it runs first and the synthesis
+            // epilogue applies the medcut test itself (no gate pass over HBM);
+            // exact_all scores every trial exactly and needs no gate at all
             CS_CUDA(launch_sigma(a, H->stream, max_hk, max_np, d_err), "sigma launch");
-            CS_CUDA(cudaEventRecord(H->ev[3], H->stream), "event");
+            CS_CUDA(cudaEventRecord(H->ev[2], H->stream), "event");
+            S.launches += 1;
             if (!R.exact_all) {
-                CS_CUDA(launch_flag(a, H->stream), "flag launch");
+                if (tensor)
+                    CS_CUDA(launch_synth_tc(a, H->tc, H->d_tcB.p, d_err, H->stream, H->num_sms), "synth launch");
+                else
+                    CS_CUDA(launch_synth_fp32(a, H->stream, (int)smem_synth), "synth launch");
                 S.launches += 1;
             }
+            CS_CUDA(cudaEventRecord(H->ev[3], H->stream), "event");
             CS_CUDA(launch_rescue(a, H->stream, H->num_sms), "rescue launch");
             CS_CUDA(cudaEventRecord(H->ev[4], H->stream), "event");
-            S.launches += 3;
+            S.launches += 1;
         }
         CS_CUDA(cudaMemcpyAsync(counts, H->d_counts.p, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost,
                                 H->stream),
                 "read counters");
+        const int n_pre = (int)std::min<size_t>((size_t)kCandPrefix, H->d_cands.bytes / sizeof(DevCand));
+        if (cands && !R.interp_only && n_pre > 0)
+            CS_CUDA(cudaMemcpyAsync(cand_pre, H->d_cands.p, (size_t)n_pre * sizeof(DevCand),
+                                    cudaMemcpyDeviceToHost, H->stream),
+                    "read candidates");
         CS_CUDA(cudaStreamSynchronize(H->stream), "wave");
         S.d2h_bytes += 4 * sizeof(int32_t);
         if (counts[2] == 1) return fail(H, CS_ERR_CUDA, "interpolation window exceeded its bound");
@@ -579,9 +619,9 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         S.ms_interp += ms;
         if (!R.interp_only) {
             CS_CUDA(cudaEventElapsedTime(&ms, H->ev[1], H->ev[2]), "timing");
-            S.ms_synth += ms;
-            CS_CUDA(cudaEventElapsedTime(&ms, H->ev[2], H->ev[3]), "timing");
             S.ms_sigma += ms;
+            CS_CUDA(cudaEventElapsedTime(&ms, H->ev[2], H->ev[3]), "timing");
+            S.ms_synth += ms;
             CS_CUDA(cudaEventElapsedTime(&ms, H->ev[3], H->ev[4]), "timing");
             S.ms_rescue += ms;
             CS_CUDA(cudaEventElapsedTime(&ms, H->ev[0], H->ev[4]), "timing");
@@ -603,18 +643,21 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         if (!R.exact_all && n_items > a.cap_items) return fail(H, CS_ERR_CAPACITY, "rescue list overflow");
         if (n_c > a.cap_cands) return fail(H, CS_ERR_CAPACITY, "candidate list overflow");
         if (cands && n_c > 0) {
-            wave_c.resize(n_c);
-            CS_CUDA(cudaMemcpy(wave_c.data(), H->d_cands.p, (size_t)n_c * sizeof(DevCand),
-                               cudaMemcpyDeviceToHost),
-                    "read candidates");
-            cands->insert(cands->end(), wave_c.begin(), wave_c.end());
+            cands->insert(cands->end(), cand_pre, cand_pre + std::min(n_c, n_pre));
+            if (n_c > n_pre) {
+                const size_t old_n = cands->size();
+                cands->resize(old_n + (size_t)(n_c - n_pre));
+                CS_CUDA(cudaMemcpy(cands->data() + old_n, H->d_cands.as<DevCand>() + n_pre,
+                                   (size_t)(n_c - n_pre) * sizeof(DevCand), cudaMemcpyDeviceToHost),
+                        "read candidates");
+            }
             S.d2h_bytes += (int64_t)n_c * (int64_t)sizeof(DevCand);
         }
         if (R.keep_diag) {
             CS_CUDA(cudaMemcpy(H->last_sigma.data() + (size_t)c0 * nlev, H->d_sigma.p,
                                (size_t)nb * nlev * sizeof(float), cudaMemcpyDeviceToHost),
                     "read sigma");
-            std::copy(nvalid.begin(), nvalid.end(), H->last_nvalid.begin() + (size_t)c0 * nlev);
+            std::copy(nvalid, nvalid + (size_t)nb * nlev, H->last_nvalid.begin() + (size_t)c0 * nlev);
             S.d2h_bytes += (int64_t)nb * nlev * (int64_t)sizeof(float);
             if (R.exact_all)
                 CS_CUDA(cudaMemcpy(H->last_tmetric.data() + (size_t)c0 * nlev * Nprof, H->d_tmetric.p,
@@ -694,6 +737,8 @@ cs_status cs_destroy(cs_handle* H) {
                     &H->d_ctab, &H->d_nvalid, &H->d_X, &H->d_Q0, &H->d_sigma,
                     &H->d_tmetric, &H->d_items, &H->d_counts, &H->d_cands};
     for (DBuf* b : bufs) b->release();
+    H->h_nvalid.release();
+    H->h_io.release();
     for (auto& ev : H->ev)
         if (ev) cudaEventDestroy(ev);
     if (H->own_stream) cudaStreamDestroy(H->own_stream);

@@ -91,7 +91,7 @@ struct WaveArgs {
     int32_t tiles_per_blk;
     int32_t fp16;           // A-tile format: 1 = FP16, 0 = BF16
     float2* samp;           // [nblk][nlev][kSampStride]: pooled columns' amplitudes, [jh-1][slot]
-    float* Q0;              // [nblk][nlev][Nprof] zero-baseline gate (unscaled by 1/sigma)
+    float* Q0;              // [nblk][nlev][Nprof] zero-baseline gate (unscaled by 1/sigma); diagnostics only, may be null
     float* sigma;           // [nblk][nlev]
     float* tmetric;         // [nblk][nlev][Nprof] exact metrics (exact_all mode) or nullptr
     DevItem* items;         // rescue list
@@ -215,6 +215,49 @@ __device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_
                  ::"r"(dst), "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+
+// ---------------------------------------------------------------------------
+// Candidates and the medcut test of a gate value (boxcar_metrics!,
+// src/search.jl:825-843), shared by both synthesis kernels' epilogues.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void push_cand(const WaveArgs& a, int blk, int l, int j, float metric) {
+    const int pos = atomicAdd(a.n_cands, 1);
+    if (pos < a.cap_cands) {
+        DevCand c;
+        c.blk = a.blk_base + blk;
+        c.lev = l;
+        c.j = j;
+        c.metric = metric;
+        a.cands[pos] = c;
+    }
+}
+
+__device__ __forceinline__ float inv_sigma(float sig) { return sig > 0.0f ? 1.0f / sig : 0.0f; }
+
+// Gate value g (zero-baseline boxcar maximum, not yet divided by sigma) of
+// valid trial j: at or above medcut_gate it goes to the rescan list, else its
+// gate S/N is final (a candidate only if above threshold).
+// invsig = inv_sigma(sigma of (blk, l)), loaded by the caller ahead of time.
+__device__ __forceinline__ void gate_flag(const WaveArgs& a, int blk, int l, int j, float g, float invsig) {
+    if (!(invsig > 0.0f)) {
+        if (0.0f > a.threshold) push_cand(a, blk, l, j, 0.0f);
+        return;
+    }
+    const float m0 = g * invsig;
+    if (m0 >= a.medcut_gate) {
+        const int pos = atomicAdd(a.n_items, 1);
+        if (pos < a.cap_items) {
+            DevItem it;
+            it.blk = blk;
+            it.lev = l;
+            it.j = j;
+            it.pad = 0;
+            a.items[pos] = it;
+        }
+    } else if (m0 > a.threshold) {
+        push_cand(a, blk, l, j, m0);
+    }
+}
 #endif  // __CUDACC__
 
 cudaError_t launch_interp(const WaveArgs& a, cudaStream_t st, int win_max, int* err);
@@ -222,7 +265,6 @@ cudaError_t launch_synth_fp32(const WaveArgs& a, cudaStream_t st, int smem_bytes
 size_t sigma_smem(int max_hk, int max_np);
 size_t interp_smem(int win_max, int Nprof);
 cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np, int* err);
-cudaError_t launch_flag(const WaveArgs& a, cudaStream_t st);
 cudaError_t launch_rescue(const WaveArgs& a, cudaStream_t st, int num_sms);
 size_t synth_fp32_smem(int nharms, int maxbins, int maxwmax);
 

@@ -1,14 +1,17 @@
-// cs_kernels.cu -- sm_100a kernels of the coherent-search hot path.
+// cs_kernels.cu -- sm_100a kernels of the coherent-search hot path, in launch order.
 //
 //   k_interp       Eqn-30 direct interpolation of every harmonic's complex
 //                  amplitude (fill_harmonic_row_direct!, src/directinterp.jl:470-572;
-//                  per-trial fallback _fill_row_direct_slow!, :623-661).
+//                  per-trial fallback _fill_row_direct_slow!, :623-661); writes
+//                  X rows (plain form) or 16-bit A tiles (tensor form) and the
+//                  exact amplitudes of the columns the block sigma pools.
+//   k_sigma        block sigma (_block_sigma, src/search.jl:490-566): exact FP32
+//                  profiles of the pooled columns and their exact median.
 //   k_synth_fp32   profile synthesis for every decimation level (the brfft of
 //                  src/search.jl:1291 and :1675) + zero-baseline boxcar gate
-//                  (_boxcar_gate!, src/search.jl:784-807) + the |x| samples the
-//                  block sigma pools (_block_sigma, src/search.jl:490-566).
-//   k_sigma        exact median of the pooled samples per (block, level).
-//   k_flag         medcut test of the gate (boxcar_metrics!, src/search.jl:825-843).
+//                  (_boxcar_gate!, src/search.jl:784-807) + medcut test
+//                  (boxcar_metrics!, src/search.jl:825-843).  The tcgen05 form
+//                  of this stage is k_synth_tc (cs_synth_tc.cu).
 //   k_rescue       exact median-baseline rescan (_boxcar_exact, src/search.jl:893-904)
 //                  and candidate emission (src/search.jl:1827-1838, :1695-1708).
 #include "cs_internal.h"
@@ -551,6 +554,7 @@ __global__ void __launch_bounds__(2 * kTileTrials) k_synth_fp32(WaveArgs a) {
         const int k = L.k, Hk = L.Hk, nbins = L.nbins, wmax = L.wmax, np = L.np, nw = L.nw;
         const int nv = a.nvalid[blk * a.nlev + l];
         if (tile * TT >= nv) continue;  // uniform: nothing valid in this tile
+        const float invsig = inv_sigma(a.sigma[blk * a.nlev + l]);   // used by the medcut test below
         const int OFF = wmax + 1;
         const float* C2 = a.tw + L.tw_off;
         const float* S2 = C2 + (int64_t)Hk * np;
@@ -588,8 +592,11 @@ __global__ void __launch_bounds__(2 * kTileTrials) k_synth_fp32(WaveArgs a) {
         }
         red[half][t] = best;
         __syncthreads();
-        if (half == 0 && j < nv)
-            a.Q0[((int64_t)blk * a.nlev + l) * a.Nprof + j] = fmaxf(red[0][t], red[1][t]);
+        if (half == 0 && j < nv) {
+            const float g = fmaxf(red[0][t], red[1][t]);
+            if (a.Q0) a.Q0[((int64_t)blk * a.nlev + l) * a.Nprof + j] = g;
+            gate_flag(a, blk, l, j, g, invsig);
+        }
         __syncthreads();
     }
 }
@@ -827,58 +834,6 @@ cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max
 // ---------------------------------------------------------------------------
 // Gate test and exact rescan
 // ---------------------------------------------------------------------------
-
-__device__ __forceinline__ void push_cand(const WaveArgs& a, int blk, int l, int j, float metric) {
-    const int pos = atomicAdd(a.n_cands, 1);
-    if (pos < a.cap_cands) {
-        DevCand c;
-        c.blk = a.blk_base + blk;
-        c.lev = l;
-        c.j = j;
-        c.metric = metric;
-        a.cands[pos] = c;
-    }
-}
-
-__device__ __forceinline__ float inv_sigma(float sig) { return sig > 0.0f ? 1.0f / sig : 0.0f; }
-
-// medcut test of the gate (boxcar_metrics!, src/search.jl:825-843).
-__global__ void __launch_bounds__(256) k_flag(WaveArgs a) {
-    const int64_t n_all = (int64_t)a.nblk * a.nlev * a.Nprof;
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n_all;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int j = (int)(idx % a.Nprof);
-        const int bl = (int)(idx / a.Nprof);
-        if (j >= a.nvalid[bl]) continue;
-        const int l = bl % a.nlev, blk = bl / a.nlev;
-        const float invsig = inv_sigma(a.sigma[bl]);
-        if (!(invsig > 0.0f)) {
-            if (0.0f > a.threshold) push_cand(a, blk, l, j, 0.0f);
-            continue;
-        }
-        const float m0 = a.Q0[idx] * invsig;
-        if (m0 >= a.medcut_gate) {
-            const int pos = atomicAdd(a.n_items, 1);
-            if (pos < a.cap_items) {
-                DevItem it;
-                it.blk = blk;
-                it.lev = l;
-                it.j = j;
-                it.pad = 0;
-                a.items[pos] = it;
-            }
-        } else if (m0 > a.threshold) {
-            push_cand(a, blk, l, j, m0);
-        }
-    }
-}
-
-cudaError_t launch_flag(const WaveArgs& a, cudaStream_t st) {
-    const int64_t n_all = (int64_t)a.nblk * a.nlev * a.Nprof;
-    const int grid = (int)(((n_all + 255) / 256) < 148 * 16 ? ((n_all + 255) / 256) : 148 * 16);
-    k_flag<<<grid, 256, 0, st>>>(a);
-    return cudaGetLastError();
-}
 
 constexpr int kRescueWarps = 4;
 

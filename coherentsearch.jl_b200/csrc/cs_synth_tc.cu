@@ -182,6 +182,8 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     __shared__ TcLevel lev_sh[kMaxLevels];
     __shared__ TcUnit unit_sh[kMaxUnits];
     __shared__ float part_sh[kMaxUnits][kTM];   // per-unit gate partials of the tile
+    __shared__ float inv_sh[kMaxLevels];        // 1/sigma of the tile's block, per level
+    __shared__ int nv_sh[kMaxLevels];           // valid trials of the tile's block, per level
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
@@ -221,6 +223,12 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
         const int buf = it & 1;
         const int blk = tile / tiles_per_blk;
         const int j0 = (tile % tiles_per_blk) * kTM;
+        // the block's per-level sigma and valid counts, for the epilogue (ordered
+        // by the barrier below; the previous epilogue finished at the loop's end)
+        if (tid < t.nlev) {
+            inv_sh[tid] = inv_sigma(a.sigma[blk * a.nlev + tid]);
+            nv_sh[tid] = a.nvalid[blk * a.nlev + tid];
+        }
         // Prefetch the next tile into the other buffer: its previous reader (the
         // MMA of the last iteration) has completed.
         if (tid == 0 && tile + (int)gridDim.x < ntiles)
@@ -267,20 +275,21 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
             for (int u = 0; u < t.nunit; ++u) {
                 const TcUnit& U = unit_sh[u];
                 if (U.wg != wg) continue;                               // warp-uniform
-                if (j0 >= a.nvalid[blk * a.nlev + U.lev]) continue;     // warp-uniform
+                if (j0 >= nv_sh[U.lev]) continue;                       // warp-uniform
                 const TcLevel& L = lev_sh[U.lev];
                 part_sh[u][row] = gate_dispatch<HM>(lane_base + (uint32_t)U.col, U.nstart, U.pw, L.wmask, L.rsq);
             }
             __syncthreads();
-            // Q0 = max over the level's units.
+            // gate = max over the level's units, then the medcut test
             for (int idx = tid; idx < t.nlev * kTM; idx += blockDim.x) {
                 const int l = idx / kTM, r = idx % kTM;
                 const int j = j0 + r;
-                if (j >= a.nvalid[blk * a.nlev + l]) continue;
+                if (j >= nv_sh[l]) continue;
                 float g = -INFINITY;
                 for (int u = 0; u < t.nunit; ++u)
                     if (unit_sh[u].lev == l) g = fmaxf(g, part_sh[u][r]);
-                a.Q0[((int64_t)blk * a.nlev + l) * a.Nprof + j] = g;
+                if (a.Q0) a.Q0[((int64_t)blk * a.nlev + l) * a.Nprof + j] = g;
+                gate_flag(a, blk, l, j, g, inv_sh[l]);
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

@@ -85,9 +85,9 @@ typedef struct cs_stats {
     int64_t waves;           /* device passes the blocks were split into */
     int64_t launches;        /* kernels launched by the last call */
     double ms_interp;        /* CUDA-event time of each stage, summed over waves */
-    double ms_synth;         /* profile synthesis + gate scan */
-    double ms_sigma;
-    double ms_rescue;        /* flag + exact rescan */
+    double ms_synth;         /* profile synthesis + gate scan + medcut test */
+    double ms_sigma;         /* block sigma (runs before the synthesis) */
+    double ms_rescue;        /* exact rescan of the flagged trials */
     double ms_total;         /* first to last event of the call */
     int64_t h2d_bytes;       /* host->device bytes the call copied */
     int64_t d2h_bytes;       /* device->host bytes the call copied */

@@ -71,6 +71,13 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float v[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Three-input maximum (sm_100 max.f32 a, b, c): exact, like two fmaxf.
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
 // Zero-baseline gate of one level streamed out of TMEM: wrapped prefix sums
 // ps[e] over the level's columns (nbins bins, then its first wmax bins again,
 // then zero padding to a multiple of HM), ring[e mod HM] holding the prefix at
@@ -93,6 +100,29 @@ struct GateScan {
         ps = 0.0f;
         wm = MASK ? MASK : runtime_mask;
     }
+    // Two bins at columns e_bin, e_bin+1 (ring slots SLOT, SLOT+1): the same
+    // adds as two single steps, each width's maximum taken over both columns
+    // by one three-input max.  FAST: both columns lie before the profile's
+    // last bin, so the ring takes the prefix sums without a test.
+    template <int SLOT, bool FAST>
+    __device__ __forceinline__ void step2(float x0, float x1, int e_bin, int nbins) {
+        const float ps0 = ps + x0;
+        const float ps1 = ps0 + x1;
+        const float r0 = FAST ? ps0 : ((e_bin + 1 < nbins) ? ps0 : INFINITY);
+        const float r1 = FAST ? ps1 : ((e_bin + 2 < nbins) ? ps1 : INFINITY);
+#pragma unroll
+        for (int w = 1; w <= HM; ++w) {
+            const bool on = MASK ? ((MASK >> (w - 1)) & 1u) : ((wm >> (w - 1)) & 1u);
+            if (on) {
+                const float d0 = ps0 - ring[(SLOT - w + HM) % HM];
+                const float d1 = ps1 - (w == 1 ? r0 : ring[(SLOT + 1 - w + HM) % HM]);
+                mw[w - 1] = fmax3(mw[w - 1], d0, d1);
+            }
+        }
+        ring[SLOT % HM] = r0;
+        ring[(SLOT + 1) % HM] = r1;
+        ps = ps1;
+    }
     // One bin at column e_bin, whose ring slot of position e_bin+1 is SLOT.
     template <int SLOT>
     __device__ __forceinline__ void step(float x, int e_bin, int nbins) {
@@ -113,6 +143,18 @@ struct GateScan {
         }
         return best;
     }
+};
+
+template <int U, int N, bool FAST, class G>
+struct Unroll2 {
+    __device__ __forceinline__ static void run(G& g, const float* x, int base, int nbins) {
+        g.template step2<U + 1, FAST>(x[U], x[U + 1], base + U, nbins);
+        Unroll2<U + 2, N, FAST, G>::run(g, x, base, nbins);
+    }
+};
+template <int N, bool FAST, class G>
+struct Unroll2<N, N, FAST, G> {
+    __device__ __forceinline__ static void run(G&, const float*, int, int) {}
 };
 
 template <int U, int N, class G>
@@ -137,12 +179,15 @@ __device__ __noinline__ float gate_level(uint32_t tcol, int nbins, int pw, uint3
         if (c0 + 32 <= pw) {
             float x[32];
             tmem_ld32(tcol + c0, x);
-            Unroll<0, 32, GateScan<HM, MASK>>::run(g, x, c0, nbins);
+            if (c0 + 32 < nbins)
+                Unroll2<0, 32, true, GateScan<HM, MASK>>::run(g, x, c0, nbins);
+            else
+                Unroll2<0, 32, false, GateScan<HM, MASK>>::run(g, x, c0, nbins);
         } else {
             for (int c1 = c0; c1 < pw; c1 += 8) {   // HM == 8 here: pw is a multiple of 8
                 float x[8];
                 tmem_ld8(tcol + c1, x);
-                Unroll<0, 8, GateScan<HM, MASK>>::run(g, x, c1, nbins);
+                Unroll2<0, 8, false, GateScan<HM, MASK>>::run(g, x, c1, nbins);
             }
         }
     }
@@ -182,6 +227,7 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     __shared__ TcLevel lev_sh[kMaxLevels];
     __shared__ TcUnit unit_sh[kMaxUnits];
     __shared__ float part_sh[kMaxUnits][kTM];   // per-unit gate partials of the tile
+    __shared__ uint8_t lu_start[kMaxLevels + 1], lu_idx[kMaxUnits];
     __shared__ float inv_sh[kMaxLevels];        // 1/sigma of the tile's block, per level
     __shared__ int nv_sh[kMaxLevels];           // valid trials of the tile's block, per level
 
@@ -195,6 +241,16 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     for (int i = tid; i < bwords; i += blockDim.x) reinterpret_cast<uint4*>(Bs)[i] = Bg[i];
     if (tid < t.nlev) lev_sh[tid] = t.lev[tid];
     if (tid < t.nunit) unit_sh[tid] = t.unit[tid];
+    if (tid == 0) {
+        // each level's units, listed contiguously, for the per-level gate maximum
+        int c = 0;
+        for (int l = 0; l < t.nlev; ++l) {
+            lu_start[l] = (uint8_t)c;
+            for (int u = 0; u < t.nunit; ++u)
+                if (t.unit[u].lev == l) lu_idx[c++] = (uint8_t)u;
+        }
+        lu_start[t.nlev] = (uint8_t)c;
+    }
     if (tid == 0) {
         mbar_init(&mbar, 1);
         mbar_init(&lbar[0], 1);
@@ -286,8 +342,7 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
                 const int j = j0 + r;
                 if (j >= nv_sh[l]) continue;
                 float g = -INFINITY;
-                for (int u = 0; u < t.nunit; ++u)
-                    if (unit_sh[u].lev == l) g = fmaxf(g, part_sh[u][r]);
+                for (int i = lu_start[l]; i < lu_start[l + 1]; ++i) g = fmaxf(g, part_sh[lu_idx[i]][r]);
                 if (a.Q0) a.Q0[((int64_t)blk * a.nlev + l) * a.Nprof + j] = g;
                 gate_flag(a, blk, l, j, g, inv_sh[l]);
             }

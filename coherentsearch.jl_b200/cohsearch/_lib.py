@@ -87,6 +87,8 @@ PROTOTYPES = {
     "cs_set_spectrum": (_i32, [_P, _P, _i64, _i64, _f64]),
     "cs_set_spectrum_device": (_i32, [_P, _P, _i64, _i64, _f64]),
     "cs_search": (_i32, [_P, _f64, _f64, _i64, _i64, _f64, _i32, _P, _i64, ctypes.POINTER(_i64)]),
+    "cs_search_range": (_i32, [_P, _f64, _f64, _i64, _i64, _f64, _i32, _i64, _i64, _P, _i64,
+                               ctypes.POINTER(_i64)]),
     "cs_search_stats": (_i32, [_P, ctypes.POINTER(cs_stats)]),
     "cs_chunk_metrics": (_i32, [_P, _f64, _i64, _P]),
     "cs_interp_chunk": (_i32, [_P, _f64, _i64, _i64, _P]),

@@ -244,7 +244,9 @@ class Engine:
 
     # -- calls ------------------------------------------------------------
     def search_raw(self, lofreq=0.1, hifreq=100.0, lobin=100, blocksize=2048, threshold=None,
-                   exact_all=False, cap=1 << 16) -> np.ndarray:
+                   exact_all=False, cap=1 << 16, blocks=None) -> np.ndarray:
+        """Raw detections of the band (cs_search), or of the block range
+        `blocks = (begin, end)` of the band's grid (cs_search_range)."""
         thr = self.params.threshold if threshold is None else threshold
         while True:
             # one reusable output array per engine: no per-call zero fill
@@ -252,9 +254,14 @@ class Engine:
                 self._cand_buf = np.empty(cap, dtype=_lib.CAND_DTYPE)
             out = self._cand_buf
             n = ctypes.c_int64()
-            st = self.lib.cs_search(self._h, float(lofreq), float(hifreq), int(lobin), int(blocksize),
-                                    float(thr), int(bool(exact_all)), out.ctypes.data, cap,
-                                    ctypes.byref(n))
+            if blocks is None:
+                st = self.lib.cs_search(self._h, float(lofreq), float(hifreq), int(lobin), int(blocksize),
+                                        float(thr), int(bool(exact_all)), out.ctypes.data, cap,
+                                        ctypes.byref(n))
+            else:
+                st = self.lib.cs_search_range(self._h, float(lofreq), float(hifreq), int(lobin), int(blocksize),
+                                              float(thr), int(bool(exact_all)), int(blocks[0]), int(blocks[1]),
+                                              out.ctypes.data, cap, ctypes.byref(n))
             if st == _lib.CS_ERR_CAPACITY and n.value > cap:
                 cap = int(n.value)
                 continue

@@ -783,9 +783,10 @@ cs_status cs_set_spectrum_device(cs_handle* H, const float* d_amps, int64_t namp
     return CS_OK;
 }
 
-cs_status cs_search(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
-                    double threshold, int32_t exact_all, cs_candidate* out, int64_t cap, int64_t* n_out) {
-    if (!H || !n_out || (cap > 0 && !out) || cap < 0) return CS_ERR_INVALID_ARGUMENT;
+cs_status cs_search_range(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
+                          double threshold, int32_t exact_all, int64_t block_begin, int64_t block_end,
+                          cs_candidate* out, int64_t cap, int64_t* n_out) {
+    if (!H || !n_out || (cap > 0 && !out) || cap < 0 || block_begin < 0) return CS_ERR_INVALID_ARGUMENT;
     *n_out = 0;
     if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");
     CS_CUDA(cudaSetDevice(H->device), "set device");
@@ -803,13 +804,19 @@ cs_status cs_search(cs_handle* H, double lofreq, double hifreq, int64_t lobin, i
     if (total == 0) return CS_OK;
     const int Nprof = (int)std::max<int64_t>(1, blocksize);
     if (blocksize > (1 << 16)) return fail(H, CS_ERR_UNSUPPORTED, "blocksize above 65536 is not built");
+    // Blocks [block_begin, block_end) of the band's grid (block_end < 0: to the
+    // end); the trial anchor stays r_lo, so a range reproduces exactly the
+    // blocks, sigmas and candidates of the whole search.
+    const int64_t nblk_all = (total + Nprof - 1) / Nprof;
+    const int64_t b1 = block_end < 0 ? nblk_all : std::min(block_end, nblk_all);
+    if (block_begin >= b1) return CS_OK;
     RunSpec R{};
     R.r_lo = r_lo;
     R.lodr = lodr;
     R.Nprof = Nprof;
-    R.nblocks = (total + Nprof - 1) / Nprof;
-    R.t_base = 0;
-    R.t_end = total;
+    R.nblocks = b1 - block_begin;
+    R.t_base = block_begin * Nprof;
+    R.t_end = std::min(total, b1 * Nprof);
     R.nlev = (int)H->levels.size();
     R.exact_all = exact_all != 0;
     R.threshold = (float)threshold;
@@ -829,7 +836,7 @@ cs_status cs_search(cs_handle* H, double lofreq, double hifreq, int64_t lobin, i
     for (int64_t i = 0; i < std::min(n, cap); ++i) {
         const DevCand& c = raw[i];
         const LevelHost& L = H->levels[c.lev];
-        const int64_t i0 = (int64_t)c.blk * Nprof;
+        const int64_t i0 = (block_begin + (int64_t)c.blk) * Nprof;
         const double rstart = r_lo + (double)i0 * lodr;
         cs_candidate o{};
         if (L.k == 1) {
@@ -848,6 +855,11 @@ cs_status cs_search(cs_handle* H, double lofreq, double hifreq, int64_t lobin, i
     *n_out = n;
     if (n > cap) return fail(H, CS_ERR_CAPACITY, "candidate array too small");
     return CS_OK;
+}
+
+cs_status cs_search(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
+                    double threshold, int32_t exact_all, cs_candidate* out, int64_t cap, int64_t* n_out) {
+    return cs_search_range(H, lofreq, hifreq, lobin, blocksize, threshold, exact_all, 0, -1, out, cap, n_out);
 }
 
 cs_status cs_search_stats(const cs_handle* H, cs_stats* out) {

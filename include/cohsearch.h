@@ -136,6 +136,16 @@ cs_status cs_search(cs_handle* h, double lofreq, double hifreq, int64_t lobin, i
                     double threshold, int32_t exact_all, cs_candidate* out, int64_t cap,
                     int64_t* n_out);
 
+/* cs_search restricted to blocks [block_begin, block_end) of the band's grid
+ * of blocksize-trial blocks (block_end < 0: through the last block).  The
+ * trial grid stays anchored at the band's start, so the blocks, their sigmas
+ * and the candidates (trial indices global to the band) are exactly those of
+ * the whole search: the unit a multi-GPU run shards over (the reference's
+ * chunk loop, src/search.jl:1768-1894, over a contiguous range of chunks). */
+cs_status cs_search_range(cs_handle* h, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
+                          double threshold, int32_t exact_all, int64_t block_begin, int64_t block_end,
+                          cs_candidate* out, int64_t cap, int64_t* n_out);
+
 /* Counters and stage timings of the last cs_search on this handle. */
 cs_status cs_search_stats(const cs_handle* h, cs_stats* out);
 

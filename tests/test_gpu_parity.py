@@ -257,3 +257,21 @@ def test_tensor_candidates_identical_to_plain(synth):
     a, b = out["fp32"], out[synth]
     assert len(a) > 0
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("synth", ["fp32", "fp16"])
+def test_block_ranges_reproduce_the_search(synth):
+    """cs_search_range over contiguous block ranges (the multi-GPU shard unit)
+    concatenates to exactly the whole search: same records, bit for bit."""
+    from cohsearch import parallel
+    amps, N, dt = multi_spectrum()
+    cs = _cs()
+    dec = cs.decimation_set(32, 4)
+    eng = _engine(cs.SearchParams(nharms=32, m=16, decimations=dec, threshold=7.0, synth=synth), amps, N, dt)
+    whole = eng.search_raw(1.0, 60.0, 100, 2048, 7.0)
+    nb = parallel.band_blocks(N, dt, 0.5, 32, 1.0, 60.0, 100, 2048)
+    for world in (2, 3):
+        parts = [eng.search_raw(1.0, 60.0, 100, 2048, 7.0, blocks=parallel.block_shard(nb, r, world))
+                 for r in range(world)]
+        assert np.array_equal(np.concatenate(parts), whole)
+    assert len(eng.search_raw(1.0, 60.0, 100, 2048, 7.0, blocks=(nb, nb + 5))) == 0

@@ -5,6 +5,8 @@ loop runs in ``libcohsearch_cuda.so`` (sm_100a) through its C ABI.
 """
 from ._lib import CohSearchError, LIB_PATH, load as load_library
 from .fileio import FFTFile, SimpleInf, freqs, write_fft
+from .metricstats import (BlockMetricStats, MetricHistogram, MetricNorm, MetricStats, build_metricnorm,
+                          hist_quantile, metricstats_summary, metricstats_windows)
 from .search import (Candidate, Engine, SearchCache, SearchParams, boxcar_widths, chunk_metrics,
                      decimation_set, ladder_boxcar_widths, proftype, remove_duplicates,
                      remove_harmonics, search, write_candidates)
@@ -13,5 +15,6 @@ __all__ = [
     "CohSearchError", "LIB_PATH", "load_library", "FFTFile", "SimpleInf", "freqs", "write_fft",
     "Candidate", "Engine", "SearchCache", "SearchParams", "boxcar_widths", "chunk_metrics",
     "decimation_set", "ladder_boxcar_widths", "proftype", "remove_duplicates", "remove_harmonics",
-    "search", "write_candidates",
+    "search", "write_candidates", "BlockMetricStats", "MetricHistogram", "MetricNorm", "MetricStats",
+    "build_metricnorm", "hist_quantile", "metricstats_summary", "metricstats_windows",
 ]

@@ -60,6 +60,14 @@ class cs_candidate(ctypes.Structure):
     ]
 
 
+class cs_block_stats(ctypes.Structure):
+    _fields_ = [("block", ctypes.c_int64), ("k", ctypes.c_int32), ("Hk", ctypes.c_int32),
+                ("nbins", ctypes.c_int32), ("pad", ctypes.c_int32), ("ngoodbins", ctypes.c_double),
+                ("flo", ctypes.c_double), ("fhi", ctypes.c_double), ("n", ctypes.c_int64),
+                ("min", ctypes.c_double), ("median", ctypes.c_double), ("mean", ctypes.c_double),
+                ("std", ctypes.c_double), ("max", ctypes.c_double)]
+
+
 CAND_DTYPE = np.dtype([("freq", "<f8"), ("metric", "<f8"), ("r", "<f8"), ("nharm", "<i4"),
                        ("k", "<i4"), ("trial", "<i8")])
 assert CAND_DTYPE.itemsize == ctypes.sizeof(cs_candidate)
@@ -98,6 +106,11 @@ PROTOTYPES = {
     "cs_set_diagnostics": (_i32, [_P, _i32]),
     "cs_search_gate_values": (_i32, [_P, _P, _i64, ctypes.POINTER(_i64)]),
     "cs_version": (ctypes.c_char_p, []),
+    "cs_set_metricstats": (_i32, [_P, _i32, _f64, _f64, _i32, _i32]),
+    "cs_get_block_stats": (_i32, [_P, _P, _i64, ctypes.POINTER(_i64)]),
+    "cs_get_metric_hists": (_i32, [_P, ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(_i32), _P, _P,
+                                   _P, _P]),
+    "cs_set_metricnorm": (_i32, [_P, _i32, _i32, _P, _P, _P, _P]),
 }
 
 _lib = None

@@ -300,6 +300,77 @@ class Engine:
                    self._h)
         return out
 
+    # -- metric statistics and normalisation (src/search.jl:1296-1643) --------------
+
+    def set_metricstats(self, ms):
+        """Collect `ms` (a MetricStats) in the following searches, or stop (None)."""
+        if ms is None:
+            st = self.lib.cs_set_metricstats(self._h, 0, 0.0, 1.0, 1, 1)
+        else:
+            st = self.lib.cs_set_metricstats(self._h, 1, float(ms.hist_lo), float(ms.hist_hi), int(ms.hist_nb),
+                                             int(ms.nwin))
+        _lib.check(st, self._h, "cs_set_metricstats")
+
+    def fetch_metricstats(self, ms):
+        """Append the last search's statistics to `ms`, as _search_region! does
+        (src/search.jl:1870-1889): blocks by (block, k), per-(k, window)
+        histograms and their per-k merges, sorted by k."""
+        from .metricstats import BlockMetricStats, MetricHistogram, merge_hists
+        n = ctypes.c_int64()
+        self.lib.cs_get_block_stats(self._h, None, 0, ctypes.byref(n))
+        recs = (_lib.cs_block_stats * max(1, n.value))()
+        _lib.check(self.lib.cs_get_block_stats(self._h, recs, n.value, ctypes.byref(n)), self._h,
+                   "cs_get_block_stats")
+        for r in recs[:n.value]:
+            ms.blocks.append(BlockMetricStats(int(r.block), int(r.k), int(r.Hk), int(r.nbins), r.ngoodbins, r.flo,
+                                              r.fhi, int(r.n), r.min, r.median, r.mean, r.std, r.max))
+        L, W, B = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        _lib.check(self.lib.cs_get_metric_hists(self._h, ctypes.byref(L), ctypes.byref(W), ctypes.byref(B), None,
+                                                None, None, None), self._h, "cs_get_metric_hists")
+        L, W, B = L.value, W.value, B.value
+        if L == 0:
+            return ms
+        ks = np.zeros(L, np.int32)
+        edges = np.zeros((L, W + 1))
+        counts = np.zeros((L, W, B), np.int64)
+        mom = np.zeros((L, W, 7))
+        _lib.check(self.lib.cs_get_metric_hists(self._h, ctypes.byref(ctypes.c_int32(L)),
+                                                ctypes.byref(ctypes.c_int32(W)), ctypes.byref(ctypes.c_int32(B)),
+                                                ks.ctypes.data, edges.ctypes.data, counts.ctypes.data,
+                                                mom.ctypes.data), self._h, "cs_get_metric_hists")
+        for i in range(L):
+            k = int(ks[i])
+            Hk = self.params.nharms // k
+            wins = []
+            for w in range(W):
+                m = mom[i, w]
+                wins.append(MetricHistogram(k, Hk, 2 * Hk, w + 1, float(edges[i, w]), float(edges[i, w + 1]),
+                                            float(ms.hist_lo), float(ms.hist_hi),
+                                            ms.hist_nb / (ms.hist_hi - ms.hist_lo), counts[i, w].copy(),
+                                            int(m[0]), int(m[1]), int(m[2]), float(m[3]), float(m[4]),
+                                            float(m[5]), float(m[6])))
+            ms.whists.extend(wins)
+            ms.hists.append(merge_hists(wins, 0, float(edges[i, 0]), float(edges[i, W])))
+        ms.hists.sort(key=lambda h: h.k)
+        ms.whists.sort(key=lambda h: (h.k, h.win))
+        return ms
+
+    def set_metricnorm(self, norm):
+        """Normalise the following searches' candidate test with `norm` (a
+        MetricNorm), or stop (None)."""
+        if norm is None:
+            _lib.check(self.lib.cs_set_metricnorm(self._h, 0, 0, None, None, None, None), self._h,
+                       "cs_set_metricnorm")
+            return
+        ks = sorted(norm.edges)
+        W = len(norm.edges[ks[0]]) - 1
+        kk = np.array(ks, np.int32)
+        e = np.array([norm.edges[k] for k in ks], np.float64)
+        lc = np.array([norm.loc[k] for k in ks], np.float64)
+        sc = np.array([norm.scale[k] for k in ks], np.float64)
+        _lib.check(self.lib.cs_set_metricnorm(self._h, len(ks), W, kk.ctypes.data, e.ctypes.data, lc.ctypes.data,
+                                              sc.ctypes.data), self._h, "cs_set_metricnorm")
+
     def chunk_metrics(self, rstart: float, n: int) -> np.ndarray:
         out = np.zeros(int(n), np.float64)
         _lib.check(self.lib.cs_chunk_metrics(self._h, float(rstart), int(n), out.ctypes.data), self._h,
@@ -345,17 +416,36 @@ def search(ft, params: SearchParams = None, lofreq=0.1, hifreq=100.0, lobin=100,
     (src/search.jl:2002-2111) on the device.
 
     ``wisdom``/``wisdom_file`` are accepted for compatibility; no FFTW plans
-    exist on the device path.  ``metricstats``/``normalize`` are not built.
+    exist on the device path.  ``metricstats`` (a MetricStats) is filled from
+    the search's exact pass; ``normalize`` runs the reference's two passes
+    (src/search.jl:2063-2094): measure the per-(k, window) noise, build the
+    MetricNorm, then detect on the normalised metric.
     """
+    from .metricstats import MetricStats, build_metricnorm
     params = SearchParams() if params is None else params
     if progress not in ("none", "text", "bar"):
         raise ValueError(f"progress must be :none, :text or :bar, got :{progress}")
-    if metricstats is not None or normalize:
-        raise NotImplementedError("metricstats/normalize are not built on the device path yet")
     thr = params.threshold if threshold is None else threshold
     eng = cache.engine_for(params, device) if cache is not None else Engine(params, device)
     eng.set_spectrum(ft)
-    raw = eng.search_raw(lofreq, hifreq, lobin, blocksize, thr)
+    try:
+        if normalize:
+            normstats = MetricStats() if metricstats is None else metricstats
+            eng.set_metricstats(normstats)
+            eng.search_raw(lofreq, hifreq, lobin, blocksize, math.inf)
+            eng.fetch_metricstats(normstats)
+            eng.set_metricstats(None)
+            eng.set_metricnorm(build_metricnorm(normstats))
+            raw = eng.search_raw(lofreq, hifreq, lobin, blocksize, thr)
+        elif metricstats is not None:
+            eng.set_metricstats(metricstats)
+            raw = eng.search_raw(lofreq, hifreq, lobin, blocksize, thr)
+            eng.fetch_metricstats(metricstats)
+        else:
+            raw = eng.search_raw(lofreq, hifreq, lobin, blocksize, thr)
+    finally:
+        eng.set_metricstats(None)
+        eng.set_metricnorm(None)
     cands = _to_candidates(raw)
     if remove:
         cands = remove_duplicates(cands, dr_tol)

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdarg>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <new>
 #include <string>
@@ -249,6 +250,20 @@ struct cs_handle {
     double plan_rlo = 0.0;
     HostPlans plans;
     int64_t plan_bytes = 0;
+    // metric statistics (MetricStats) and normalisation (MetricNorm)
+    bool ms_on = false;
+    double ms_lo = 0.0, ms_hi = 64.0;
+    int ms_nb = 3200, ms_nwin = 16;
+    std::vector<cs_block_stats> ms_blocks;
+    std::vector<double> ms_edges;     // [level][nwin+1], handle level order
+    std::vector<int64_t> ms_counts;   // [level][nwin][nb]
+    std::vector<double> ms_mom;       // [level][nwin][7]: under, over, total, sum, sumsq, vmin, vmax
+    int ms_nlev = 0;
+    bool norm_on = false;
+    int norm_nwin = 0;
+    std::vector<double> norm_edges, norm_loc, norm_scale;   // handle level order
+    DBuf d_mst, d_mwin, d_mhist, d_muo, d_norm;
+    HBuf h_mwin, h_mst;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     cs_stats stats{};
     std::vector<float> last_sigma;
@@ -392,7 +407,27 @@ struct RunSpec {
     float medcut;
     bool interp_only;     // stop after interpolation (cs_interp_chunk)
     bool keep_diag;       // keep sigma/nvalid/tmetric of the run on the host
+    bool stats = false;   // collect MetricStats (exact_all)
+    bool norm = false;    // normalised candidate test (exact_all)
+    double r_hi = 0.0;    // band end (Fourier bins) and observation time, for the
+    double T = 0.0;       // frequency windows
+    double threshold_d = 0.0;
 };
+
+// _logedges (src/search.jl:1406-1411): nwin+1 log-spaced edges over [a, b].
+void logedges(double a, double b, int nwin, double* e) {
+    a = std::max(a, std::numeric_limits<double>::min());
+    b = std::max(b, a * (1 + 1e-9));
+    const double la = std::log10(a), lb = std::log10(b);
+    for (int i = 0; i <= nwin; ++i) e[i] = std::pow(10.0, la + (lb - la) * i / nwin);
+}
+
+// _window_index (src/search.jl:1415-1416), 0-based: clamp(searchsortedlast(e, f), 1, nwin) - 1.
+int window_index(const double* e, int nwin, double f) {
+    int c = 0;
+    for (int i = 0; i <= nwin; ++i) c += e[i] <= f;
+    return std::min(std::max(c, 1), nwin) - 1;
+}
 
 cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands, float2* x_out) {
     const cs_params& p = H->p;
@@ -482,6 +517,39 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             CS_CUDA(H->d_tmetric.ensure((size_t)WB * nlev * Nprof * sizeof(float)), "alloc tmetric");
     }
     CS_CUDA(H->d_counts.ensure(4 * sizeof(int32_t)), "alloc counters");
+    const int mnw = H->ms_nwin, mnb = H->ms_nb;
+    if (R.stats) {
+        H->ms_nlev = nlev;
+        H->ms_blocks.clear();
+        H->ms_edges.assign((size_t)nlev * (mnw + 1), 0.0);
+        H->ms_mom.assign((size_t)nlev * mnw * 7, 0.0);
+        for (int l = 0; l < nlev; ++l) {
+            const double k = (double)H->dlev[l].k;
+            logedges(k * R.r_lo / R.T, k * R.r_hi / R.T, mnw, &H->ms_edges[(size_t)l * (mnw + 1)]);
+            for (int w = 0; w < mnw; ++w) {
+                H->ms_mom[((size_t)l * mnw + w) * 7 + 5] = INFINITY;
+                H->ms_mom[((size_t)l * mnw + w) * 7 + 6] = -INFINITY;
+            }
+        }
+        CS_CUDA(H->d_mhist.ensure((size_t)nlev * mnw * mnb * sizeof(unsigned long long)), "alloc histograms");
+        CS_CUDA(H->d_muo.ensure((size_t)nlev * mnw * 2 * sizeof(unsigned long long)), "alloc histogram tails");
+        CS_CUDA(cudaMemsetAsync(H->d_mhist.p, 0, (size_t)nlev * mnw * mnb * sizeof(unsigned long long), H->stream),
+                "clear histograms");
+        CS_CUDA(cudaMemsetAsync(H->d_muo.p, 0, (size_t)nlev * mnw * 2 * sizeof(unsigned long long), H->stream),
+                "clear histogram tails");
+        CS_CUDA(H->d_mst.ensure((size_t)WB * nlev * kMstFields * sizeof(double)), "alloc block stats");
+        CS_CUDA(H->d_mwin.ensure((size_t)WB * nlev * sizeof(int32_t)), "alloc block windows");
+        CS_CUDA(H->h_mwin.ensure((size_t)WB * nlev * sizeof(int32_t)), "pinned block windows");
+        CS_CUDA(H->h_mst.ensure((size_t)WB * nlev * kMstFields * sizeof(double)), "pinned block stats");
+    }
+    if (R.norm) {
+        const int nw = H->norm_nwin;
+        std::vector<double> nd;
+        nd.insert(nd.end(), H->norm_edges.begin(), H->norm_edges.begin() + (size_t)nlev * (nw + 1));
+        nd.insert(nd.end(), H->norm_loc.begin(), H->norm_loc.begin() + (size_t)nlev * nw);
+        nd.insert(nd.end(), H->norm_scale.begin(), H->norm_scale.begin() + (size_t)nlev * nw);
+        CS_CUDA(upload(H->d_norm, nd, H->stream), "upload normalisation");
+    }
 
     cs_stats& S = H->stats;
     S = cs_stats{};
@@ -555,6 +623,31 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             a.verify_gate = 1;
         }
         a.exact_all = R.exact_all ? 1 : 0;
+        a.r_lo = R.r_lo;
+        a.lodr = R.lodr;
+        a.T = R.T;
+        a.norm_thr = R.threshold_d;
+        if (R.norm) {
+            const int nw = H->norm_nwin;
+            const double* nd = H->d_norm.as<double>();
+            a.norm_edges = nd;
+            a.norm_loc = nd + (size_t)nlev * (nw + 1);
+            a.norm_scale = nd + (size_t)nlev * (nw + 1) + (size_t)nlev * nw;
+            a.norm_nwin = nw;
+        }
+        int32_t* mwin = nullptr;
+        if (R.stats) {
+            a.mst = H->d_mst.as<double>();
+            a.mwin = H->d_mwin.as<int32_t>();
+            a.mhist = H->d_mhist.as<unsigned long long>();
+            a.muo = H->d_muo.as<unsigned long long>();
+            a.hist_lo = H->ms_lo;
+            a.hist_hi = H->ms_hi;
+            a.hist_invw = (double)mnb / (H->ms_hi - H->ms_lo);   // MetricHistogram's nb / (hi - lo)
+            a.hist_nb = mnb;
+            a.hist_nwin = mnw;
+            mwin = H->h_mwin.as<int32_t>();
+        }
         int* d_err = H->d_counts.as<int32_t>() + 2;
 
         CS_CUDA(H->h_nvalid.ensure((size_t)nb * nlev * sizeof(int32_t)), "pinned valid counts");
@@ -568,8 +661,20 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
                 const int k = H->dlev[l].k;
                 nvalid[(size_t)b * nlev + l] = (k == 1) ? n : nvalid_decim(k, rstart, R.lodr, n, nyq);
                 S.profiles += nvalid[(size_t)b * nlev + l];
+                if (mwin) {
+                    // the whole block goes to the window of its centre frequency
+                    // (src/search.jl:1825-1826, :1848-1849)
+                    const double rmean = rstart + (n - 1) * R.lodr / 2;
+                    const double f = k == 1 ? rmean / R.T : (double)k * rmean / R.T;
+                    mwin[(size_t)b * nlev + l] =
+                        window_index(&H->ms_edges[(size_t)l * (mnw + 1)], mnw, f);
+                }
             }
         }
+        if (mwin)
+            CS_CUDA(cudaMemcpyAsync(H->d_mwin.p, mwin, (size_t)nb * nlev * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                    H->stream),
+                    "upload block windows");
         CS_CUDA(cudaMemsetAsync(H->d_counts.p, 0, 4 * sizeof(int32_t), H->stream), "reset counters");
         if (!R.interp_only) {
             CS_CUDA(cudaMemcpyAsync(H->d_nvalid.p, nvalid, (size_t)nb * nlev * sizeof(int32_t),
@@ -598,8 +703,15 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             }
             CS_CUDA(cudaEventRecord(H->ev[3], H->stream), "event");
             CS_CUDA(launch_rescue(a, H->stream, H->num_sms), "rescue launch");
-            CS_CUDA(cudaEventRecord(H->ev[4], H->stream), "event");
             S.launches += 1;
+            if (R.stats) {
+                CS_CUDA(launch_mstats(a, H->stream), "stats launch");
+                S.launches += 1;
+                CS_CUDA(cudaMemcpyAsync(H->h_mst.p, H->d_mst.p, (size_t)nb * nlev * kMstFields * sizeof(double),
+                                        cudaMemcpyDeviceToHost, H->stream),
+                        "read block stats");
+            }
+            CS_CUDA(cudaEventRecord(H->ev[4], H->stream), "event");
         }
         CS_CUDA(cudaMemcpyAsync(counts, H->d_counts.p, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost,
                                 H->stream),
@@ -630,6 +742,56 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             S.ms_total += ms;
         }
         S.waves += 1;
+        if (R.stats) {
+            // BlockMetricStats per (block, k) (src/search.jl:1839-1844, :1710-1717):
+            // every base-fold block, decimated blocks with a valid trial; their
+            // moments also enter the (k, window) histogram's exact accumulators.
+            const double* mst = H->h_mst.as<double>();
+            const int64_t gblk0 = R.t_base / Nprof + c0;
+            for (int b = 0; b < nb; ++b) {
+                const int64_t c = c0 + b;
+                const int64_t i0 = c * (int64_t)Nprof;
+                const int n = (int)std::min<int64_t>(Nprof, R.t_end - (R.t_base + i0));
+                const double rstart = R.r_lo + (double)(R.t_base + i0) * R.lodr;
+                const double rmean = rstart + (n - 1) * R.lodr / 2;
+                for (int l = 0; l < nlev; ++l) {
+                    const int k = H->dlev[l].k, Hk = H->dlev[l].Hk;
+                    const int nv = nvalid[(size_t)b * nlev + l];
+                    if (k > 1 && nv == 0) continue;
+                    const double* m = mst + ((size_t)b * nlev + l) * kMstFields;
+                    cs_block_stats r{};
+                    r.block = gblk0 + b + 1;
+                    r.k = k;
+                    r.Hk = Hk;
+                    r.nbins = 2 * Hk;
+                    const double half_n = (double)H->N / 2;
+                    if (k == 1) {
+                        r.ngoodbins = std::min(half_n / rmean, (double)p.nharms);
+                        r.flo = rstart / R.T;
+                        r.fhi = (rstart + (n - 1) * R.lodr) / R.T;
+                    } else {
+                        r.ngoodbins = std::min(half_n / ((double)k * rmean), (double)Hk);
+                        r.flo = (double)k * rstart / R.T;
+                        r.fhi = (double)k * (rstart + (nv - 1) * R.lodr) / R.T;
+                    }
+                    r.n = nv;
+                    r.min = m[1];
+                    r.median = m[2];
+                    r.mean = m[3];
+                    r.std = m[4];
+                    r.max = m[5];
+                    H->ms_blocks.push_back(r);
+                    double* mom = &H->ms_mom[((size_t)l * mnw + mwin[(size_t)b * nlev + l]) * 7];
+                    mom[2] += nv;
+                    mom[3] += m[6];
+                    mom[4] += m[7];
+                    if (nv > 0) {
+                        mom[5] = std::min(mom[5], m[1]);
+                        mom[6] = std::max(mom[6], m[5]);
+                    }
+                }
+            }
+        }
         if (R.interp_only) {
             if (x_out)
                 CS_CUDA(cudaMemcpy(x_out, H->d_X.p, (size_t)nb * p.nharms * Nprof * sizeof(float2),
@@ -678,6 +840,21 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
                     }
             }
         }
+    }
+    if (R.stats) {
+        std::vector<unsigned long long> cnt((size_t)nlev * mnw * mnb), uo((size_t)nlev * mnw * 2);
+        CS_CUDA(cudaMemcpy(cnt.data(), H->d_mhist.p, cnt.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
+                "read histograms");
+        CS_CUDA(cudaMemcpy(uo.data(), H->d_muo.p, uo.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
+                "read histogram tails");
+        H->ms_counts.assign(cnt.begin(), cnt.end());
+        for (size_t i = 0; i < (size_t)nlev * mnw; ++i) {
+            H->ms_mom[i * 7 + 0] = (double)uo[2 * i];
+            H->ms_mom[i * 7 + 1] = (double)uo[2 * i + 1];
+        }
+        std::stable_sort(H->ms_blocks.begin(), H->ms_blocks.end(), [](const cs_block_stats& x, const cs_block_stats& y) {
+            return x.block != y.block ? x.block < y.block : x.k < y.k;
+        });
     }
     return CS_OK;
 }
@@ -739,6 +916,10 @@ cs_status cs_destroy(cs_handle* H) {
     for (DBuf* b : bufs) b->release();
     H->h_nvalid.release();
     H->h_io.release();
+    H->h_mwin.release();
+    H->h_mst.release();
+    DBuf* mbufs[] = {&H->d_mst, &H->d_mwin, &H->d_mhist, &H->d_muo, &H->d_norm};
+    for (DBuf* b : mbufs) b->release();
     for (auto& ev : H->ev)
         if (ev) cudaEventDestroy(ev);
     if (H->own_stream) cudaStreamDestroy(H->own_stream);
@@ -818,10 +999,16 @@ cs_status cs_search_range(cs_handle* H, double lofreq, double hifreq, int64_t lo
     R.t_base = block_begin * Nprof;
     R.t_end = std::min(total, b1 * Nprof);
     R.nlev = (int)H->levels.size();
-    R.exact_all = exact_all != 0;
+    R.stats = H->ms_on;
+    R.norm = H->norm_on;
+    // statistics and normalisation need every trial's exact metric (medcut = -Inf)
+    R.exact_all = exact_all != 0 || R.stats || R.norm;
     R.threshold = (float)threshold;
-    R.medcut = exact_all ? -INFINITY : (float)(threshold - p.boxcar_medmargin);
+    R.threshold_d = threshold;
+    R.medcut = R.exact_all ? -INFINITY : (float)(threshold - p.boxcar_medmargin);
     R.keep_diag = H->diag >= 1;
+    R.r_hi = r_hi;
+    R.T = T;
     std::vector<DevCand> raw;
     cs_status st = run_blocks(H, R, &raw, nullptr);
     if (st != CS_OK) return st;
@@ -848,6 +1035,12 @@ cs_status cs_search_range(cs_handle* H, double lofreq, double hifreq, int64_t lo
         }
         o.freq = o.r / T;
         o.metric = (double)c.metric;
+        if (R.norm) {
+            // z of the normalised test, with the device's FP64 expressions
+            const int nw = H->norm_nwin;
+            const int w = window_index(&H->norm_edges[(size_t)c.lev * (nw + 1)], nw, o.freq);
+            o.metric = ((double)c.metric - H->norm_loc[(size_t)c.lev * nw + w]) / H->norm_scale[(size_t)c.lev * nw + w];
+        }
         o.k = L.k;
         o.trial = i0 + c.j;
         out[i] = o;
@@ -860,6 +1053,85 @@ cs_status cs_search_range(cs_handle* H, double lofreq, double hifreq, int64_t lo
 cs_status cs_search(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
                     double threshold, int32_t exact_all, cs_candidate* out, int64_t cap, int64_t* n_out) {
     return cs_search_range(H, lofreq, hifreq, lobin, blocksize, threshold, exact_all, 0, -1, out, cap, n_out);
+}
+
+cs_status cs_set_metricstats(cs_handle* H, int32_t enable, double hist_lo, double hist_hi, int32_t hist_nb,
+                             int32_t nwin) {
+    if (!H) return CS_ERR_INVALID_ARGUMENT;
+    if (enable) {
+        // MetricHistogram's checks (src/search.jl:1397-1398) plus a bounded size
+        if (!(hist_hi > hist_lo)) return fail(H, CS_ERR_INVALID_ARGUMENT, "histogram hi must exceed lo");
+        if (hist_nb < 1 || hist_nb > (1 << 20)) return fail(H, CS_ERR_INVALID_ARGUMENT, "histogram bin count must be >= 1");
+        if (nwin < 1 || nwin > 4096) return fail(H, CS_ERR_INVALID_ARGUMENT, "window count must be 1..4096");
+        H->ms_lo = hist_lo;
+        H->ms_hi = hist_hi;
+        H->ms_nb = hist_nb;
+        H->ms_nwin = nwin;
+    }
+    H->ms_on = enable != 0;
+    return CS_OK;
+}
+
+cs_status cs_get_block_stats(const cs_handle* H, cs_block_stats* out, int64_t cap, int64_t* n_out) {
+    if (!H || !n_out) return CS_ERR_INVALID_ARGUMENT;
+    const int64_t n = (int64_t)H->ms_blocks.size();
+    *n_out = n;
+    if (cap < n) return CS_ERR_CAPACITY;
+    if (out) std::copy(H->ms_blocks.begin(), H->ms_blocks.end(), out);
+    return CS_OK;
+}
+
+cs_status cs_get_metric_hists(const cs_handle* H, int32_t* nlev, int32_t* nwin, int32_t* nb, int32_t* ks,
+                              double* edges, int64_t* counts, double* moments) {
+    if (!H || !nlev || !nwin || !nb) return CS_ERR_INVALID_ARGUMENT;
+    const int L = H->ms_nlev, W = H->ms_nwin, B = H->ms_nb;
+    *nlev = L;
+    *nwin = W;
+    *nb = B;
+    if (H->ms_counts.size() != (size_t)L * W * B) {   // no statistics collected yet
+        *nlev = 0;
+        return CS_OK;
+    }
+    // levels in ascending k (the reference sorts its histograms by k)
+    std::vector<int> order(L);
+    for (int l = 0; l < L; ++l) order[l] = l;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return H->dlev[x].k < H->dlev[y].k; });
+    for (int i = 0; i < L; ++i) {
+        const int l = order[i];
+        if (ks) ks[i] = H->dlev[l].k;
+        if (edges) std::copy_n(&H->ms_edges[(size_t)l * (W + 1)], W + 1, edges + (size_t)i * (W + 1));
+        if (counts) std::copy_n(&H->ms_counts[(size_t)l * W * B], (size_t)W * B, counts + (size_t)i * W * B);
+        if (moments) std::copy_n(&H->ms_mom[(size_t)l * W * 7], (size_t)W * 7, moments + (size_t)i * W * 7);
+    }
+    return CS_OK;
+}
+
+cs_status cs_set_metricnorm(cs_handle* H, int32_t nlev, int32_t nwin, const int32_t* ks, const double* edges,
+                            const double* loc, const double* scale) {
+    if (!H) return CS_ERR_INVALID_ARGUMENT;
+    if (nlev == 0) {
+        H->norm_on = false;
+        return CS_OK;
+    }
+    if (nlev < 0 || nwin < 1 || !ks || !edges || !loc || !scale)
+        return fail(H, CS_ERR_INVALID_ARGUMENT, "normalisation needs ks, edges, loc and scale");
+    const int L = (int)H->dlev.size();
+    std::vector<double> e((size_t)L * (nwin + 1)), lc((size_t)L * nwin), sc((size_t)L * nwin);
+    for (int l = 0; l < L; ++l) {
+        int src = -1;
+        for (int i = 0; i < nlev; ++i)
+            if (ks[i] == H->dlev[l].k) src = i;
+        if (src < 0) return fail(H, CS_ERR_INVALID_ARGUMENT, "normalisation lacks a decimation factor of the search");
+        std::copy_n(edges + (size_t)src * (nwin + 1), nwin + 1, &e[(size_t)l * (nwin + 1)]);
+        std::copy_n(loc + (size_t)src * nwin, nwin, &lc[(size_t)l * nwin]);
+        std::copy_n(scale + (size_t)src * nwin, nwin, &sc[(size_t)l * nwin]);
+    }
+    H->norm_edges.swap(e);
+    H->norm_loc.swap(lc);
+    H->norm_scale.swap(sc);
+    H->norm_nwin = nwin;
+    H->norm_on = true;
+    return CS_OK;
 }
 
 cs_status cs_search_stats(const cs_handle* H, cs_stats* out) {

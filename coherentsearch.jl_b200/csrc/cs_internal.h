@@ -105,7 +105,26 @@ struct WaveArgs {
     float medcut_gate;    // the flag kernel's cut: medcut, less a slack for 16-bit gates
     int32_t verify_gate;  // rescan recomputes the FP32 gate and applies medcut itself
     int32_t exact_all;
+    // Metric statistics (exact_all mode; the reference's MetricStats sink):
+    // per (block, level) moments and the per-(level, window) histograms.
+    double* mst;              // [nblk][nlev][kMstFields] or nullptr
+    const int32_t* mwin;      // [nblk][nlev] window of the block's centre frequency
+    unsigned long long* mhist;  // [nlev][nwin][hist_nb] counts
+    unsigned long long* muo;    // [nlev][nwin][2] under / over
+    double hist_lo, hist_hi, hist_invw;
+    int32_t hist_nb, hist_nwin;
+    // In-situ normalisation (MetricNorm): a trial is a candidate when
+    // z = (M - loc[l][w]) / scale[l][w] > threshold, w the window of its
+    // searched frequency k*rf/T among norm_edges[l][0..nwin].
+    const double* norm_edges;   // [nlev][norm_nwin + 1] or nullptr
+    const double* norm_loc;     // [nlev][norm_nwin]
+    const double* norm_scale;   // [nlev][norm_nwin]
+    int32_t norm_nwin;
+    double norm_thr;            // the threshold, in FP64
+    double r_lo, lodr, T;       // band anchor, trial step and observation time (FP64 frequencies)
 };
+
+constexpr int kMstFields = 8;   // n, min, median, mean, std, max, sum, sumsq
 
 // Tensor-core synthesis (cs_synth_tc.cu): per-level TMEM column layout.
 struct TcLevel {
@@ -266,6 +285,8 @@ size_t sigma_smem(int max_hk, int max_np);
 size_t interp_smem(int win_max, int Nprof);
 cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np, int* err);
 cudaError_t launch_rescue(const WaveArgs& a, cudaStream_t st, int num_sms);
+cudaError_t launch_mstats(const WaveArgs& a, cudaStream_t st);
+size_t mstats_smem(int nprof, int hist_nb);
 size_t synth_fp32_smem(int nharms, int maxbins, int maxwmax);
 
 }  // namespace cs

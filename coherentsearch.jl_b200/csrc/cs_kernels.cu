@@ -19,6 +19,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <math.h>
+#include <math_constants.h>
 
 namespace cs {
 
@@ -835,6 +836,26 @@ cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max
 // Gate test and exact rescan
 // ---------------------------------------------------------------------------
 
+// In-situ normalisation (_normalize, src/search.jl:1638-1643; the candidate
+// test of decim_pass!/_search_region!, :1704-1707, :1834-1837): the trial's
+// searched frequency f = k*(rstart + j*lodr)/T in FP64 (the host's expressions,
+// no contraction), its window w = clamp(searchsortedlast(edges, f), 1, nwin),
+// and z = (M - loc[w]) / scale[w] against the threshold.
+__device__ bool norm_pass(const WaveArgs& a, int blk, int l, int k, int j, float metric) {
+    const int64_t i0 = a.t_first + (int64_t)blk * a.Nprof;
+    const double rstart = __dadd_rn(a.r_lo, __dmul_rn((double)i0, a.lodr));
+    const double rf = __dadd_rn(rstart, __dmul_rn((double)j, a.lodr));
+    const double r = k == 1 ? rf : __dmul_rn((double)k, rf);
+    const double f = __ddiv_rn(r, a.T);
+    const int nw = a.norm_nwin;
+    const double* e = a.norm_edges + (int64_t)l * (nw + 1);
+    int w = 0;
+    for (int i = 0; i <= nw; ++i) w += e[i] <= f;   // searchsortedlast: edges <= f
+    w = min(max(w, 1), nw) - 1;
+    const double z = __ddiv_rn(__dsub_rn((double)metric, a.norm_loc[l * nw + w]), a.norm_scale[l * nw + w]);
+    return z > a.norm_thr;
+}
+
 constexpr int kRescueWarps = 4;
 
 // One warp per (block, level, trial).  Lanes recompute the exact amplitudes of
@@ -977,7 +998,8 @@ __global__ void __launch_bounds__(32 * kRescueWarps) k_rescue(WaveArgs a) {
         }
         if (lane == 0) {
             if (a.tmetric) a.tmetric[((int64_t)blk * a.nlev + l) * a.Nprof + j] = metric;
-            if (metric > a.threshold) push_cand(a, blk, l, j, metric);
+            if (a.norm_edges ? norm_pass(a, blk, l, k, j, metric) : metric > a.threshold)
+                push_cand(a, blk, l, j, metric);
         }
         __syncwarp();
     }
@@ -985,6 +1007,171 @@ __global__ void __launch_bounds__(32 * kRescueWarps) k_rescue(WaveArgs a) {
 
 cudaError_t launch_rescue(const WaveArgs& a, cudaStream_t st, int num_sms) {
     k_rescue<<<num_sms * 8, 32 * kRescueWarps, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Metric statistics (the opt-in MetricStats sink, src/search.jl:1296-1560)
+// ---------------------------------------------------------------------------
+
+constexpr int kMstSmemBins = 8192;   // histograms up to this many bins accumulate in shared memory
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One CTA per (block, level) of an exact_all wave: over the valid trials'
+// exact metrics (tmetric), the moments and exact median of _block_stats
+// (:1339-1359: two-pass std with n-1, _median! mean of the two central values)
+// and the histogram pushes of _hist_push! (:1428-1442) into the (level, window)
+// histogram of the block's centre frequency.  Sums are FP64 per block; the host
+// adds the blocks in order.
+__global__ void __launch_bounds__(256) k_mstats(WaveArgs a) {
+    extern __shared__ uint32_t msm[];
+    uint32_t* rhist = msm;          // radix histogram (2048)
+    uint32_t* hbins = msm + 2048;   // metric histogram when it fits
+    __shared__ int sh[4];
+    __shared__ int wtot[32];
+    __shared__ double dred[4][32];
+    __shared__ uint32_t ured[32];
+    const int bl = blockIdx.x;
+    const int l = bl % a.nlev;
+    const int nv = a.nvalid[bl];
+    double* out = a.mst + (int64_t)bl * kMstFields;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarp = blockDim.x >> 5;
+    if (nv <= 0) {
+        if (tid < kMstFields) out[tid] = tid == 0 ? 0.0 : CUDART_NAN;
+        return;
+    }
+    const float* v = a.tmetric + (int64_t)bl * a.Nprof;
+    const int nb = a.hist_nb;
+    const bool smh = nb <= kMstSmemBins;
+    for (int i = tid; i < (smh ? nb : 0); i += blockDim.x) hbins[i] = 0;
+    __syncthreads();
+    const int w = a.mwin[bl];
+    unsigned long long* gcount = a.mhist + ((int64_t)l * a.hist_nwin + w) * nb;
+    double s = 0.0, s2 = 0.0, mn = CUDART_INF, mx = -CUDART_INF;
+    uint32_t under = 0, over = 0;
+    for (int j = tid; j < nv; j += blockDim.x) {
+        const double x = (double)v[j];
+        s = __dadd_rn(s, x);
+        s2 = __dadd_rn(s2, __dmul_rn(x, x));
+        mn = fmin(mn, x);
+        mx = fmax(mx, x);
+        if (x < a.hist_lo) {
+            ++under;
+        } else if (x >= a.hist_hi) {
+            ++over;
+        } else {
+            int bin = (int)floor(__dmul_rn(__dsub_rn(x, a.hist_lo), a.hist_invw));
+            bin = min(bin, nb - 1);
+            if (smh) atomicAdd(&hbins[bin], 1u);
+            else atomicAdd(&gcount[bin], 1ull);
+        }
+    }
+    s = warp_sum_d(s);
+    s2 = warp_sum_d(s2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        under += __shfl_xor_sync(0xffffffffu, under, o);
+        over += __shfl_xor_sync(0xffffffffu, over, o);
+    }
+    if (lane == 0) {
+        dred[0][wid] = s;
+        dred[1][wid] = s2;
+        dred[2][wid] = mn;
+        dred[3][wid] = mx;
+        wtot[wid] = (int)under;
+        ured[wid] = over;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double ts = 0.0, ts2 = 0.0, tmn = CUDART_INF, tmx = -CUDART_INF;
+        uint32_t tu = 0, to = 0;
+        for (int q = 0; q < nwarp; ++q) {
+            ts = __dadd_rn(ts, dred[0][q]);
+            ts2 = __dadd_rn(ts2, dred[1][q]);
+            tmn = fmin(tmn, dred[2][q]);
+            tmx = fmax(tmx, dred[3][q]);
+            tu += (uint32_t)wtot[q];
+            to += ured[q];
+        }
+        out[0] = (double)nv;
+        out[1] = tmn;
+        out[5] = tmx;
+        out[6] = ts;
+        out[7] = ts2;
+        out[3] = ts / (double)nv;
+        if (tu) atomicAdd(&a.muo[((int64_t)l * a.hist_nwin + w) * 2 + 0], (unsigned long long)tu);
+        if (to) atomicAdd(&a.muo[((int64_t)l * a.hist_nwin + w) * 2 + 1], (unsigned long long)to);
+    }
+    __syncthreads();
+    for (int i = tid; i < (smh ? nb : 0); i += blockDim.x)
+        if (hbins[i]) atomicAdd(&gcount[i], (unsigned long long)hbins[i]);
+    // second pass: sum of squared deviations from the mean
+    const double mean = out[3];
+    double ss = 0.0;
+    for (int j = tid; j < nv; j += blockDim.x) {
+        const double d = __dsub_rn((double)v[j], mean);
+        ss = __dadd_rn(ss, __dmul_rn(d, d));
+    }
+    ss = warp_sum_d(ss);
+    __syncthreads();
+    if (lane == 0) dred[0][wid] = ss;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int q = 0; q < nwarp; ++q) t = __dadd_rn(t, dred[0][q]);
+        out[4] = nv > 1 ? sqrt(t / (double)(nv - 1)) : 0.0;
+    }
+    // exact median (metrics are non-negative, so their bit patterns order like them)
+    const uint32_t* vb = reinterpret_cast<const uint32_t*>(v);
+    const int half = nv >> 1;
+    double med;
+    if (nv & 1) {
+        med = (double)__uint_as_float(radix_select(vb, nv, half, rhist, sh, wtot));
+    } else {
+        const uint32_t lo = radix_select(vb, nv, half - 1, rhist, sh, wtot);
+        int le = 0;
+        uint32_t above = 0xFFFFFFFFu;
+        for (int i = tid; i < nv; i += blockDim.x) {
+            const uint32_t x = vb[i];
+            le += x <= lo;
+            if (x > lo && x < above) above = x;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            le += __shfl_xor_sync(0xffffffffu, le, o);
+            above = min(above, __shfl_xor_sync(0xffffffffu, above, o));
+        }
+        __syncthreads();
+        if (lane == 0) { wtot[wid] = le; ured[wid] = above; }
+        __syncthreads();
+        if (tid == 0) {
+            int tle = 0;
+            uint32_t tab = 0xFFFFFFFFu;
+            for (int q = 0; q < nwarp; ++q) { tle += wtot[q]; tab = min(tab, ured[q]); }
+            sh[3] = (int)(tle >= half + 1 ? lo : tab);
+        }
+        __syncthreads();
+        med = 0.5 * ((double)__uint_as_float(lo) + (double)__uint_as_float((uint32_t)sh[3]));
+    }
+    if (tid == 0) out[2] = med;
+}
+
+size_t mstats_smem(int nprof, int hist_nb) {
+    (void)nprof;
+    return (size_t)2048 * sizeof(uint32_t) + (hist_nb <= kMstSmemBins ? (size_t)hist_nb * sizeof(uint32_t) : 0);
+}
+
+cudaError_t launch_mstats(const WaveArgs& a, cudaStream_t st) {
+    const size_t smem = mstats_smem(a.Nprof, a.hist_nb);
+    cudaFuncSetAttribute(k_mstats, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_mstats<<<a.nblk * a.nlev, 256, smem, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -146,6 +146,53 @@ cs_status cs_search_range(cs_handle* h, double lofreq, double hifreq, int64_t lo
                           double threshold, int32_t exact_all, int64_t block_begin, int64_t block_end,
                           cs_candidate* out, int64_t cap, int64_t* n_out);
 
+/* ---------------------------------------------------------------------------
+ * Metric statistics and in-situ normalisation (the reference's --metricstats
+ * and --normalize: MetricStats, BlockMetricStats, MetricHistogram, MetricNorm,
+ * src/search.jl:1296-1643, collected in _search_region!/decim_pass!,
+ * :1664-1894, driven by search, :2063-2094).
+ * ------------------------------------------------------------------------- */
+
+/* One (block, k) record of BlockMetricStats (src/search.jl:1321-1335); block is
+ * the reference's 1-based chunk index of the band. */
+typedef struct cs_block_stats {
+    int64_t block;
+    int32_t k, Hk, nbins, pad;
+    double ngoodbins, flo, fhi;
+    int64_t n;
+    double min, median, mean, std, max;
+} cs_block_stats;
+
+/* enable != 0: every following cs_search / cs_search_range scores every trial
+ * exactly (medcut = -Inf, as the reference does when collecting) and collects
+ * the per-(block, k) statistics and the per-(k, window) histograms of the raw
+ * metric: hist_nb bins over [hist_lo, hist_hi), nwin log-spaced searched-
+ * frequency windows per k (MetricStats defaults: 0, 64, 3200, 16).  Candidates
+ * are unchanged. */
+cs_status cs_set_metricstats(cs_handle* h, int32_t enable, double hist_lo, double hist_hi, int32_t hist_nb,
+                             int32_t nwin);
+
+/* The last search's BlockMetricStats records, sorted by (block, k); if cap is
+ * too small, CS_ERR_CAPACITY with *n_out = the number available. */
+cs_status cs_get_block_stats(const cs_handle* h, cs_block_stats* out, int64_t cap, int64_t* n_out);
+
+/* The last search's per-(k, window) histograms (MetricHistogram, one per k
+ * and window, ks ascending).  *nlev, *nwin, *nb receive the shape; with null
+ * arrays only the shape is returned.  ks[nlev]; edges[nlev][nwin+1] (Hz);
+ * counts[nlev][nwin][nb]; moments[nlev][nwin][7] = under, over, total, sum,
+ * sumsq, vmin, vmax. */
+cs_status cs_get_metric_hists(const cs_handle* h, int32_t* nlev, int32_t* nwin, int32_t* nb, int32_t* ks,
+                              double* edges, int64_t* counts, double* moments);
+
+/* In-situ normalisation for the following searches (MetricNorm, built by the
+ * caller from a stats pass as build_metricnorm does): for decimation ks[i],
+ * window edges edges[i][0..nwin] (Hz) and per-window loc/scale[i][0..nwin-1].
+ * Every trial is scored exactly and is a candidate when its
+ * z = (M - loc) / scale > threshold; the candidate's metric is z.  nlev = 0
+ * clears it.  Each k of the handle's levels must be given. */
+cs_status cs_set_metricnorm(cs_handle* h, int32_t nlev, int32_t nwin, const int32_t* ks, const double* edges,
+                            const double* loc, const double* scale);
+
 /* Counters and stage timings of the last cs_search on this handle. */
 cs_status cs_search_stats(const cs_handle* h, cs_stats* out);
 

@@ -7,14 +7,15 @@ from ._lib import CohSearchError, LIB_PATH, load as load_library
 from .fileio import FFTFile, SimpleInf, freqs, write_fft
 from .metricstats import (BlockMetricStats, MetricHistogram, MetricNorm, MetricStats, build_metricnorm,
                           hist_quantile, metricstats_summary, metricstats_windows)
-from .search import (Candidate, Engine, SearchCache, SearchParams, boxcar_widths, chunk_metrics,
+from .search import (Candidate, Engine, SearchCache, SearchParams, block_metrics, boxcar_widths, chunk_metrics,
                      decimation_set, ladder_boxcar_widths, proftype, remove_duplicates,
-                     remove_harmonics, search, write_candidates)
+                     remove_harmonics, search, search_block, write_candidates)
 
 __all__ = [
     "CohSearchError", "LIB_PATH", "load_library", "FFTFile", "SimpleInf", "freqs", "write_fft",
     "Candidate", "Engine", "SearchCache", "SearchParams", "boxcar_widths", "chunk_metrics",
     "decimation_set", "ladder_boxcar_widths", "proftype", "remove_duplicates", "remove_harmonics",
     "search", "write_candidates", "BlockMetricStats", "MetricHistogram", "MetricNorm", "MetricStats",
-    "build_metricnorm", "hist_quantile", "metricstats_summary", "metricstats_windows",
+    "build_metricnorm", "hist_quantile", "metricstats_summary", "metricstats_windows", "block_metrics",
+    "search_block",
 ]

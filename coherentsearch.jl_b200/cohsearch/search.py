@@ -371,6 +371,20 @@ class Engine:
         _lib.check(self.lib.cs_set_metricnorm(self._h, len(ks), W, kk.ctypes.data, e.ctypes.data, lc.ctypes.data,
                                               sc.ctypes.data), self._h, "cs_set_metricnorm")
 
+    def block_metrics(self, rfund, kernel: str = "fft", widths=None) -> np.ndarray:
+        """block_metrics (src/search.jl:1061-1079) on the device, FP64."""
+        if kernel not in ("fft", "direct"):
+            raise ValueError(f"kernel must be :fft or :direct, got :{kernel}")
+        r = np.ascontiguousarray(rfund, dtype=np.float64)
+        if r.size == 0:
+            return np.zeros(0)
+        out = np.zeros(r.size, np.float64)
+        w = None if widths is None else np.ascontiguousarray(widths, dtype=np.int32)
+        _lib.check(self.lib.cs_block_metrics(self._h, r.ctypes.data, r.size, 0 if kernel == "fft" else 1,
+                                             None if w is None else w.ctypes.data, 0 if w is None else w.size,
+                                             out.ctypes.data), self._h, "cs_block_metrics")
+        return out
+
     def chunk_metrics(self, rstart: float, n: int) -> np.ndarray:
         out = np.zeros(int(n), np.float64)
         _lib.check(self.lib.cs_chunk_metrics(self._h, float(rstart), int(n), out.ctypes.data), self._h,
@@ -454,6 +468,23 @@ def search(ft, params: SearchParams = None, lofreq=0.1, hifreq=100.0, lobin=100,
     if harm_remove:
         cands = remove_harmonics(cands, numharm, harm_tol)
     return cands
+
+
+def block_metrics(ft, rfund, params: SearchParams, kernel="fft", widths=None, cache=None,
+                  device: int = 0) -> np.ndarray:
+    """Coherent-fold S/N of every trial fundamental in `rfund` through the
+    reference path (src/search.jl:1061-1079), on the device."""
+    eng = cache.engine_for(params, device) if cache is not None else Engine(params, device)
+    eng.set_spectrum(ft)
+    return eng.block_metrics(rfund, kernel, widths)
+
+
+def search_block(ft, rfund, params: SearchParams, threshold=None, cache=None, device: int = 0) -> List[Candidate]:
+    """search_block (src/search.jl:1087-1097): trials of `rfund` above threshold."""
+    thr = params.threshold if threshold is None else threshold
+    met = block_metrics(ft, rfund, params, cache=cache, device=device)
+    return [Candidate(float(rfund[j]) / ft.T, float(met[j]), float(rfund[j]), params.nharms)
+            for j in range(len(rfund)) if met[j] > thr]
 
 
 def chunk_metrics(ft, params: SearchParams, rstart: float, n: int, lodr=None, cache=None,

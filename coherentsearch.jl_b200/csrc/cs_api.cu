@@ -263,6 +263,7 @@ struct cs_handle {
     int norm_nwin = 0;
     std::vector<double> norm_edges, norm_loc, norm_scale;   // handle level order
     DBuf d_mst, d_mwin, d_mhist, d_muo, d_norm;
+    DBuf d_bm_r, d_bm_h, d_bm_st, d_bm_prof, d_bm_w, d_bm_sig, d_bm_out;   // block_metrics
     HBuf h_mwin, h_mst;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     cs_stats stats{};
@@ -918,7 +919,8 @@ cs_status cs_destroy(cs_handle* H) {
     H->h_io.release();
     H->h_mwin.release();
     H->h_mst.release();
-    DBuf* mbufs[] = {&H->d_mst, &H->d_mwin, &H->d_mhist, &H->d_muo, &H->d_norm};
+    DBuf* mbufs[] = {&H->d_mst, &H->d_mwin, &H->d_mhist, &H->d_muo, &H->d_norm, &H->d_bm_r, &H->d_bm_h,
+                     &H->d_bm_st, &H->d_bm_prof, &H->d_bm_w, &H->d_bm_sig, &H->d_bm_out};
     for (DBuf* b : mbufs) b->release();
     for (auto& ev : H->ev)
         if (ev) cudaEventDestroy(ev);
@@ -1159,6 +1161,60 @@ cs_status cs_chunk_metrics(cs_handle* H, double rstart, int64_t n, double* out) 
     cs_status st = run_blocks(H, R, nullptr, nullptr);
     if (st != CS_OK) return st;
     for (int64_t j = 0; j < n; ++j) out[j] = (double)H->last_tmetric[j];
+    return CS_OK;
+}
+
+cs_status cs_block_metrics(cs_handle* H, const double* rfund, int64_t L, int32_t kernel, const int32_t* widths,
+                           int32_t nw, double* out) {
+    if (!H || !rfund || !out || L < 1 || L > (1 << 22)) return CS_ERR_INVALID_ARGUMENT;
+    if (kernel != 0 && kernel != 1) return fail(H, CS_ERR_INVALID_ARGUMENT, "kernel must be :fft (0) or :direct (1)");
+    if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");
+    const cs_params& p = H->p;
+    const int nh = p.nharms, m = p.m, m2 = p.m / 2, nb = p.numbetween, nbins = 2 * p.nharms;
+    if (nb < 1) return fail(H, CS_ERR_INVALID_ARGUMENT, "numbetween must be >= 1");
+    if (nbins > kMaxBins) return fail(H, CS_ERR_UNSUPPORTED, "nharms > 128 is not built");
+    for (int64_t j = 0; j < L; ++j)
+        if (!(rfund[j] >= 0.0)) return fail(H, CS_ERR_INVALID_ARGUMENT, "r must be non-negative");
+    std::vector<int> ws;
+    if (widths && nw > 0) {
+        ws.assign(widths, widths + nw);
+        for (int i = 0; i < nw; ++i)
+            if (ws[i] < 1 || ws[i] > kMaxBins || (i > 0 && ws[i] <= ws[i - 1]))
+                return fail(H, CS_ERR_INVALID_ARGUMENT, "widths must ascend within 1..256");
+    } else {
+        ws = ladder_widths(nbins, 1, p);   // the base pass's bank (src/search.jl:1069-1070)
+    }
+    // reference_profiles' per-harmonic grid and guard (src/search.jl:1024-1034)
+    std::vector<BmHarm> hm(nh);
+    const int64_t Nhalf = H->N / 2;
+    for (int h = 1; h <= nh; ++h) {
+        const double rmin = rfund[0] * h, rmax = rfund[L - 1] * h;
+        const int64_t lobin = (int64_t)std::floor(rmin);
+        const int64_t hibin = (int64_t)std::ceil(rmax) + 1;
+        const int64_t numbins = hibin - lobin;
+        BmHarm& b = hm[h - 1];
+        b.lobin = lobin;
+        b.K = numbins * nb;
+        b.ok = (lobin >= m2 && lobin + numbins + m2 <= H->namps && hibin < Nhalf) ? 1 : 0;
+        b.pad = 0;
+    }
+    CS_CUDA(cudaSetDevice(H->device), "set device");
+    CS_CUDA(H->d_bm_r.ensure((size_t)L * sizeof(double)), "alloc trials");
+    CS_CUDA(H->d_bm_st.ensure((size_t)L * nh * sizeof(double2)), "alloc amplitudes");
+    CS_CUDA(H->d_bm_prof.ensure((size_t)L * nbins * sizeof(double)), "alloc profiles");
+    CS_CUDA(H->d_bm_out.ensure((size_t)L * sizeof(double)), "alloc metrics");
+    CS_CUDA(H->d_bm_sig.ensure(sizeof(double)), "alloc sigma");
+    CS_CUDA(cudaMemcpyAsync(H->d_bm_r.p, rfund, (size_t)L * sizeof(double), cudaMemcpyHostToDevice, H->stream),
+            "copy trials");
+    CS_CUDA(upload(H->d_bm_h, hm, H->stream), "copy harmonic grid");
+    CS_CUDA(upload(H->d_bm_w, ws, H->stream), "copy widths");
+    CS_CUDA(run_block_metrics(H->d_bm_r.as<double>(), (int)L, H->d_bm_h.as<BmHarm>(), nh, m, nb, kernel, H->amps,
+                              H->namps, H->d_bm_st.as<double2>(), H->d_bm_prof.as<double>(), H->d_bm_w.as<int>(),
+                              (int)ws.size(), H->d_bm_sig.as<double>(), H->d_bm_out.as<double>(), H->stream),
+            "block metrics launch");
+    CS_CUDA(cudaMemcpyAsync(out, H->d_bm_out.p, (size_t)L * sizeof(double), cudaMemcpyDeviceToHost, H->stream),
+            "read metrics");
+    CS_CUDA(cudaStreamSynchronize(H->stream), "block metrics");
     return CS_OK;
 }
 

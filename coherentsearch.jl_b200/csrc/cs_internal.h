@@ -286,6 +286,18 @@ size_t interp_smem(int win_max, int Nprof);
 cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np, int* err);
 cudaError_t launch_rescue(const WaveArgs& a, cudaStream_t st, int num_sms);
 cudaError_t launch_mstats(const WaveArgs& a, cudaStream_t st);
+
+// block_metrics (reference path): per harmonic, the fine-grid origin, its
+// length (numbins * numbetween) and the reference's range guard.
+struct BmHarm {
+    int64_t lobin;
+    int64_t K;
+    int32_t ok;
+    int32_t pad;
+};
+cudaError_t run_block_metrics(const double* d_rfund, int L, const BmHarm* d_hm, int nh, int m, int nb, int kernel,
+                              const float2* amps, int64_t namps, double2* d_st, double* d_prof,
+                              const int* d_widths, int nw, double* d_sigma, double* d_out, cudaStream_t st);
 size_t mstats_smem(int nprof, int hist_nb);
 size_t synth_fp32_smem(int nharms, int maxbins, int maxwmax);
 

@@ -229,6 +229,16 @@ cs_status cs_chunk_metrics_static(const cs_params* params, const float* d_amps, 
                                   double rstart, int64_t n, float* d_out, void* stream, char* err,
                                   int64_t err_cap);
 
+/* Reference path `block_metrics(ft, rfund, params; kernel, widths)`
+ * (src/search.jl:1061-1079, with reference_profiles :1011-1049 and snr_metrics
+ * :933-951): the coherent-fold S/N of each of the L trial fundamentals rfund
+ * (Fourier bins, ascending, >= 0; any values, not a grid), FP64 throughout.
+ * kernel 0 = :fft (finterp_fft on the numbetween grid + linear interpolation),
+ * 1 = :direct (Eqn 30 at each point).  widths NULL or nw = 0: the base pass's
+ * ladder bank. */
+cs_status cs_block_metrics(cs_handle* h, const double* rfund, int64_t L, int32_t kernel, const int32_t* widths,
+                           int32_t nw, double* out);
+
 /* Interpolated amplitude stack of a chunk (the `ftprofs` rows of
  * fill_chunk_profiles!, src/search.jl:1280-1290, and fill_harmonic_row_direct!,
  * src/directinterp.jl:470-572): trials t0 .. t0+n-1 of a search whose global

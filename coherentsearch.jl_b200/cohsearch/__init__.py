@@ -9,7 +9,7 @@ from .metricstats import (BlockMetricStats, MetricHistogram, MetricNorm, MetricS
                           hist_quantile, metricstats_summary, metricstats_windows)
 from .search import (Candidate, Engine, SearchCache, SearchParams, block_metrics, boxcar_widths, chunk_metrics,
                      decimation_set, ladder_boxcar_widths, proftype, remove_duplicates,
-                     remove_harmonics, search, search_block, write_candidates)
+                     remove_harmonics, search, search_batch, search_block, write_candidates)
 
 __all__ = [
     "CohSearchError", "LIB_PATH", "load_library", "FFTFile", "SimpleInf", "freqs", "write_fft",
@@ -17,5 +17,5 @@ __all__ = [
     "decimation_set", "ladder_boxcar_widths", "proftype", "remove_duplicates", "remove_harmonics",
     "search", "write_candidates", "BlockMetricStats", "MetricHistogram", "MetricNorm", "MetricStats",
     "build_metricnorm", "hist_quantile", "metricstats_summary", "metricstats_windows", "block_metrics",
-    "search_block",
+    "search_block", "search_batch",
 ]

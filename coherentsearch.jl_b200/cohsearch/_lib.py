@@ -60,6 +60,11 @@ class cs_candidate(ctypes.Structure):
     ]
 
 
+class cs_spectrum(ctypes.Structure):
+    _fields_ = [("amps", ctypes.c_void_p), ("namps", ctypes.c_int64), ("N", ctypes.c_int64),
+                ("dt", ctypes.c_double)]
+
+
 class cs_block_stats(ctypes.Structure):
     _fields_ = [("block", ctypes.c_int64), ("k", ctypes.c_int32), ("Hk", ctypes.c_int32),
                 ("nbins", ctypes.c_int32), ("pad", ctypes.c_int32), ("ngoodbins", ctypes.c_double),
@@ -95,6 +100,8 @@ PROTOTYPES = {
     "cs_set_spectrum": (_i32, [_P, _P, _i64, _i64, _f64]),
     "cs_set_spectrum_device": (_i32, [_P, _P, _i64, _i64, _f64]),
     "cs_search": (_i32, [_P, _f64, _f64, _i64, _i64, _f64, _i32, _P, _i64, ctypes.POINTER(_i64)]),
+    "cs_search_batch": (_i32, [_P, _P, _i32, _i32, _f64, _f64, _i64, _i64, _f64, _P, _P, _i64,
+                               ctypes.POINTER(_i64)]),
     "cs_search_range": (_i32, [_P, _f64, _f64, _i64, _i64, _f64, _i32, _i64, _i64, _P, _i64,
                                ctypes.POINTER(_i64)]),
     "cs_search_stats": (_i32, [_P, ctypes.POINTER(cs_stats)]),

@@ -268,6 +268,36 @@ class Engine:
             _lib.check(st, self._h, "cs_search")
             return out[:n.value].copy()
 
+    def search_batch_raw(self, spectra, lofreq=0.1, hifreq=100.0, lobin=100, blocksize=2048, threshold=None,
+                         on_device=False, cap=1 << 18):
+        """cs_search_batch over `spectra`, a list of (amps, N, dt): amps a
+        complex64 host array (pinned for full copy/compute overlap) or, with
+        on_device, an integer device address.  Returns (candidates, file index)."""
+        thr = self.params.threshold if threshold is None else threshold
+        self._spec_key = None   # the batch replaces the handle's attached spectrum
+        arr = (_lib.cs_spectrum * max(1, len(spectra)))()
+        keep = []
+        for i, (a, N, dt) in enumerate(spectra):
+            if on_device:
+                ptr, namps = int(a[0]), int(a[1])
+            else:
+                a = np.ascontiguousarray(a, dtype=np.complex64)
+                keep.append(a)
+                ptr, namps = a.ctypes.data, a.size
+            arr[i] = _lib.cs_spectrum(ptr, namps, int(N), float(dt))
+        while True:
+            out = np.empty(cap, dtype=_lib.CAND_DTYPE)
+            owner = np.empty(cap, dtype=np.int32)
+            n = ctypes.c_int64()
+            st = self.lib.cs_search_batch(self._h, arr, len(spectra), int(bool(on_device)), float(lofreq),
+                                          float(hifreq), int(lobin), int(blocksize), float(thr), out.ctypes.data,
+                                          owner.ctypes.data, cap, ctypes.byref(n))
+            if st == _lib.CS_ERR_CAPACITY and n.value > cap:
+                cap = int(n.value)
+                continue
+            _lib.check(st, self._h, "cs_search_batch")
+            return out[:n.value].copy(), owner[:n.value].copy()
+
     def stats(self) -> dict:
         s = _lib.cs_stats()
         _lib.check(self.lib.cs_search_stats(self._h, ctypes.byref(s)), self._h, "cs_search_stats")
@@ -468,6 +498,26 @@ def search(ft, params: SearchParams = None, lofreq=0.1, hifreq=100.0, lobin=100,
     if harm_remove:
         cands = remove_harmonics(cands, numharm, harm_tol)
     return cands
+
+
+def search_batch(fts, params: SearchParams = None, lofreq=0.1, hifreq=100.0, lobin=100, blocksize=2048,
+                 threshold=None, remove=True, dr_tol=1.0, harm_remove=True, numharm=16, harm_tol=1.0,
+                 cache: Optional[SearchCache] = None, device: int = 0) -> List[List[Candidate]]:
+    """`search` over many spectra (a DM sweep) with one device engine: each
+    file's candidates, post-processed as `search` does, in file order."""
+    params = SearchParams() if params is None else params
+    thr = params.threshold if threshold is None else threshold
+    eng = cache.engine_for(params, device) if cache is not None else Engine(params, device)
+    raw, owner = eng.search_batch_raw([(ft.amps, ft.N, ft.dt) for ft in fts], lofreq, hifreq, lobin,
+                                      blocksize, thr)
+    res = []
+    for i in range(len(fts)):
+        cands = _to_candidates(raw[owner == i])
+        cands = remove_duplicates(cands, dr_tol) if remove else sorted(cands, key=lambda c: c.freq)
+        if harm_remove:
+            cands = remove_harmonics(cands, numharm, harm_tol)
+        res.append(cands)
+    return res
 
 
 def block_metrics(ft, rfund, params: SearchParams, kernel="fft", widths=None, cache=None,

@@ -77,3 +77,17 @@ def survey_config(seed: int = 2):
            Pulsar(117.0, 0.08, 15.0, 0.7), Pulsar(341.0, 0.15, 20.0, 0.2), Pulsar(702.0, 0.20, 10.0, 0.9)]
     amps = make_spectrum(nsamp, dt, psr, seed)
     return amps, nsamp, dt
+
+
+def dmsweep_config(seed: int = 4, lengths=(1 << 21, 1 << 22, 1 << 23, 1 << 24), per_length: int = 16,
+                   dt: float = 64e-6):
+    """A batched DM sweep: `per_length` spectra of each length, each with 0-3
+    pulsars drawn like the precision study (f log-uniform 0.1-750 Hz, duty
+    log-uniform 1-30 %, S/N uniform 6-20).  Returns [(amps, N, dt)]."""
+    rng = np.random.default_rng(seed)
+    files = []
+    for n in lengths:
+        for _ in range(per_length):
+            ps = random_pulsars(rng, int(rng.integers(0, 4)), 0.1, 750.0, 0.01, 0.30, 6.0, 20.0)
+            files.append((make_spectrum(n, dt, ps, int(rng.integers(1 << 31))), n, dt))
+    return files

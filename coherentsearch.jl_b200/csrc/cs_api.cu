@@ -249,6 +249,7 @@ struct cs_handle {
     bool plan_valid = false;
     double plan_rlo = 0.0;
     HostPlans plans;
+    std::vector<std::pair<double, HostPlans>> plan_cache;   // host tables of recent anchors
     int64_t plan_bytes = 0;
     // metric statistics (MetricStats) and normalisation (MetricNorm)
     bool ms_on = false;
@@ -264,6 +265,10 @@ struct cs_handle {
     std::vector<double> norm_edges, norm_loc, norm_scale;   // handle level order
     DBuf d_mst, d_mwin, d_mhist, d_muo, d_norm;
     DBuf d_bm_r, d_bm_h, d_bm_st, d_bm_prof, d_bm_w, d_bm_sig, d_bm_out;   // block_metrics
+    // batch: spectra copied on a second stream into two alternating buffers
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_ev[2] = {nullptr, nullptr};
+    DBuf d_batch[2];
     HBuf h_mwin, h_mst;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     cs_stats stats{};
@@ -438,7 +443,17 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
     int64_t plan_bytes = 0;
     if (!H->plan_valid || H->plan_rlo != R.r_lo) {
         H->plan_valid = false;
-        build_plans(p, R.r_lo, H->plans);
+        // a few recent anchors stay cached on the host: a batch of spectra of
+        // several lengths alternates between them
+        auto hit = std::find_if(H->plan_cache.begin(), H->plan_cache.end(),
+                                [&](const std::pair<double, HostPlans>& e) { return e.first == R.r_lo; });
+        if (hit != H->plan_cache.end()) {
+            H->plans = hit->second;
+        } else {
+            build_plans(p, R.r_lo, H->plans);
+            if (H->plan_cache.size() >= 8) H->plan_cache.erase(H->plan_cache.begin());
+            H->plan_cache.emplace_back(R.r_lo, H->plans);
+        }
         const HostPlans& plans = H->plans;
         CS_CUDA(upload(H->d_harms, plans.harms, H->stream), "upload plans");
         CS_CUDA(upload(H->d_wtab, plans.w, H->stream), "upload weights");
@@ -919,6 +934,12 @@ cs_status cs_destroy(cs_handle* H) {
     H->h_io.release();
     H->h_mwin.release();
     H->h_mst.release();
+    if (H->copy_stream) cudaStreamSynchronize(H->copy_stream);
+    H->d_batch[0].release();
+    H->d_batch[1].release();
+    for (auto& e : H->copy_ev)
+        if (e) cudaEventDestroy(e);
+    if (H->copy_stream) cudaStreamDestroy(H->copy_stream);
     DBuf* mbufs[] = {&H->d_mst, &H->d_mwin, &H->d_mhist, &H->d_muo, &H->d_norm, &H->d_bm_r, &H->d_bm_h,
                      &H->d_bm_st, &H->d_bm_prof, &H->d_bm_w, &H->d_bm_sig, &H->d_bm_out};
     for (DBuf* b : mbufs) b->release();
@@ -966,11 +987,15 @@ cs_status cs_set_spectrum_device(cs_handle* H, const float* d_amps, int64_t namp
     return CS_OK;
 }
 
-cs_status cs_search_range(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
-                          double threshold, int32_t exact_all, int64_t block_begin, int64_t block_end,
-                          cs_candidate* out, int64_t cap, int64_t* n_out) {
-    if (!H || !n_out || (cap > 0 && !out) || cap < 0 || block_begin < 0) return CS_ERR_INVALID_ARGUMENT;
-    *n_out = 0;
+}  // extern "C"
+
+namespace {
+
+// The search of one spectrum over blocks [block_begin, block_end) of the band's
+// grid; candidates appended to `outv` in the reference's order.
+cs_status search_core(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
+                      double threshold, int32_t exact_all, int64_t block_begin, int64_t block_end,
+                      std::vector<cs_candidate>* outv) {
     if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");
     CS_CUDA(cudaSetDevice(H->device), "set device");
     const cs_params& p = H->p;
@@ -1022,7 +1047,8 @@ cs_status cs_search_range(cs_handle* H, double lofreq, double hifreq, int64_t lo
         return x.j < y.j;
     });
     const int64_t n = (int64_t)raw.size();
-    for (int64_t i = 0; i < std::min(n, cap); ++i) {
+    outv->reserve(outv->size() + (size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
         const DevCand& c = raw[i];
         const LevelHost& L = H->levels[c.lev];
         const int64_t i0 = (block_begin + (int64_t)c.blk) * Nprof;
@@ -1045,12 +1071,112 @@ cs_status cs_search_range(cs_handle* H, double lofreq, double hifreq, int64_t lo
         }
         o.k = L.k;
         o.trial = i0 + c.j;
-        out[i] = o;
+        outv->push_back(o);
     }
+    return CS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+cs_status cs_search_range(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
+                          double threshold, int32_t exact_all, int64_t block_begin, int64_t block_end,
+                          cs_candidate* out, int64_t cap, int64_t* n_out) {
+    if (!H || !n_out || (cap > 0 && !out) || cap < 0 || block_begin < 0) return CS_ERR_INVALID_ARGUMENT;
+    *n_out = 0;
+    std::vector<cs_candidate> v;
+    cs_status st = search_core(H, lofreq, hifreq, lobin, blocksize, threshold, exact_all, block_begin, block_end,
+                               &v);
+    if (st != CS_OK) return st;
+    const int64_t n = (int64_t)v.size();
+    std::copy_n(v.begin(), std::min(n, cap), out);
     *n_out = n;
     if (n > cap) return fail(H, CS_ERR_CAPACITY, "candidate array too small");
     return CS_OK;
 }
+
+cs_status cs_search_batch(cs_handle* H, const cs_spectrum* files, int32_t nfiles, int32_t on_device,
+                          double lofreq, double hifreq, int64_t lobin, int64_t blocksize, double threshold,
+                          cs_candidate* out, int32_t* file_of, int64_t cap, int64_t* n_out) {
+    if (!H || !files || nfiles < 0 || !n_out || (cap > 0 && (!out || !file_of)) || cap < 0)
+        return CS_ERR_INVALID_ARGUMENT;
+    *n_out = 0;
+    for (int i = 0; i < nfiles; ++i) {
+        const cs_spectrum& f = files[i];
+        if (!f.amps || f.namps < 1 || f.N < 2 || !(f.dt > 0))
+            return fail(H, CS_ERR_INVALID_ARGUMENT, "every spectrum needs namps >= 1, N >= 2, dt > 0");
+        if (on_device && (reinterpret_cast<uintptr_t>(f.amps) & 7u) != 0)
+            return fail(H, CS_ERR_INVALID_ARGUMENT, "device spectra must be 8-byte aligned");
+    }
+    CS_CUDA(cudaSetDevice(H->device), "set device");
+    // Host spectra: file i+1 is copied on the copy stream into the other of two
+    // device buffers while file i is searched; the search stream waits on the
+    // copy's event.  A buffer is refilled only after the search that read it
+    // returned (each search ends with a stream synchronisation).
+    int64_t maxa = 0;
+    for (int i = 0; i < nfiles; ++i) maxa = std::max(maxa, files[i].namps);
+    if (!on_device && nfiles > 0) {
+        if (!H->copy_stream) CS_CUDA(cudaStreamCreateWithFlags(&H->copy_stream, cudaStreamNonBlocking), "copy stream");
+        for (int b = 0; b < 2; ++b) {
+            if (!H->copy_ev[b]) CS_CUDA(cudaEventCreateWithFlags(&H->copy_ev[b], cudaEventDisableTiming), "copy event");
+            CS_CUDA(H->d_batch[b].ensure((size_t)maxa * sizeof(float2)), "alloc spectrum buffer");
+        }
+    }
+    auto issue_copy = [&](int i) -> cudaError_t {
+        const int b = i & 1;
+        cudaError_t e = cudaMemcpyAsync(H->d_batch[b].p, files[i].amps, (size_t)files[i].namps * sizeof(float2),
+                                        cudaMemcpyHostToDevice, H->copy_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(H->copy_ev[b], H->copy_stream);
+        return e;
+    };
+    if (!on_device && nfiles > 0) CS_CUDA(issue_copy(0), "copy spectrum");
+    std::vector<cs_candidate> all;
+    std::vector<int32_t> owner;
+    cs_stats tot{};
+    for (int i = 0; i < nfiles; ++i) {
+        if (!on_device) {
+            if (i + 1 < nfiles) CS_CUDA(issue_copy(i + 1), "copy spectrum");
+            CS_CUDA(cudaStreamWaitEvent(H->stream, H->copy_ev[i & 1], 0), "wait spectrum");
+            H->amps = H->d_batch[i & 1].as<float2>();
+        } else {
+            H->amps = reinterpret_cast<const float2*>(files[i].amps);
+        }
+        H->namps = files[i].namps;
+        H->N = files[i].N;
+        H->dt = files[i].dt;
+        H->has_spec = true;
+        H->spec_h2d_bytes = on_device ? 0 : files[i].namps * (int64_t)sizeof(float2);
+        const size_t before = all.size();
+        cs_status st = search_core(H, lofreq, hifreq, lobin, blocksize, threshold, 0, 0, -1, &all);
+        if (st != CS_OK) return st;
+        owner.insert(owner.end(), all.size() - before, i);
+        const cs_stats& S = H->stats;
+        tot.trials += S.trials;
+        tot.blocks += S.blocks;
+        tot.profiles += S.profiles;
+        tot.rescued += S.rescued;
+        tot.candidates += S.candidates;
+        tot.waves += S.waves;
+        tot.launches += S.launches;
+        tot.ms_interp += S.ms_interp;
+        tot.ms_synth += S.ms_synth;
+        tot.ms_sigma += S.ms_sigma;
+        tot.ms_rescue += S.ms_rescue;
+        tot.ms_total += S.ms_total;
+        tot.h2d_bytes += S.h2d_bytes;
+        tot.d2h_bytes += S.d2h_bytes;
+    }
+    H->stats = tot;
+    H->has_spec = false;   // the batch buffers are not a spectrum of the handle's
+    const int64_t n = (int64_t)all.size();
+    std::copy_n(all.begin(), std::min(n, cap), out);
+    std::copy_n(owner.begin(), std::min(n, cap), file_of);
+    *n_out = n;
+    if (n > cap) return fail(H, CS_ERR_CAPACITY, "candidate array too small");
+    return CS_OK;
+}
+
 
 cs_status cs_search(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
                     double threshold, int32_t exact_all, cs_candidate* out, int64_t cap, int64_t* n_out) {

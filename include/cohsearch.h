@@ -193,6 +193,27 @@ cs_status cs_get_metric_hists(const cs_handle* h, int32_t* nlev, int32_t* nwin, 
 cs_status cs_set_metricnorm(cs_handle* h, int32_t nlev, int32_t nwin, const int32_t* ks, const double* edges,
                             const double* loc, const double* scale);
 
+/* One spectrum of a batch: complex64 amps [namps] (host or device memory,
+ * per cs_search_batch's on_device), N samples at dt seconds. */
+typedef struct cs_spectrum {
+    const float* amps;
+    int64_t namps;
+    int64_t N;
+    double dt;
+} cs_spectrum;
+
+/* `search` over each of nfiles spectra (a DM sweep: many .fft files of uneven
+ * length, src/cli.jl:237-246 loops `search_one` over them) with one handle:
+ * candidates as cs_search emits them, file by file in order, file_of[c] the
+ * index of candidate c's spectrum.  Host spectra (on_device = 0; pinned memory
+ * for full overlap) are copied on a second stream, file i+1's copy running
+ * under file i's search.  No counterpart takes all files at once in the
+ * reference.  cs_search_stats then gives the totals over the batch.  If cap is
+ * too small, CS_ERR_CAPACITY with *n_out = the number found. */
+cs_status cs_search_batch(cs_handle* h, const cs_spectrum* files, int32_t nfiles, int32_t on_device,
+                          double lofreq, double hifreq, int64_t lobin, int64_t blocksize, double threshold,
+                          cs_candidate* out, int32_t* file_of, int64_t cap, int64_t* n_out);
+
 /* Counters and stage timings of the last cs_search on this handle. */
 cs_status cs_search_stats(const cs_handle* h, cs_stats* out);
 

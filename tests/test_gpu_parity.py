@@ -275,3 +275,28 @@ def test_block_ranges_reproduce_the_search(synth):
                  for r in range(world)]
         assert np.array_equal(np.concatenate(parts), whole)
     assert len(eng.search_raw(1.0, 60.0, 100, 2048, 7.0, blocks=(nb, nb + 5))) == 0
+
+
+def test_batch_equals_file_by_file_searches():
+    """cs_search_batch over spectra of several lengths (host memory, copies
+    overlapped with the searches) returns, file by file, exactly the
+    candidates of separate cs_search calls."""
+    cs = _cs()
+    from cohsearch import synth
+    files = []
+    for i, nsamp in enumerate([1 << 18, 1 << 19, 1 << 18, 1 << 20]):
+        dt = 64e-6
+        amps = synth.make_spectrum(nsamp, dt, [synth.Pulsar(11.0 + 3.0 * i, 0.05, 40.0, 0.3)], 100 + i)
+        files.append((amps, nsamp, dt))
+    dec = cs.decimation_set(32, 4)
+    params = cs.SearchParams(nharms=32, m=16, decimations=dec, threshold=7.0, synth="fp16")
+    eng = cs.Engine(params)
+    raw, owner = eng.search_batch_raw(files, 1.0, 60.0, 100, 2048, 7.0)
+    st = eng.stats()
+    assert st["trials"] > 0
+    for i, (amps, N, dt) in enumerate(files):
+        single = cs.Engine(params)
+        single.set_spectrum(cs.FFTFile.from_array(amps, N, dt))
+        want = single.search_raw(1.0, 60.0, 100, 2048, 7.0)
+        assert np.array_equal(raw[owner == i], want)
+    assert any(len(raw[owner == i]) > 0 for i in range(len(files)))

@@ -1,0 +1,80 @@
+"""Error against the FP64 oracle, stated per configuration: the small plain
+search (one 7.3 Hz pulsar, nharms 32, 1-50 Hz) and the precision study (the
+same noise with 40 injections, f 0.1-750 Hz, duty 1-30 %, S/N 6-20).
+
+  * amplitudes: the device's FP32 interpolation (Float32 weights, FP32 tap
+    chain) against Float64 weights and FP64 accumulation, relative to the RMS
+    amplitude of the chunk;
+  * S/N: chunk_metrics (FP32 profiles, exact median rescan) against the FP64
+    oracle's, |dS/N| / max(S/N, 1);
+  * 16-bit gates: the tensor-core (BF16 / FP16) zero-baseline gate against the
+    FP32 one over the whole band, |dg| / max(|g|, 1).
+
+The bounds asserted are the ones the design states; the measured values are
+printed (pytest -s) for the record.
+"""
+import numpy as np
+import pytest
+
+from oracle import cs_ref as o
+
+pytestmark = pytest.mark.gpu
+
+
+def _configs():
+    from cohsearch import synth
+    amps1, N, dt = synth.small_config()
+    rng = np.random.default_rng(33)
+    ps = synth.random_pulsars(rng, 40, 0.1, 750.0, 0.01, 0.30, 6.0, 20.0)
+    amps3 = synth.make_spectrum(N, dt, ps, 31)
+    return {"config 1 (plain, small)": (amps1, N, dt), "config 3 (40 injections)": (amps3, N, dt)}
+
+
+def _stats(err):
+    err = np.abs(np.asarray(err, np.float64))
+    return float(err.max()), float(np.sqrt(np.mean(err ** 2)))
+
+
+@pytest.mark.parametrize("name", list(_configs()))
+def test_error_vs_fp64_oracle(name):
+    import cohsearch as cs
+    amps, N, dt = _configs()[name]
+    T = N * dt
+    params = cs.SearchParams(nharms=32, m=16)
+    op = o.SearchParams(nharms=32, m=16)
+    eng = cs.Engine(params)
+    eng.set_spectrum(cs.FFTFile.from_array(amps, N, dt))
+    lodr = params.hidr / params.nharms
+    amp_err, snr_err = [], []
+    for f0 in (1.3, 7.29, 19.0, 33.3, 48.0):
+        rstart = f0 * T
+        n = 512
+        # amplitudes of one chunk: device FP32 vs Float64 weights, FP64 accumulation
+        dev = eng.interp_chunk(rstart, 0, n)
+        plans = o.build_direct_plans(op, rstart, np.float64)
+        ref = o.chunk_stack(plans, amps, op, 0, n, N, np.float64)[:, 1:].T   # (nharms, n)
+        scale = np.sqrt(np.mean(np.abs(ref) ** 2))
+        amp_err.append(np.abs(dev.astype(np.complex128) - ref).ravel() / scale)
+        # exact S/N
+        got = eng.chunk_metrics(rstart, n)
+        want = o.chunk_metrics(amps, N, op, rstart, n, weights=np.float64)
+        snr_err.append((got - want) / np.maximum(np.abs(want), 1.0))
+    amax, arms = _stats(np.concatenate(amp_err))
+    smax, srms = _stats(np.concatenate(snr_err))
+    # 16-bit gates against the FP32 gate, whole band, every level
+    dec = cs.decimation_set(32, 4)
+    gates = {}
+    for mode in ("fp32", "bf16", "fp16"):
+        e = cs.Engine(cs.SearchParams(nharms=32, m=16, decimations=dec, synth=mode))
+        e.set_diagnostics(2)
+        e.set_spectrum(cs.FFTFile.from_array(amps, N, dt))
+        e.search_raw(1.0, 50.0, 100, 2048, 8.0)
+        gates[mode] = e.gate_values()
+    g32 = gates["fp32"]
+    live = g32 != 0
+    gerr = {m: _stats((gates[m][live] - g32[live]) / np.maximum(np.abs(g32[live]), 1.0)) for m in ("bf16", "fp16")}
+    print(f"\n| {name} | amplitude max/RMS {amax:.2e}/{arms:.2e} | S/N max/RMS {smax:.2e}/{srms:.2e} | "
+          f"BF16 gate {gerr['bf16'][0]:.2e}/{gerr['bf16'][1]:.2e} | FP16 gate {gerr['fp16'][0]:.2e}/{gerr['fp16'][1]:.2e} |")
+    assert amax < 1e-5
+    assert smax <= 1e-3
+    assert gerr["fp16"][0] < 2e-2 and gerr["bf16"][0] < 8e-2

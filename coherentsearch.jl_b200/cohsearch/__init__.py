@@ -7,7 +7,8 @@ from ._lib import CohSearchError, LIB_PATH, load as load_library
 from .fileio import FFTFile, SimpleInf, freqs, write_fft
 from .metricstats import (BlockMetricStats, MetricHistogram, MetricNorm, MetricStats, build_metricnorm,
                           hist_quantile, metricstats_summary, metricstats_windows)
-from .search import (Candidate, Engine, SearchCache, SearchParams, block_metrics, boxcar_widths, chunk_metrics,
+from .search import (Candidate, Engine, SearchCache, SearchParams, block_metrics, boxcar_widths, candidate_profile,
+                     chunk_metrics, measure_ducy, rotate_to_peak,
                      decimation_set, ladder_boxcar_widths, proftype, remove_duplicates,
                      remove_harmonics, search, search_batch, search_block, write_candidates)
 
@@ -17,5 +18,5 @@ __all__ = [
     "decimation_set", "ladder_boxcar_widths", "proftype", "remove_duplicates", "remove_harmonics",
     "search", "write_candidates", "BlockMetricStats", "MetricHistogram", "MetricNorm", "MetricStats",
     "build_metricnorm", "hist_quantile", "metricstats_summary", "metricstats_windows", "block_metrics",
-    "search_block", "search_batch",
+    "search_block", "search_batch", "candidate_profile", "measure_ducy", "rotate_to_peak",
 ]

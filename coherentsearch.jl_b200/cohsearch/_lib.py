@@ -107,6 +107,7 @@ PROTOTYPES = {
     "cs_search_stats": (_i32, [_P, ctypes.POINTER(cs_stats)]),
     "cs_chunk_metrics": (_i32, [_P, _f64, _i64, _P]),
     "cs_block_metrics": (_i32, [_P, _P, _i64, _i32, _P, _i32, _P]),
+    "cs_refold": (_i32, [_P, _P, _P, _i64, _i32, _P, _P, _P]),
     "cs_interp_chunk": (_i32, [_P, _f64, _i64, _i64, _P]),
     "cs_chunk_metrics_static": (_i32, [_P, _P, _i64, _i64, _f64, _i64, _P, _P, _P, _i64]),
     "cs_search_block_values": (_i32, [_P, _P, _P, _i64, ctypes.POINTER(_i64)]),

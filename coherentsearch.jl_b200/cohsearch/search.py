@@ -415,6 +415,21 @@ class Engine:
                                              out.ctypes.data), self._h, "cs_block_metrics")
         return out
 
+    def refold(self, r, nharm, m: int = 64):
+        """cs_refold: (H, profiles as a list of arrays, ducy) for candidates at
+        fundamentals r with nharm requested harmonics each."""
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        nh = np.ascontiguousarray(np.broadcast_to(nharm, r.shape), dtype=np.int32)
+        n = r.size
+        H = np.zeros(n, np.int32)
+        prof = np.zeros((max(n, 1), 1024), np.float64)
+        ducy = np.zeros(n, np.float64)
+        if n:
+            _lib.check(self.lib.cs_refold(self._h, r.ctypes.data, nh.ctypes.data, n, int(m), H.ctypes.data,
+                                          prof.ctypes.data, ducy.ctypes.data), self._h, "cs_refold")
+        profs = [prof[i, :2 * H[i]].copy() if H[i] >= 1 else np.zeros(2) for i in range(n)]
+        return H, profs, ducy
+
     def chunk_metrics(self, rstart: float, n: int) -> np.ndarray:
         out = np.zeros(int(n), np.float64)
         _lib.check(self.lib.cs_chunk_metrics(self._h, float(rstart), int(n), out.ctypes.data), self._h,
@@ -518,6 +533,42 @@ def search_batch(fts, params: SearchParams = None, lofreq=0.1, hifreq=100.0, lob
             cands = remove_harmonics(cands, numharm, harm_tol)
         res.append(cands)
     return res
+
+
+def candidate_profile(ft, r: float, nharm: int, m: int = 64, params: SearchParams = None,
+                      cache=None, device: int = 0) -> np.ndarray:
+    """candidate_profile (src/candidate.jl:37-61) on the device: the 2H-bin
+    coherent-fold profile of fundamental `r`, not rotated."""
+    if nharm < 1:
+        raise ValueError("nharm must be >= 1")
+    if m % 2:
+        raise ValueError("m must be even")
+    params = SearchParams() if params is None else params
+    eng = cache.engine_for(params, device) if cache is not None else Engine(params, device)
+    eng.set_spectrum(ft)
+    H, profs, _ = eng.refold([r], [nharm], m)
+    return profs[0]
+
+
+def measure_ducy(ft, cands: Sequence[Candidate], params: SearchParams, m: int = 64, cache=None,
+                 device: int = 0) -> List[Candidate]:
+    """measure_ducy (src/candidate.jl:63-99): each candidate refolded at its own
+    r with its own nharm on the device; ducy = best boxcar width / bins."""
+    eng = cache.engine_for(params, device) if cache is not None else Engine(params, device)
+    eng.set_spectrum(ft)
+    if not cands:
+        return []
+    _, _, ducy = eng.refold([c.r for c in cands], [c.nharm for c in cands], m)
+    return [Candidate(c.freq, c.metric, c.r, c.nharm, float(d), c.k, c.trial) for c, d in zip(cands, ducy)]
+
+
+def rotate_to_peak(prof) -> np.ndarray:
+    """rotate_to_peak (src/candidate.jl:101-110): the maximum bin moved to phase 0.5."""
+    prof = np.asarray(prof, dtype=np.float64)
+    n = len(prof)
+    if n == 0:
+        return prof
+    return np.roll(prof, n // 2 - int(np.argmax(prof)))
 
 
 def block_metrics(ft, rfund, params: SearchParams, kernel="fft", widths=None, cache=None,

@@ -1344,6 +1344,40 @@ cs_status cs_block_metrics(cs_handle* H, const double* rfund, int64_t L, int32_t
     return CS_OK;
 }
 
+cs_status cs_refold(cs_handle* H, const double* r, const int32_t* nharm, int64_t n, int32_t m, int32_t* Hout,
+                    double* profiles, double* ducy) {
+    if (!H || !r || !nharm || !Hout || !ducy || n < 0 || n > (1 << 24)) return CS_ERR_INVALID_ARGUMENT;
+    if (m < 2 || (m % 2) != 0) return fail(H, CS_ERR_INVALID_ARGUMENT, "m must be even");
+    if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");
+    const int maxh = 512;   // the kernel's kRefoldMaxH
+    for (int64_t i = 0; i < n; ++i)
+        if (nharm[i] > maxh) return fail(H, CS_ERR_UNSUPPORTED, "nharm above 512 is not built");
+    if (n == 0) return CS_OK;
+    CS_CUDA(cudaSetDevice(H->device), "set device");
+    CS_CUDA(H->d_bm_r.ensure((size_t)n * sizeof(double)), "alloc candidates");
+    CS_CUDA(H->d_bm_w.ensure((size_t)n * sizeof(int32_t) * 2), "alloc harmonics");
+    CS_CUDA(H->d_bm_out.ensure((size_t)n * sizeof(double)), "alloc duty cycles");
+    if (profiles) CS_CUDA(H->d_bm_prof.ensure((size_t)n * 2 * maxh * sizeof(double)), "alloc profiles");
+    int32_t* d_nh = H->d_bm_w.as<int32_t>();
+    int32_t* d_H = d_nh + n;
+    CS_CUDA(cudaMemcpyAsync(H->d_bm_r.p, r, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, H->stream), "copy r");
+    CS_CUDA(cudaMemcpyAsync(d_nh, nharm, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, H->stream),
+            "copy nharm");
+    CS_CUDA(run_refold(H->d_bm_r.as<double>(), d_nh, (int)n, m, H->p.boxcar_fsp, H->p.boxcar_maxfrac, H->amps,
+                       H->namps, H->N / 2, maxh, profiles ? H->d_bm_prof.as<double>() : nullptr, d_H,
+                       H->d_bm_out.as<double>(), H->stream),
+            "refold launch");
+    CS_CUDA(cudaMemcpyAsync(Hout, d_H, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, H->stream), "read H");
+    CS_CUDA(cudaMemcpyAsync(ducy, H->d_bm_out.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, H->stream),
+            "read duty cycles");
+    if (profiles)
+        CS_CUDA(cudaMemcpyAsync(profiles, H->d_bm_prof.p, (size_t)n * 2 * maxh * sizeof(double),
+                                cudaMemcpyDeviceToHost, H->stream),
+                "read profiles");
+    CS_CUDA(cudaStreamSynchronize(H->stream), "refold");
+    return CS_OK;
+}
+
 cs_status cs_interp_chunk(cs_handle* H, double r_lo, int64_t t0, int64_t n, float* out) {
     if (!H || !out || n < 1 || n > (1 << 16) || t0 < 0) return CS_ERR_INVALID_ARGUMENT;
     if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");

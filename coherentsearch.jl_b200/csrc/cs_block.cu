@@ -213,4 +213,115 @@ cudaError_t run_block_metrics(const double* d_rfund, int L, const BmHarm* d_hm, 
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Candidate refold (candidate_profile / measure_ducy, src/candidate.jl:37-99)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr int kRefoldMaxH = 512;   // harmonics a refold may request
+
+// One CTA per candidate: the contiguous harmonics 1..H that fit (the first
+// whose m-bin window crosses Nyquist or the file's end stops the sum), each a
+// wide-kernel fourier_interp at r*h; the normalised irfft to 2H bins; then
+// boxcar_best_width (src/search.jl:617-638) on that profile for the duty cycle.
+__global__ void __launch_bounds__(128) k_refold(const double* __restrict__ rr, const int* __restrict__ nh_in,
+                                                int n, int m, double fsp, double maxfrac,
+                                                const float2* __restrict__ amps, int64_t namps, int64_t Nhalf,
+                                                int maxh, double* __restrict__ prof_out, int* __restrict__ H_out,
+                                                double* __restrict__ ducy_out) {
+    __shared__ double2 X[kRefoldMaxH];
+    __shared__ double prof[2 * kRefoldMaxH];
+    __shared__ double ps[4 * kRefoldMaxH + 2];
+    __shared__ int sH;
+    __shared__ double smed[2];
+    const int c = blockIdx.x;
+    if (c >= n) return;
+    const double r = rr[c];
+    const int nharm = nh_in[c];
+    const int m2 = m / 2;
+    if (!(nharm >= 1 && r > 0.0)) {
+        if (threadIdx.x == 0) {
+            H_out[c] = -1;
+            ducy_out[c] = CUDART_NAN;
+        }
+        return;
+    }
+    if (threadIdx.x == 0) {
+        int H = 0;
+        for (int h = 1; h <= min(nharm, maxh); ++h) {
+            const double rh = r * (double)h;
+            const int64_t rint = (int64_t)floor(rh + 1e-15) + 1;
+            if (!(rint - m2 >= 0 && rint + m2 <= namps && rh < (double)Nhalf)) break;
+            H = h;
+        }
+        sH = H;
+    }
+    __syncthreads();
+    const int H = sH;
+    for (int h = threadIdx.x; h < H; h += blockDim.x) X[h] = fourier_interp_d(r * (double)(h + 1), amps, namps, m);
+    __syncthreads();
+    const int nb = H >= 1 ? 2 * H : 2;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        double s = 0.0;
+        if (H >= 1) {
+            for (int h = 1; h < H; ++h) {
+                const double ang = 2.0 * (double)(((int64_t)h * b) % nb) / (double)nb;
+                s += 2.0 * (X[h - 1].x * cospi(ang) - X[h - 1].y * sinpi(ang));
+            }
+            s += (b & 1) ? -X[H - 1].x : X[H - 1].x;
+            s /= (double)nb;
+        }
+        prof[b] = s;
+        if (prof_out) prof_out[(int64_t)c * 2 * maxh + b] = s;
+    }
+    __syncthreads();
+    // exact median by rank counting
+    const int half = nb >> 1;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        const double v = prof[i];
+        int lt = 0, le = 0;
+        for (int q = 0; q < nb; ++q) {
+            lt += prof[q] < v;
+            le += prof[q] <= v;
+        }
+        if (lt <= half - 1 && half - 1 < le) smed[0] = v;
+        if (lt <= half && half < le) smed[1] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double med = (smed[0] + smed[1]) / 2.0;   // nb is even
+        // boxcar_widths (src/search.jl:387-396)
+        const int wmax = max(1, (int)floor(maxfrac * nb));
+        int wlast = 1;
+        for (int w = 1; w <= wmax; w = max((int)floor(fsp * w), w + 1)) wlast = w;
+        ps[0] = 0.0;
+        for (int i = 0; i < nb + wlast; ++i) ps[i + 1] = ps[i] + (prof[i % nb] - med);
+        double best = -CUDART_INF;
+        int bestw = 1;
+        for (int w = 1; w <= wmax; w = max((int)floor(fsp * w), w + 1)) {
+            const double invsw = 1.0 / sqrt((double)w);
+            double mm = ps[w] - ps[0];
+            for (int p = 1; p < nb; ++p) mm = fmax(mm, ps[p + w] - ps[p]);
+            const double cand = mm * invsw;
+            if (cand > best) {
+                best = cand;
+                bestw = w;
+            }
+        }
+        H_out[c] = H;
+        ducy_out[c] = (double)bestw / (double)nb;
+    }
+}
+
+}  // namespace
+
+cudaError_t run_refold(const double* d_r, const int* d_nharm, int n, int m, double fsp, double maxfrac,
+                       const float2* amps, int64_t namps, int64_t Nhalf, int maxh, double* d_prof, int* d_H,
+                       double* d_ducy, cudaStream_t st) {
+    if (n > 0)
+        k_refold<<<n, 128, 0, st>>>(d_r, d_nharm, n, m, fsp, maxfrac, amps, namps, Nhalf, maxh, d_prof, d_H, d_ducy);
+    return cudaGetLastError();
+}
+
 }  // namespace cs

@@ -298,6 +298,9 @@ struct BmHarm {
 cudaError_t run_block_metrics(const double* d_rfund, int L, const BmHarm* d_hm, int nh, int m, int nb, int kernel,
                               const float2* amps, int64_t namps, double2* d_st, double* d_prof,
                               const int* d_widths, int nw, double* d_sigma, double* d_out, cudaStream_t st);
+cudaError_t run_refold(const double* d_r, const int* d_nharm, int n, int m, double fsp, double maxfrac,
+                       const float2* amps, int64_t namps, int64_t Nhalf, int maxh, double* d_prof, int* d_H,
+                       double* d_ducy, cudaStream_t st);
 size_t mstats_smem(int nprof, int hist_nb);
 size_t synth_fp32_smem(int nharms, int maxbins, int maxwmax);
 

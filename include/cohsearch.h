@@ -260,6 +260,18 @@ cs_status cs_chunk_metrics_static(const cs_params* params, const float* d_amps, 
 cs_status cs_block_metrics(cs_handle* h, const double* rfund, int64_t L, int32_t kernel, const int32_t* widths,
                            int32_t nw, double* out);
 
+/* candidate_profile / measure_ducy (src/candidate.jl:37-99) for n candidates:
+ * fundamental Fourier frequency r[i] (bins) and requested harmonics nharm[i]
+ * (<= 512).  Each harmonic h = 1, 2, ... is an m-bin (reference default 64)
+ * exact fourier_interp at r*h, stopping at the first whose window crosses
+ * Nyquist or the file's end; H[i] receives the harmonics used (-1 when
+ * nharm < 1 or r <= 0, whose duty cycle is NaN), profiles[i*256 + 0 .. 2H)
+ * the normalised irfft profile (NULL: not returned; H = 0 gives two zero bins),
+ * ducy[i] the best boxcar width / profile bins (boxcar_best_width,
+ * src/search.jl:617-638, with the handle's boxcar_fsp / boxcar_maxfrac). */
+cs_status cs_refold(cs_handle* h, const double* r, const int32_t* nharm, int64_t n, int32_t m, int32_t* H,
+                    double* profiles, double* ducy);
+
 /* Interpolated amplitude stack of a chunk (the `ftprofs` rows of
  * fill_chunk_profiles!, src/search.jl:1280-1290, and fill_harmonic_row_direct!,
  * src/directinterp.jl:470-572): trials t0 .. t0+n-1 of a search whose global

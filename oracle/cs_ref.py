@@ -718,6 +718,46 @@ def block_metrics(amps, N, rfund, params: SearchParams, kernel="fft", widths=Non
                        sigma_samples=BOXCAR_SIGMA_SAMPLES, widths=widths)
 
 
+def candidate_profile(amps: np.ndarray, N: int, r: float, nharm: int, m: int = 64) -> np.ndarray:
+    """candidate_profile (src/candidate.jl:37-61): contiguous harmonics while
+    their m-bin window fits below Nyquist and inside the file, each an exact
+    fourier_interp; irfft of [0, amps...] to 2H bins (two zeros if H = 0)."""
+    if nharm < 1:
+        raise ValueError("nharm must be >= 1")
+    if m % 2:
+        raise ValueError("m must be even")
+    m2 = m // 2
+    Nhalf = N // 2
+    namps = len(amps)
+    out = []
+    for h in range(1, nharm + 1):
+        rh = r * h
+        rint = math.floor(rh + 1e-15) + 1
+        if not (rint - m2 >= 0 and rint + m2 <= namps and rh < Nhalf):
+            break
+        out.append(fourier_interp(rh, amps, m))
+    H = len(out)
+    if H < 1:
+        return np.zeros(2)
+    stack = np.zeros(H + 1, dtype=np.complex128)
+    stack[1:] = out
+    return np.fft.irfft(stack, 2 * H)
+
+
+def measure_ducy(amps: np.ndarray, N: int, rs, nharms, params: "SearchParams", m: int = 64) -> np.ndarray:
+    """measure_ducy (src/candidate.jl:63-99): per candidate (r, nharm) the duty
+    cycle of the best boxcar of its refolded profile; NaN when nharm < 1 or r <= 0."""
+    res = []
+    for r, nh in zip(rs, nharms):
+        d = math.nan
+        if nh >= 1 and r > 0:
+            prof = candidate_profile(amps, N, r, nh, m)
+            if len(prof) >= 2:
+                _, d = boxcar_best_width(prof, params.boxcar_fsp, params.boxcar_maxfrac)
+        res.append(d)
+    return np.array(res)
+
+
 @dataclass
 class Candidate:
     """src/search.jl:179-191."""

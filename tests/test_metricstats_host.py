@@ -74,3 +74,13 @@ def test_build_metricnorm_fallbacks_and_windows():
     z1 = normalize(norm, 1, 1.5, 7.0)
     assert z1 == pytest.approx((7.0 - norm.loc[1][0]) / norm.scale[1][0])
     assert normalize(norm, 5, 1.5, 7.0) == 7.0                  # no model for k: unchanged
+
+
+def test_rotate_to_peak():
+    """test/test_candidate.jl:14-21: the maximum moves to bin n//2 (0-based)."""
+    from cohsearch import rotate_to_peak
+    for n in (8, 9, 64, 65):
+        prof = np.arange(1.0, n + 1)
+        rp = rotate_to_peak(prof)
+        assert len(rp) == n and int(np.argmax(rp)) == n // 2 and sorted(rp) == sorted(prof)
+    assert rotate_to_peak(np.zeros(0)).size == 0

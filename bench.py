@@ -140,11 +140,11 @@ def interp_flops_per_trial(m=16):
 # DRAM bytes (read + write) per trial of one launch, from the ncu captures
 # summarised under profiles/ (small survey case, 1,282,048 trials; the traffic
 # of these kernels grows in proportion to the trial count).
-NCU_BYTES_PER_TRIAL = {"k_interp": 295.3, "k_synth_tc": 277.3, "k_sigma": 98.9, "k_flag+k_rescue": 24.5}
+NCU_BYTES_PER_TRIAL = {"k_interp": 295.3, "k_synth_tc": 259.2, "k_sigma": 98.9, "k_rescue": 0.44}
 # Algorithmic DRAM bytes per trial: k_interp writes 240 B of FP16 A-tile chunks
 # and 96 B of sigma samples and reads ~4 B of spectrum; k_sigma reads the 96 B
-# of samples; the flag pass reads 6 levels x 4 B of gate values.
-ALG_BYTES_PER_TRIAL = {"k_interp": 340.0, "k_sigma": 96.0, "k_flag+k_rescue": 24.0}
+# of samples.
+ALG_BYTES_PER_TRIAL = {"k_interp": 340.0, "k_sigma": 96.0}
 
 
 def load_peaks():
@@ -429,7 +429,7 @@ def main():
     fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12   # TFLOP/s, nominal
     tc_flops = trials * 2.0 * 128 * 352     # dense product per trial: 2 * K(128) * N(352 columns)
     kname = {"ms_interp": "k_interp", "ms_synth": "k_synth_tc" if args.synth != "fp32" else "k_synth_fp32",
-             "ms_sigma": "k_sigma", "ms_rescue": "k_flag+k_rescue"}[dom]
+             "ms_sigma": "k_sigma", "ms_rescue": "k_rescue"}[dom]
     traffic = NCU_BYTES_PER_TRIAL.get(kname)
     traffic = traffic * trials if traffic is not None else None
     if kname == "k_synth_tc":
@@ -446,11 +446,13 @@ def main():
                                "(no measured FP32 peak exists)",
                 "work": "4(Hk+1)(Hk-1) flops per trial per level"}
     else:
-        alg = ALG_BYTES_PER_TRIAL[kname] * trials
+        # (a stage without an algorithmic count is rated on its measured bytes)
+        alg_b = ALG_BYTES_PER_TRIAL.get(kname, NCU_BYTES_PER_TRIAL.get(kname, 0.0))
+        alg = alg_b * trials
         achieved = alg / (stage[dom] / 1000.0) / 1e9
         roof = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                "work": f"{ALG_BYTES_PER_TRIAL[kname]:.0f} algorithmic DRAM bytes per trial"}
+                "work": f"{alg_b:.0f} algorithmic DRAM bytes per trial"}
         if kname == "k_interp":
             fl = trials * interp_flops_per_trial()
             roof["fp32"] = {"achieved_tflops": fl / (stage[dom] / 1000.0) / 1e12, "peak_tflops": fp32_peak,

@@ -472,23 +472,35 @@ __device__ __forceinline__ void synth_chunk8(const float2* __restrict__ xs, int 
                                              const float* __restrict__ C2,
                                              const float* __restrict__ S2, int np, int k, int Hk,
                                              int n0, float E[8], float O[8]) {
+    // adjacent outputs (u, u+1) as one packed fma.rn.f32x2: per output the
+    // same sequential fmaf chain
+    unsigned long long e[4], o[4];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) { E[u] = 0.0f; O[u] = 0.0f; }
+    for (int v = 0; v < 4; ++v) e[v] = o[v] = f2_pack(0.0f, 0.0f);
 #pragma unroll 4
     for (int jh = 1; jh < Hk; ++jh) {
         const float2 x = xs[(jh * k - 1) * xstride];
-        const float4 c0 = *reinterpret_cast<const float4*>(C2 + jh * np + n0);
-        const float4 c1 = *reinterpret_cast<const float4*>(C2 + jh * np + n0 + 4);
-        const float4 s0 = *reinterpret_cast<const float4*>(S2 + jh * np + n0);
-        const float4 s1 = *reinterpret_cast<const float4*>(S2 + jh * np + n0 + 4);
-        E[0] = fmaf(x.x, c0.x, E[0]); E[1] = fmaf(x.x, c0.y, E[1]);
-        E[2] = fmaf(x.x, c0.z, E[2]); E[3] = fmaf(x.x, c0.w, E[3]);
-        E[4] = fmaf(x.x, c1.x, E[4]); E[5] = fmaf(x.x, c1.y, E[5]);
-        E[6] = fmaf(x.x, c1.z, E[6]); E[7] = fmaf(x.x, c1.w, E[7]);
-        O[0] = fmaf(x.y, s0.x, O[0]); O[1] = fmaf(x.y, s0.y, O[1]);
-        O[2] = fmaf(x.y, s0.z, O[2]); O[3] = fmaf(x.y, s0.w, O[3]);
-        O[4] = fmaf(x.y, s1.x, O[4]); O[5] = fmaf(x.y, s1.y, O[5]);
-        O[6] = fmaf(x.y, s1.z, O[6]); O[7] = fmaf(x.y, s1.w, O[7]);
+        const ulonglong2 c01 = *reinterpret_cast<const ulonglong2*>(C2 + jh * np + n0);
+        const ulonglong2 c23 = *reinterpret_cast<const ulonglong2*>(C2 + jh * np + n0 + 4);
+        const ulonglong2 s01 = *reinterpret_cast<const ulonglong2*>(S2 + jh * np + n0);
+        const ulonglong2 s23 = *reinterpret_cast<const ulonglong2*>(S2 + jh * np + n0 + 4);
+        const unsigned long long xr = f2_pack(x.x, x.x), xi = f2_pack(x.y, x.y);
+        e[0] = f2_fma(xr, c01.x, e[0]);
+        e[1] = f2_fma(xr, c01.y, e[1]);
+        e[2] = f2_fma(xr, c23.x, e[2]);
+        e[3] = f2_fma(xr, c23.y, e[3]);
+        o[0] = f2_fma(xi, s01.x, o[0]);
+        o[1] = f2_fma(xi, s01.y, o[1]);
+        o[2] = f2_fma(xi, s23.x, o[2]);
+        o[3] = f2_fma(xi, s23.y, o[3]);
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const float2 ev = f2_unpack(e[v]), ov = f2_unpack(o[v]);
+        E[2 * v] = ev.x;
+        E[2 * v + 1] = ev.y;
+        O[2 * v] = ov.x;
+        O[2 * v + 1] = ov.y;
     }
     const float ny = xs[(Hk * k - 1) * xstride].x;
 #pragma unroll
@@ -496,30 +508,43 @@ __device__ __forceinline__ void synth_chunk8(const float2* __restrict__ xs, int 
 }
 
 // synth_chunk8 for two columns sharing each twiddle load; per output the same
-// sequential FMA chain, hence the same values.
+// sequential FMA chain, hence the same values.  Adjacent outputs (u, u+1) go
+// as one packed fma.rn.f32x2 (two IEEE fmaf), the twiddle pair loaded as one
+// 64-bit operand.
 __device__ __forceinline__ void synth_chunk8x2(const float2* __restrict__ xa, const float2* __restrict__ xb,
                                                int xstride, const float* __restrict__ C2,
                                                const float* __restrict__ S2, int np, int Hk, int n0,
                                                float Ea[8], float Oa[8], float Eb[8], float Ob[8]) {
+    unsigned long long ea[4], oa[4], eb[4], ob[4];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) { Ea[u] = 0.0f; Oa[u] = 0.0f; Eb[u] = 0.0f; Ob[u] = 0.0f; }
+    for (int v = 0; v < 4; ++v) ea[v] = oa[v] = eb[v] = ob[v] = f2_pack(0.0f, 0.0f);
 #pragma unroll 2
     for (int jh = 1; jh < Hk; ++jh) {
         const float2 x = xa[(jh - 1) * xstride];
         const float2 y = xb[(jh - 1) * xstride];
-        const float4 c0 = *reinterpret_cast<const float4*>(C2 + jh * np + n0);
-        const float4 c1 = *reinterpret_cast<const float4*>(C2 + jh * np + n0 + 4);
-        const float4 s0 = *reinterpret_cast<const float4*>(S2 + jh * np + n0);
-        const float4 s1 = *reinterpret_cast<const float4*>(S2 + jh * np + n0 + 4);
-        const float c[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-        const float sv[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
+        const ulonglong2 c01 = *reinterpret_cast<const ulonglong2*>(C2 + jh * np + n0);
+        const ulonglong2 c23 = *reinterpret_cast<const ulonglong2*>(C2 + jh * np + n0 + 4);
+        const ulonglong2 s01 = *reinterpret_cast<const ulonglong2*>(S2 + jh * np + n0);
+        const ulonglong2 s23 = *reinterpret_cast<const ulonglong2*>(S2 + jh * np + n0 + 4);
+        const unsigned long long c[4] = {c01.x, c01.y, c23.x, c23.y};
+        const unsigned long long sv[4] = {s01.x, s01.y, s23.x, s23.y};
+        const unsigned long long xr = f2_pack(x.x, x.x), xi = f2_pack(x.y, x.y);
+        const unsigned long long yr = f2_pack(y.x, y.x), yi = f2_pack(y.y, y.y);
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            Ea[u] = fmaf(x.x, c[u], Ea[u]);
-            Oa[u] = fmaf(x.y, sv[u], Oa[u]);
-            Eb[u] = fmaf(y.x, c[u], Eb[u]);
-            Ob[u] = fmaf(y.y, sv[u], Ob[u]);
+        for (int v = 0; v < 4; ++v) {
+            ea[v] = f2_fma(xr, c[v], ea[v]);
+            oa[v] = f2_fma(xi, sv[v], oa[v]);
+            eb[v] = f2_fma(yr, c[v], eb[v]);
+            ob[v] = f2_fma(yi, sv[v], ob[v]);
         }
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const float2 e0 = f2_unpack(ea[v]), o0 = f2_unpack(oa[v]), e1 = f2_unpack(eb[v]), o1 = f2_unpack(ob[v]);
+        Ea[2 * v] = e0.x; Ea[2 * v + 1] = e0.y;
+        Oa[2 * v] = o0.x; Oa[2 * v + 1] = o0.y;
+        Eb[2 * v] = e1.x; Eb[2 * v + 1] = e1.y;
+        Ob[2 * v] = o1.x; Ob[2 * v + 1] = o1.y;
     }
     const float nya = xa[(Hk - 1) * xstride].x;
     const float nyb = xb[(Hk - 1) * xstride].x;

@@ -244,7 +244,7 @@ struct cs_handle {
     DBuf d_A, d_samp;
     HBuf h_nvalid, h_io;                // pinned: valid counts up; counters + candidate prefix down
     DBuf d_levels, d_tw, d_harms, d_wtab, d_atab, d_ctab, d_nvalid, d_X, d_Q0, d_sigma,
-        d_tmetric, d_items, d_counts, d_cands;
+        d_tmetric, d_items, d_counts, d_cands, d_amax;
     // FP64 plan tables of the last anchor r_lo, already on the device
     bool plan_valid = false;
     double plan_rlo = 0.0;
@@ -590,6 +590,15 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
     int32_t* counts = H->h_io.as<int32_t>();
     DevCand* cand_pre = reinterpret_cast<DevCand*>(H->h_io.as<uint8_t>() + 64);
 
+    // FP16 A tiles: the spectrum's largest component, for their range scale
+    const bool fp16_scale = tensor && !R.interp_only && p.synth == CS_SYNTH_FP16;
+    if (fp16_scale) {
+        CS_CUDA(H->d_amax.ensure(16), "alloc spectrum maximum");
+        CS_CUDA(cudaMemsetAsync(H->d_amax.p, 0, sizeof(uint32_t), H->stream), "reset spectrum maximum");
+        CS_CUDA(launch_amax(H->amps, H->namps, H->d_amax.as<uint32_t>(), H->stream, H->num_sms), "maximum launch");
+        S.launches += 1;
+    }
+
     for (int64_t c0 = 0; c0 < R.nblocks; c0 += WB) {
         const int nb = (int)std::min<int64_t>(WB, R.nblocks - c0);
         WaveArgs a{};
@@ -615,6 +624,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         a.Atile = (tensor && !R.interp_only) ? H->d_A.as<uint8_t>() : nullptr;
         a.tiles_per_blk = tiles_per_blk;
         a.fp16 = p.synth == CS_SYNTH_FP16 ? 1 : 0;
+        a.amax_bits = fp16_scale ? H->d_amax.as<uint32_t>() : nullptr;
         a.samp = R.interp_only ? nullptr : H->d_samp.as<float2>();
         a.Q0 = (H->diag >= 2 && !R.exact_all) ? H->d_Q0.as<float>() : nullptr;   // gate values: diagnostics only
         a.sigma = H->d_sigma.as<float>();
@@ -926,7 +936,7 @@ cs_status cs_destroy(cs_handle* H) {
     cudaSetDevice(H->device);
     if (H->stream) cudaStreamSynchronize(H->stream);
     if (H->own_stream) cudaStreamSynchronize(H->own_stream);
-    DBuf* bufs[] = {&H->d_A, &H->d_samp, &H->d_tcB, &H->amps_owned, &H->d_levels, &H->d_tw, &H->d_harms, &H->d_wtab, &H->d_atab,
+    DBuf* bufs[] = {&H->d_A, &H->d_samp, &H->d_tcB, &H->amps_owned, &H->d_levels, &H->d_tw, &H->d_harms, &H->d_wtab, &H->d_atab, &H->d_amax,
                     &H->d_ctab, &H->d_nvalid, &H->d_X, &H->d_Q0, &H->d_sigma,
                     &H->d_tmetric, &H->d_items, &H->d_counts, &H->d_cands};
     for (DBuf* b : bufs) b->release();

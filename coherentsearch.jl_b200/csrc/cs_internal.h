@@ -90,6 +90,10 @@ struct WaveArgs {
     uint8_t* Atile;         // [nblk][tiles_per_blk] 16-bit A tiles (tensor synthesis) or nullptr
     int32_t tiles_per_blk;
     int32_t fp16;           // A-tile format: 1 = FP16, 0 = BF16
+    // FP16 A tiles: bits of the spectrum's largest |Re| or |Im| (k_amax), from
+    // which a power-of-two scale keeps the tiles inside FP16's range; nullptr:
+    // no scale (BF16 has FP32's range)
+    const uint32_t* amax_bits;
     float2* samp;           // [nblk][nlev][kSampStride]: pooled columns' amplitudes, [jh-1][slot]
     float* Q0;              // [nblk][nlev][Nprof] zero-baseline gate (unscaled by 1/sigma); diagnostics only, may be null
     float* sigma;           // [nblk][nlev]
@@ -253,6 +257,23 @@ __device__ __forceinline__ void push_cand(const WaveArgs& a, int blk, int l, int
 
 __device__ __forceinline__ float inv_sigma(float sig) { return sig > 0.0f ? 1.0f / sig : 0.0f; }
 
+// Exponent s >= 0 of the FP16 A-tile scale 2^-s: the smallest with
+// 16 * amax * 2^-s < 65504.  An interpolated amplitude is at most about
+// 2.7 * sqrt(2) times the largest |Re| or |Im| of the spectrum (the sum of the
+// 16 taps' |sinc| weights), so 16 leaves a further factor 4 of headroom for
+// the tiles.  The gate is linear in the amplitudes: it comes back exactly by
+// 2^s.
+__device__ __forceinline__ int ascale_exp(const uint32_t* amax_bits) {
+    if (!amax_bits) return 0;
+    const float r = __uint_as_float(*amax_bits) * (16.0f / 65504.0f);
+    if (!(r >= 1.0f)) return 0;
+    if (!(r < 1e30f)) return 100;                 // inf or NaN in the spectrum
+    int e;
+    frexpf(r, &e);                                // r = f * 2^e, f in [0.5, 1): r < 2^e
+    return min(e, 100);
+}
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }   // |e| <= 126
+
 // Gate value g (zero-baseline boxcar maximum, not yet divided by sigma) of
 // valid trial j: at or above medcut_gate it goes to the rescan list, else its
 // gate S/N is final (a candidate only if above threshold).
@@ -286,6 +307,8 @@ size_t interp_smem(int win_max, int Nprof);
 cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np, int* err);
 cudaError_t launch_rescue(const WaveArgs& a, cudaStream_t st, int num_sms);
 cudaError_t launch_mstats(const WaveArgs& a, cudaStream_t st);
+// the largest |Re| or |Im| of the spectrum, as float bits, into *out (zeroed by the caller)
+cudaError_t launch_amax(const float2* amps, int64_t n, uint32_t* out, cudaStream_t st, int num_sms);
 
 // block_metrics (reference path): per harmonic, the fine-grid origin, its
 // length (numbins * numbetween) and the reference's range guard.

@@ -134,6 +134,7 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
         const float2* x2 = xo + 2 * Nst;
         const float2* x3 = xo + 3 * Nst;
         const float2 z = make_float2(0.0f, 0.0f);
+        const float sc = a.fp16 ? pow2f(-ascale_exp(a.amax_bits)) : 1.0f;   // exact power of two
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
             const float2 v0 = xo[j];
             const float2 v1 = ng > 1 ? x1[j] : z;
@@ -141,8 +142,8 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
             const float2 v3 = ng > 3 ? x3[j] : z;
             uint4 pk;
             if (a.fp16) {
-                __half2 h0 = __floats2half2_rn(v0.x, v0.y), h1 = __floats2half2_rn(v1.x, v1.y);
-                __half2 h2 = __floats2half2_rn(v2.x, v2.y), h3 = __floats2half2_rn(v3.x, v3.y);
+                __half2 h0 = __floats2half2_rn(v0.x * sc, v0.y * sc), h1 = __floats2half2_rn(v1.x * sc, v1.y * sc);
+                __half2 h2 = __floats2half2_rn(v2.x * sc, v2.y * sc), h3 = __floats2half2_rn(v3.x * sc, v3.y * sc);
                 pk = make_uint4(*reinterpret_cast<uint32_t*>(&h0), *reinterpret_cast<uint32_t*>(&h1),
                                 *reinterpret_cast<uint32_t*>(&h2), *reinterpret_cast<uint32_t*>(&h3));
             } else {
@@ -427,6 +428,25 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
     }
     __syncthreads();
     emit_rows(a, xo, Nst, blk, hidx0, ng, n);
+}
+
+// The largest |Re| or |Im| of a spectrum (NaN ignored), for the FP16 A-tile
+// scale: grid-stride maximum, warp reduction, one atomicMax on the float bits
+// (non-negative floats order like their bits) per warp.
+__global__ void __launch_bounds__(256) k_amax(const float2* __restrict__ amps, int64_t n, uint32_t* out) {
+    float mx = 0.0f;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float2 x = amps[i];
+        mx = fmaxf(mx, fmaxf(fabsf(x.x), fabsf(x.y)));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(mx));
+}
+
+cudaError_t launch_amax(const float2* amps, int64_t n, uint32_t* out, cudaStream_t st, int num_sms) {
+    k_amax<<<num_sms * 4, 256, 0, st>>>(amps, n, out);
+    return cudaGetLastError();
 }
 
 size_t interp_smem(int win_max, int Nprof) { return (size_t)(win_max + kHG * Nprof) * sizeof(float2); }

@@ -234,6 +234,7 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const int tiles_per_blk = a.tiles_per_blk;
+    const float gup = a.fp16 ? pow2f(ascale_exp(a.amax_bits)) : 1.0f;   // undoes the FP16 tile scale
     const int ntiles = a.nblk * tiles_per_blk;
 
     // B once per CTA.
@@ -282,7 +283,8 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
         // the block's per-level sigma and valid counts, for the epilogue (ordered
         // by the barrier below; the previous epilogue finished at the loop's end)
         if (tid < t.nlev) {
-            inv_sh[tid] = inv_sigma(a.sigma[blk * a.nlev + tid]);
+            // 1/sigma times the A tiles' scale 2^s (exact): the gate in true units
+            inv_sh[tid] = inv_sigma(a.sigma[blk * a.nlev + tid]) * gup;
             nv_sh[tid] = a.nvalid[blk * a.nlev + tid];
         }
         // Prefetch the next tile into the other buffer: its previous reader (the
@@ -343,7 +345,7 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
                 if (j >= nv_sh[l]) continue;
                 float g = -INFINITY;
                 for (int i = lu_start[l]; i < lu_start[l + 1]; ++i) g = fmaxf(g, part_sh[lu_idx[i]][r]);
-                if (a.Q0) a.Q0[((int64_t)blk * a.nlev + l) * a.Nprof + j] = g;
+                if (a.Q0) a.Q0[((int64_t)blk * a.nlev + l) * a.Nprof + j] = g * gup;
                 gate_flag(a, blk, l, j, g, inv_sh[l]);
             }
         }

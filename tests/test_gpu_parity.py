@@ -259,6 +259,25 @@ def test_tensor_candidates_identical_to_plain(synth):
     assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("synth", ["bf16", "fp16"])
+def test_tensor_bright_spectrum_scale_invariant(synth):
+    """A spectrum scaled by 2^17 (noise amplitudes ~1e5, past FP16's 65504)
+    reports exactly the unscaled spectrum's candidates: a power of two scales
+    every FP32 value exactly, and the FP16 A tiles carry a power-of-two range
+    scale taken from the spectrum's largest component, undone in the gate."""
+    amps, N, dt = multi_spectrum()
+    big = (amps * np.float32(2.0 ** 17)).astype(np.complex64)
+    assert np.abs(big.real).max() > 65504.0
+    cs = _cs()
+    dec = cs.decimation_set(60, 6)
+    plain = _engine(cs.SearchParams(nharms=60, m=16, decimations=dec, synth="fp32"), amps, N, dt, diag=0)
+    want = plain.search_raw(0.2, 180.0, 100, 2048, 8.0)
+    eng = _engine(cs.SearchParams(nharms=60, m=16, decimations=dec, synth=synth), big, N, dt, diag=0)
+    got = eng.search_raw(0.2, 180.0, 100, 2048, 8.0)
+    assert len(want) > 0
+    assert np.array_equal(got, want)
+
+
 @pytest.mark.parametrize("synth", ["fp32", "fp16"])
 def test_block_ranges_reproduce_the_search(synth):
     """cs_search_range over contiguous block ranges (the multi-GPU shard unit)

@@ -333,7 +333,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--synth", default="fp16", choices=["fp32", "bf16", "fp16"])
+    ap.add_argument("--synth", default="fp16", choices=["fp32", "bf16", "fp16", "bf16_split", "fp16_split"])
     ap.add_argument("--cpu-blocks", type=int, default=None)
     ap.add_argument("--workload", choices=["survey", "dmsweep"], default="survey",
                     help="survey: one 2^23-sample spectrum (the headline); dmsweep: 64 spectra of "
@@ -427,7 +427,8 @@ def main():
     # roofline of the dominant kernel
     dom = max(stage, key=stage.get)
     fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12   # TFLOP/s, nominal
-    tc_flops = trials * 2.0 * 128 * 352     # dense product per trial: 2 * K(128) * N(352 columns)
+    # dense product per trial: 2 * K(128) * N(352 columns), twice over hi and lo when split
+    tc_flops = trials * 2.0 * 128 * 352 * (2 if args.synth.endswith("_split") else 1)
     kname = {"ms_interp": "k_interp", "ms_synth": "k_synth_tc" if args.synth != "fp32" else "k_synth_fp32",
              "ms_sigma": "k_sigma", "ms_rescue": "k_rescue"}[dom]
     traffic = NCU_BYTES_PER_TRIAL.get(kname)

@@ -22,7 +22,7 @@ CS_ERR_TIMEOUT = 6
 CS_ERR_UNSUPPORTED = 7
 CS_MAX_DECIM = 16
 
-CS_SYNTH = {"fp32": 0, "bf16": 1, "fp16": 2}
+CS_SYNTH = {"fp32": 0, "bf16": 1, "fp16": 2, "bf16_split": 3, "fp16_split": 4}
 
 STATUS_NAMES = {
     CS_OK: "CS_OK", CS_ERR_INVALID_ARGUMENT: "CS_ERR_INVALID_ARGUMENT",

@@ -28,7 +28,9 @@ class SearchParams:
     """Tunable search parameters, defaults as src/search.jl:131-144.
 
     ``synth`` selects the device profile-synthesis arithmetic: ``"fp32"`` (the
-    plain FP32 GPU form), ``"bf16"`` or ``"fp16"`` (tensor-core forms).
+    plain FP32 GPU form), ``"bf16"`` or ``"fp16"`` (tensor-core forms), or
+    ``"bf16_split"`` / ``"fp16_split"`` (each amplitude split hi + lo into two
+    16-bit operands: a closer gate for twice the A-tile bytes).
     Equality is identity, as ``SearchCache`` keys on the object.
     """
     nharms: int = 32

@@ -21,6 +21,12 @@
 
 using namespace cs;
 
+namespace {
+// FP16 A tiles (plain or split), and A tiles per 128 trials (2: hi and lo)
+bool synth_fp16(int s) { return s == CS_SYNTH_FP16 || s == CS_SYNTH_FP16_SPLIT; }
+int synth_split(int s) { return (s == CS_SYNTH_BF16_SPLIT || s == CS_SYNTH_FP16_SPLIT) ? 2 : 1; }
+}  // namespace
+
 #define CS_VERSION_STRING "cohsearch-b200 0.1.0 (sm_100a)"
 
 namespace {
@@ -316,7 +322,7 @@ cs_status validate(const cs_params* p) {
         if (p->decimations[i] < 1 || p->nharms / p->decimations[i] < 1) return CS_ERR_INVALID_ARGUMENT;
     if (p->precision != 0 && p->precision != 1) return CS_ERR_INVALID_ARGUMENT;
     if (!(p->boxcar_fsp > 0) || !(p->boxcar_maxfrac > 0)) return CS_ERR_INVALID_ARGUMENT;
-    if (p->synth != CS_SYNTH_FP32 && p->synth != CS_SYNTH_BF16 && p->synth != CS_SYNTH_FP16)
+    if (p->synth < CS_SYNTH_FP32 || p->synth > CS_SYNTH_FP16_SPLIT)
         return CS_ERR_INVALID_ARGUMENT;
     return CS_OK;
 }
@@ -375,8 +381,8 @@ cs_status build_levels(cs_handle* H) {
     CS_CUDA(upload(H->d_levels, H->dlev, H->stream), "upload levels");
     CS_CUDA(upload(H->d_tw, tw, H->stream), "upload twiddles");
     if (p.synth != CS_SYNTH_FP32) {
-        const int rc = prepare_tc(H->dlev.data(), (int)H->dlev.size(), p.nharms, p.synth == CS_SYNTH_FP16,
-                                  &H->tc);
+        const int rc = prepare_tc(H->dlev.data(), (int)H->dlev.size(), p.nharms, synth_fp16(p.synth) ? 1 : 0,
+                                  synth_split(p.synth), &H->tc);
         if (rc != 0)
             return fail(H, CS_ERR_UNSUPPORTED,
                         "tensor-core synthesis needs nharms <= 64, boxcar widths <= 32 and <= 512 TMEM columns");
@@ -494,7 +500,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
     const int tiles_per_blk = (Nprof + 127) / 128;
     const bool want_x = !tensor || R.interp_only;
     const size_t per_blk = (want_x ? (size_t)p.nharms * Nprof * sizeof(float2) : 0) +
-                           (tensor ? (size_t)tiles_per_blk * kATileBytes : 0) +
+                           (tensor ? (size_t)tiles_per_blk * kATileBytes * synth_split(p.synth) : 0) +
                            (size_t)nlev * kSampStride * sizeof(float2) +
                            (size_t)nlev * Nprof * sizeof(float) * (R.exact_all ? 2 : 1) +
                            (size_t)nlev * Nprof * (sizeof(DevItem) + sizeof(DevCand)) + 64;
@@ -514,7 +520,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
 
     if (want_x) CS_CUDA(H->d_X.ensure((size_t)WB * p.nharms * Nprof * sizeof(float2)), "alloc X");
     if (tensor && !R.interp_only) {
-        const size_t abytes = (size_t)WB * tiles_per_blk * kATileBytes;
+        const size_t abytes = (size_t)WB * tiles_per_blk * kATileBytes * synth_split(p.synth);
         if (abytes > H->d_A.bytes) {
             // zero once: the K columns past 2*nharms are never written
             CS_CUDA(H->d_A.ensure(abytes), "alloc A tiles");
@@ -591,7 +597,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
     DevCand* cand_pre = reinterpret_cast<DevCand*>(H->h_io.as<uint8_t>() + 64);
 
     // FP16 A tiles: the spectrum's largest component, for their range scale
-    const bool fp16_scale = tensor && !R.interp_only && p.synth == CS_SYNTH_FP16;
+    const bool fp16_scale = tensor && !R.interp_only && synth_fp16(p.synth);
     if (fp16_scale) {
         CS_CUDA(H->d_amax.ensure(16), "alloc spectrum maximum");
         CS_CUDA(cudaMemsetAsync(H->d_amax.p, 0, sizeof(uint32_t), H->stream), "reset spectrum maximum");
@@ -623,7 +629,8 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         a.X = want_x ? H->d_X.as<float2>() : nullptr;
         a.Atile = (tensor && !R.interp_only) ? H->d_A.as<uint8_t>() : nullptr;
         a.tiles_per_blk = tiles_per_blk;
-        a.fp16 = p.synth == CS_SYNTH_FP16 ? 1 : 0;
+        a.fp16 = synth_fp16(p.synth) ? 1 : 0;
+        a.asplit = synth_split(p.synth);
         a.amax_bits = fp16_scale ? H->d_amax.as<uint32_t>() : nullptr;
         a.samp = R.interp_only ? nullptr : H->d_samp.as<float2>();
         a.Q0 = (H->diag >= 2 && !R.exact_all) ? H->d_Q0.as<float>() : nullptr;   // gate values: diagnostics only
@@ -643,6 +650,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             // A 16-bit gate flags with slack below medcut; the rescan re-forms
             // the FP32 gate and applies medcut itself, so the rescanned set --
             // hence every candidate -- is the plain form's.
+            // (the split modes keep FP16's slack: their gates are closer still)
             const float rel = p.synth == CS_SYNTH_BF16 ? 0.08f : 0.02f;
             const float ab = p.synth == CS_SYNTH_BF16 ? 0.10f : 0.05f;
             a.medcut_gate = R.medcut - (rel * std::fabs(R.medcut) + ab);

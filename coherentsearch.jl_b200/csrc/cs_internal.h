@@ -90,6 +90,8 @@ struct WaveArgs {
     uint8_t* Atile;         // [nblk][tiles_per_blk] 16-bit A tiles (tensor synthesis) or nullptr
     int32_t tiles_per_blk;
     int32_t fp16;           // A-tile format: 1 = FP16, 0 = BF16
+    int32_t asplit;         // 1, or 2: each 128-trial A tile is followed by the tile of the
+                            // amplitudes' rounding residuals (x - hi), in the same format
     // FP16 A tiles: bits of the spectrum's largest |Re| or |Im| (k_amax), from
     // which a power-of-two scale keeps the tiles inside FP16's range; nullptr:
     // no scale (BF16 has FP32's range)
@@ -163,6 +165,7 @@ struct TcArgs {
     int32_t ncols_total;   // columns of the product (multiple of 16)
     int32_t n1;            // N of the first MMA (<= 256); the rest is the second
     int32_t fp16;          // operand format: 1 = FP16, 0 = BF16
+    int32_t split;         // A tiles per 128 trials: 1, or 2 (hi and lo: K runs over both)
 };
 
 struct TcPlanHost {
@@ -172,7 +175,7 @@ struct TcPlanHost {
 };
 
 // Returns 0, or < 0 when the configuration does not fit the tensor path.
-int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, TcPlanHost* out);
+int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, TcPlanHost* out);
 cudaError_t launch_synth_tc(const WaveArgs& a, const TcPlanHost& tp, const void* dB, int* err,
                             cudaStream_t st, int num_sms);
 

@@ -128,8 +128,10 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
     }
     if (a.Atile) {
         // A tile (block, j/128), row r = j%128, K chunk hidx0/4 holds (Re, Im) of
-        // the 4 harmonics: SWIZZLE_NONE K-major core-matrix layout.
-        uint8_t* base = a.Atile + (int64_t)blk * a.tiles_per_blk * kATileBytes + (hidx0 >> 2) * 128;
+        // the 4 harmonics: SWIZZLE_NONE K-major core-matrix layout.  Split
+        // tiles: the tile of residuals x - hi follows each tile.
+        const int tsz = a.asplit * kATileBytes;
+        uint8_t* base = a.Atile + (int64_t)blk * a.tiles_per_blk * tsz + (hidx0 >> 2) * 128;
         const float2* x1 = xo + Nst;
         const float2* x2 = xo + 2 * Nst;
         const float2* x3 = xo + 3 * Nst;
@@ -141,6 +143,31 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
             const float2 v2 = ng > 2 ? x2[j] : z;
             const float2 v3 = ng > 3 ? x3[j] : z;
             uint4 pk;
+            const uint32_t off = (uint32_t)(j >> 7) * (uint32_t)tsz + ((uint32_t)(j & 127) >> 3) * 2048u +
+                                 (uint32_t)(j & 7) * 16u;
+            if (a.asplit == 2) {
+                const float2 vv[4] = {v0, v1, v2, v3};
+                uint32_t hw[4], lw[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (a.fp16) {
+                        const float xr = vv[q].x * sc, xi = vv[q].y * sc;
+                        const __half2 h = __floats2half2_rn(xr, xi);
+                        const __half2 lo = __floats2half2_rn(xr - __low2float(h), xi - __high2float(h));
+                        hw[q] = *reinterpret_cast<const uint32_t*>(&h);
+                        lw[q] = *reinterpret_cast<const uint32_t*>(&lo);
+                    } else {
+                        const __nv_bfloat162 h = __floats2bfloat162_rn(vv[q].x, vv[q].y);
+                        const __nv_bfloat162 lo =
+                            __floats2bfloat162_rn(vv[q].x - __low2float(h), vv[q].y - __high2float(h));
+                        hw[q] = *reinterpret_cast<const uint32_t*>(&h);
+                        lw[q] = *reinterpret_cast<const uint32_t*>(&lo);
+                    }
+                }
+                *reinterpret_cast<uint4*>(base + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                *reinterpret_cast<uint4*>(base + off + kATileBytes) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                continue;
+            }
             if (a.fp16) {
                 __half2 h0 = __floats2half2_rn(v0.x * sc, v0.y * sc), h1 = __floats2half2_rn(v1.x * sc, v1.y * sc);
                 __half2 h2 = __floats2half2_rn(v2.x * sc, v2.y * sc), h3 = __floats2half2_rn(v3.x * sc, v3.y * sc);
@@ -152,8 +179,6 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
                 pk = make_uint4(*reinterpret_cast<uint32_t*>(&h0), *reinterpret_cast<uint32_t*>(&h1),
                                 *reinterpret_cast<uint32_t*>(&h2), *reinterpret_cast<uint32_t*>(&h3));
             }
-            const uint32_t off = (uint32_t)(j >> 7) * (uint32_t)kATileBytes + ((uint32_t)(j & 127) >> 3) * 2048u +
-                                 (uint32_t)(j & 7) * 16u;
             *reinterpret_cast<uint4*>(base + off) = pk;
         }
     }

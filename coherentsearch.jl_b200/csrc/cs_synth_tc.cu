@@ -219,8 +219,12 @@ template <int HM>
 __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs t, const uint4* __restrict__ Bg,
                                                       int* err) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* As0 = smem;                      // two A buffers, kABytes each
-    uint8_t* Bs = smem + 2 * kABytes;         // ncols_total * kK * 2
+    const int abytes = kABytes * t.split;     // one tile's A bytes (hi, then lo when split)
+    // two A buffers (the next tile arrives during this tile's MMA); split tiles
+    // take one, refilled as soon as the MMA has read it (during the epilogue)
+    const int nbuf = t.split == 2 ? 1 : 2;
+    uint8_t* As0 = smem;                      // nbuf A buffers, abytes each
+    uint8_t* Bs = smem + nbuf * abytes;       // ncols_total * kK * 2
     __shared__ uint64_t mbar;                 // MMA completion
     __shared__ uint64_t lbar[2];              // A-tile arrival, one per buffer
     __shared__ uint32_t tmem_base_sh;
@@ -273,11 +277,11 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     uint32_t phase = 0;
     bool ok = true;
     if (tid == 0 && (int)blockIdx.x < ntiles)
-        bulk_load(smem_u32(As0), a.Atile + (int64_t)blockIdx.x * kABytes, kABytes, &lbar[0]);
+        bulk_load(smem_u32(As0), a.Atile + (int64_t)blockIdx.x * abytes, abytes, &lbar[0]);
 
     int it = 0;
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
-        const int buf = it & 1;
+        const int buf = nbuf == 2 ? (it & 1) : 0;
         const int blk = tile / tiles_per_blk;
         const int j0 = (tile % tiles_per_blk) * kTM;
         // the block's per-level sigma and valid counts, for the epilogue (ordered
@@ -289,15 +293,15 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
         }
         // Prefetch the next tile into the other buffer: its previous reader (the
         // MMA of the last iteration) has completed.
-        if (tid == 0 && tile + (int)gridDim.x < ntiles)
-            bulk_load(smem_u32(As0 + (buf ^ 1) * kABytes), a.Atile + (int64_t)(tile + gridDim.x) * kABytes,
-                      kABytes, &lbar[buf ^ 1]);
-        ok = __syncthreads_and(mbar_wait(&lbar[buf], (uint32_t)((it >> 1) & 1))) != 0;
+        if (nbuf == 2 && tid == 0 && tile + (int)gridDim.x < ntiles)
+            bulk_load(smem_u32(As0 + (buf ^ 1) * abytes), a.Atile + (int64_t)(tile + gridDim.x) * abytes,
+                      abytes, &lbar[buf ^ 1]);
+        ok = __syncthreads_and(mbar_wait(&lbar[buf], (uint32_t)(nbuf == 2 ? ((it >> 1) & 1) : (it & 1)))) != 0;
         if (!ok) {
             if (tid == 0) atomicExch(err, 2);
             break;
         }
-        const uint32_t a_addr = smem_u32(As0 + buf * kABytes);
+        const uint32_t a_addr = smem_u32(As0 + buf * abytes);
 
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -306,10 +310,13 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
                 const int ncol0 = part ? t.n1 : 0;
                 const int nn = part ? t.ncols_total - t.n1 : t.n1;
                 const uint32_t idesc = idesc_base | ((uint32_t)(nn >> 3) << 17);
-                for (int ks = 0; ks < kK / 16; ++ks) {
-                    const uint64_t da = umma_desc(a_addr + ks * 256);
+                // split: the hi tile's K steps, then the lo tile's against the
+                // same twiddles, into one FP32 accumulator
+                for (int kk = 0; kk < t.split * (kK / 16); ++kk) {
+                    const int sp = kk / (kK / 16), ks = kk - sp * (kK / 16);
+                    const uint64_t da = umma_desc(a_addr + sp * kABytes + ks * 256);
                     const uint64_t db = umma_desc(b_addr + (ncol0 / 8) * kSBO + ks * 256);
-                    const uint32_t acc = ks > 0;
+                    const uint32_t acc = kk > 0;
                     asm volatile(
                         "{\n\t.reg .pred p;\n\t"
                         "setp.ne.b32 p, %4, 0;\n\t"
@@ -323,6 +330,9 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
         ok = __syncthreads_and(mbar_wait(&mbar, phase)) != 0;
         if (!ok && tid == 0) atomicExch(err, 2);
         if (ok) phase ^= 1u;
+        // one buffer: the MMA has read it, so the next tile may land now
+        if (ok && nbuf == 1 && tid == 0 && tile + (int)gridDim.x < ntiles)
+            bulk_load(smem_u32(As0), a.Atile + (int64_t)(tile + gridDim.x) * abytes, abytes, &lbar[0]);
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
         if (ok) {
@@ -378,12 +388,13 @@ static uint16_t to_half_bits(float v, int fp16) {
     return *reinterpret_cast<uint16_t*>(&b);
 }
 
-int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, TcPlanHost* out) {
+int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, TcPlanHost* out) {
     if (2 * nharms > kK) return -1;
     TcArgs& t = out->args;
     t = TcArgs{};
     t.nlev = nlev;
     t.fp16 = fp16;
+    t.split = split;
     int wmax = 0;
     for (int l = 0; l < nlev; ++l) wmax = wmax > dl[l].wmax ? wmax : dl[l].wmax;
     t.hm = wmax <= 8 ? 8 : (wmax <= 32 ? 32 : 0);
@@ -478,7 +489,7 @@ int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, TcPlanHost* o
             }
         }
     }
-    out->smem = (size_t)2 * kABytes + (size_t)total * kK * 2;
+    out->smem = (size_t)(split == 2 ? 1 : 2) * kABytes * split + (size_t)total * kK * 2;
     return 0;
 }
 

@@ -39,7 +39,8 @@ struct CSCandidate
     trial::Int64
 end
 
-# synth: 0 = plain FP32, 1 = BF16 tensor cores, 2 = FP16 tensor cores.
+# synth: 0 = plain FP32, 1 = BF16 tensor cores, 2 = FP16 tensor cores,
+# 3 / 4 = BF16 / FP16 with each amplitude split hi + lo into two operands.
 function CSParams(p; synth::Integer=2)
     d = ntuple(i -> i <= length(p.decimations) ? Int32(p.decimations[i]) : Int32(0), 16)
     CSParams(p.nharms, p.m, p.numbetween, length(p.decimations), d, p.hidr, p.threshold,

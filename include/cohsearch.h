@@ -46,7 +46,10 @@ enum { CS_MAX_DECIM = 16 };
 typedef enum cs_synth {
     CS_SYNTH_FP32 = 0,   /* plain FP32 SIMT synthesis ("plain FP32 GPU form") */
     CS_SYNTH_BF16 = 1,   /* tcgen05 tensor-core product, BF16 operands, FP32 accumulate */
-    CS_SYNTH_FP16 = 2    /* tcgen05 tensor-core product, FP16 operands, FP32 accumulate */
+    CS_SYNTH_FP16 = 2,   /* tcgen05 tensor-core product, FP16 operands, FP32 accumulate */
+    CS_SYNTH_BF16_SPLIT = 3,  /* as BF16 with each amplitude split hi + lo (two BF16 operands,
+                                 twice the A-tile bytes): about 16 significant bits */
+    CS_SYNTH_FP16_SPLIT = 4   /* as FP16 with the hi + lo split: about 22 significant bits */
 } cs_synth;
 
 /* Mirrors SearchParams (src/search.jl:131-144). */

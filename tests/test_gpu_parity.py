@@ -243,7 +243,7 @@ def test_tensor_gate_tracks_fp32_gate(synth):
     assert np.all(np.abs(gtc - g32) <= rel * np.abs(g32) + ab)
 
 
-@pytest.mark.parametrize("synth", ["bf16", "fp16"])
+@pytest.mark.parametrize("synth", ["bf16", "fp16", "bf16_split", "fp16_split"])
 def test_tensor_candidates_identical_to_plain(synth):
     """Every trial near the threshold is rescored by the same exact FP32 path,
     so the mixed form reports exactly the plain form's candidates."""

@@ -11,7 +11,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SOURCES = ["csrc/cs_api.cu", "csrc/cs_kernels.cu", "csrc/cs_synth_tc.cu", "csrc/cs_block.cu"]
+SOURCES = ["csrc/cs_api.cu", "csrc/cs_kernels.cu", "csrc/cs_synth_tc.cu", "csrc/cs_block.cu", "csrc/cs_mlp.cu"]
 OUT = os.path.join(HERE, "lib", "libcohsearch_cuda.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

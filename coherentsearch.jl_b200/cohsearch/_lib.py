@@ -86,6 +86,20 @@ class cs_stats(ctypes.Structure):
                [(n, ctypes.c_int64) for n in ("h2d_bytes", "d2h_bytes")]
 
 
+class cs_mlp(ctypes.Structure):
+    _fields_ = [("din", ctypes.c_int32), ("dh", ctypes.c_int32), ("w1", ctypes.c_void_p), ("b1", ctypes.c_void_p),
+                ("w2", ctypes.c_void_p), ("b2", ctypes.c_void_p), ("w3", ctypes.c_void_p), ("b3", ctypes.c_void_p)]
+
+
+class cs_mlp_grads(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in ("w1", "b1", "w2", "b2", "w3", "b3")]
+
+
+class cs_adam_param(ctypes.Structure):
+    _fields_ = [("master", ctypes.c_void_p), ("bf16", ctypes.c_void_p), ("m", ctypes.c_void_p),
+                ("v", ctypes.c_void_p), ("grad", ctypes.c_void_p), ("n", ctypes.c_int64)]
+
+
 _P = ctypes.c_void_p
 _i32 = ctypes.c_int32
 _i64 = ctypes.c_int64
@@ -120,6 +134,13 @@ PROTOTYPES = {
     "cs_get_metric_hists": (_i32, [_P, ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(_i32), _P, _P,
                                    _P, _P]),
     "cs_set_metricnorm": (_i32, [_P, _i32, _i32, _P, _P, _P, _P]),
+    "cs_search_blocks": (_i32, [_P, _f64, _f64, _i64, _i64, _f64, _P, _i64, _P, _i64, ctypes.POINTER(_i64)]),
+    "cs_block_features": (_i32, [_P, _f64, _f64, _i64, _i64, _P, _i64, ctypes.POINTER(_i64), ctypes.POINTER(_i32)]),
+    "cs_mlp_forward": (_i32, [ctypes.POINTER(cs_mlp), _P, _i64, _P, _P, _P, _P]),
+    "cs_mlp_backward": (_i32, [ctypes.POINTER(cs_mlp), _P, _P, _P, _P, _P, _i64, ctypes.c_float, _P, _P, _P,
+                               ctypes.POINTER(cs_mlp_grads), _P, _P]),
+    "cs_adam_step": (_i32, [_P, _i32, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _i32, _P]),
+    "cs_mlp_to_bf16": (_i32, [_P, _P, _i64, _P]),
 }
 
 _lib = None

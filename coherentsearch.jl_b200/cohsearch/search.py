@@ -270,6 +270,37 @@ class Engine:
             _lib.check(st, self._h, "cs_search")
             return out[:n.value].copy()
 
+    def search_blocks_raw(self, block_list, lofreq=0.1, hifreq=100.0, lobin=100, blocksize=2048, threshold=None,
+                          cap=1 << 16) -> np.ndarray:
+        """Raw detections of the listed blocks of the band's grid only
+        (cs_search_blocks): each block exactly as in the whole search."""
+        thr = self.params.threshold if threshold is None else threshold
+        bl = np.ascontiguousarray(np.unique(np.asarray(block_list, np.int64)))
+        while True:
+            out = np.empty(cap, dtype=_lib.CAND_DTYPE)
+            n = ctypes.c_int64()
+            st = self.lib.cs_search_blocks(self._h, float(lofreq), float(hifreq), int(lobin), int(blocksize),
+                                           float(thr), bl.ctypes.data, len(bl), out.ctypes.data, cap,
+                                           ctypes.byref(n))
+            if st == _lib.CS_ERR_CAPACITY and n.value > cap:
+                cap = int(n.value)
+                continue
+            _lib.check(st, self._h, "cs_search_blocks")
+            return out[:n.value].copy()
+
+    def block_features(self, lofreq=0.1, hifreq=100.0, lobin=100, blocksize=2048):
+        """Incoherent power-sum features of every block of the band
+        (cs_block_features): a float32 CUDA tensor [nblocks, sum of Hk]."""
+        import torch
+        n, nf = ctypes.c_int64(), ctypes.c_int32()
+        self.lib.cs_block_features(self._h, float(lofreq), float(hifreq), int(lobin), int(blocksize), None, 0,
+                                   ctypes.byref(n), ctypes.byref(nf))
+        out = torch.empty((max(1, n.value), nf.value), dtype=torch.float32, device=f"cuda:{self.device}")
+        _lib.check(self.lib.cs_block_features(self._h, float(lofreq), float(hifreq), int(lobin), int(blocksize),
+                                              out.data_ptr(), n.value, ctypes.byref(n), ctypes.byref(nf)), self._h,
+                   "cs_block_features")
+        return out[:n.value]
+
     def search_batch_raw(self, spectra, lofreq=0.1, hifreq=100.0, lobin=100, blocksize=2048, threshold=None,
                          on_device=False, cap=1 << 18):
         """cs_search_batch over `spectra`, a list of (amps, N, dt): amps a

@@ -50,6 +50,38 @@ def make_spectrum(nsamp: int, dt: float, pulsars: Sequence[Pulsar] = (), seed: i
     return amps
 
 
+def make_spectrum_fd(nsamp: int, dt: float, pulsars: Sequence[Pulsar] = (), seed: int = 0,
+                     halfwidth: int = 8) -> np.ndarray:
+    """The make_spectrum model synthesised in the frequency domain, in
+    milliseconds instead of seconds (training sets of many spectra): bins of
+    unit-variance complex Gaussian noise (E|X|^2 = 1), plus for each pulsar and
+    harmonic h the Gaussian train's Fourier coefficient
+    a_h = amp * 1.0645 * duty * exp(-(pi h duty)^2 / (4 ln 2)) * exp(2 pi i h phase)
+    (amp as in make_spectrum) times sqrt(nsamp) times the response of a
+    finite-length sinusoid at fractional bin r = h f T, sinc(r - k) e^{i pi (r - k)},
+    over the `halfwidth` bins either side of r."""
+    rng = np.random.default_rng(seed)
+    nb = nsamp // 2
+    amps = ((rng.standard_normal(nb) + 1j * rng.standard_normal(nb)) * np.sqrt(0.5)).astype(np.complex128)
+    T = nsamp * dt
+    for p in pulsars:
+        amp = p.snr / np.sqrt(nsamp * 1.0645 * p.duty)
+        hmax = int(min(np.floor((nb - halfwidth - 1) / (p.freq * T)),
+                       np.ceil(3.0 * np.sqrt(4.0 * np.log(2.0)) / (np.pi * p.duty))))
+        if hmax < 1:
+            continue
+        h = np.arange(1, hmax + 1)
+        ah = (amp * 1.0645 * p.duty * np.exp(-(np.pi * h * p.duty) ** 2 / (4.0 * np.log(2.0)))
+              * np.exp(2j * np.pi * h * p.phase) * np.sqrt(nsamp))
+        r = h * p.freq * T
+        k = np.floor(r)[:, None].astype(np.int64) + np.arange(-halfwidth + 1, halfwidth + 1)[None, :]
+        d = r[:, None] - k
+        resp = np.sinc(d) * np.exp(1j * np.pi * d)
+        ok = (k >= 1) & (k < nb)
+        np.add.at(amps, k[ok], (ah[:, None] * resp)[ok])
+    return amps.astype(np.complex64)
+
+
 def random_pulsars(rng: np.random.Generator, n: int, fmin: float, fmax: float, dmin: float,
                    dmax: float, smin: float, smax: float) -> List[Pulsar]:
     """Log-uniform frequency and duty, uniform S/N and phase."""

@@ -249,8 +249,9 @@ struct cs_handle {
     DBuf d_tcB;
     DBuf d_A, d_samp;
     HBuf h_nvalid, h_io;                // pinned: valid counts up; counters + candidate prefix down
+    HBuf h_bmap;                        // pinned: a wave's block map (block-list search)
     DBuf d_levels, d_tw, d_harms, d_wtab, d_atab, d_ctab, d_nvalid, d_X, d_Q0, d_sigma,
-        d_tmetric, d_items, d_counts, d_cands, d_amax;
+        d_tmetric, d_items, d_counts, d_cands, d_amax, d_bmap;
     // FP64 plan tables of the last anchor r_lo, already on the device
     bool plan_valid = false;
     double plan_rlo = 0.0;
@@ -424,6 +425,7 @@ struct RunSpec {
     double r_hi = 0.0;    // band end (Fourier bins) and observation time, for the
     double T = 0.0;       // frequency windows
     double threshold_d = 0.0;
+    const int64_t* blist = nullptr;   // search of a block list: band block indices (ascending), nblocks of them
 };
 
 // _logedges (src/search.jl:1406-1411): nwin+1 log-spaced edges over [a, b].
@@ -578,7 +580,13 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
     S.h2d_bytes = H->spec_h2d_bytes + plan_bytes;
     H->spec_h2d_bytes = 0;
     S.blocks = R.nblocks;
-    S.trials = R.t_end - R.t_base;
+    if (R.blist) {
+        S.trials = 0;
+        for (int64_t c = 0; c < R.nblocks; ++c)
+            S.trials += std::min<int64_t>(Nprof, R.t_end - R.blist[c] * (int64_t)Nprof);
+    } else {
+        S.trials = R.t_end - R.t_base;
+    }
     if (R.keep_diag) {
         H->last_sigma.assign((size_t)R.nblocks * nlev, 0.0f);
         H->last_nvalid.assign((size_t)R.nblocks * nlev, 0);
@@ -688,9 +696,10 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         int32_t* nvalid = H->h_nvalid.as<int32_t>();
         for (int b = 0; b < nb; ++b) {
             const int64_t c = c0 + b;
-            const int64_t i0 = c * (int64_t)Nprof;  // trial offset of the block
-            const int n = (int)std::min<int64_t>(Nprof, R.t_end - (R.t_base + i0));
-            const double rstart = R.r_lo + (double)(R.t_base + i0) * R.lodr;
+            // global trial of the block's first trial
+            const int64_t tb = R.blist ? R.blist[c] * (int64_t)Nprof : R.t_base + c * (int64_t)Nprof;
+            const int n = (int)std::min<int64_t>(Nprof, R.t_end - tb);
+            const double rstart = R.r_lo + (double)tb * R.lodr;
             for (int l = 0; l < nlev; ++l) {
                 const int k = H->dlev[l].k;
                 nvalid[(size_t)b * nlev + l] = (k == 1) ? n : nvalid_decim(k, rstart, R.lodr, n, nyq);
@@ -709,6 +718,15 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             CS_CUDA(cudaMemcpyAsync(H->d_mwin.p, mwin, (size_t)nb * nlev * sizeof(int32_t), cudaMemcpyHostToDevice,
                                     H->stream),
                     "upload block windows");
+        if (R.blist) {
+            CS_CUDA(H->h_bmap.ensure((size_t)nb * sizeof(int64_t)), "pinned block map");
+            std::copy(R.blist + c0, R.blist + c0 + nb, H->h_bmap.as<int64_t>());
+            CS_CUDA(H->d_bmap.ensure((size_t)WB * sizeof(int64_t)), "alloc block map");
+            CS_CUDA(cudaMemcpyAsync(H->d_bmap.p, H->h_bmap.p, (size_t)nb * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                    H->stream),
+                    "upload block map");
+            a.blk_map = H->d_bmap.as<int64_t>();
+        }
         CS_CUDA(cudaMemsetAsync(H->d_counts.p, 0, 4 * sizeof(int32_t), H->stream), "reset counters");
         if (!R.interp_only) {
             CS_CUDA(cudaMemcpyAsync(H->d_nvalid.p, nvalid, (size_t)nb * nlev * sizeof(int32_t),
@@ -944,11 +962,12 @@ cs_status cs_destroy(cs_handle* H) {
     cudaSetDevice(H->device);
     if (H->stream) cudaStreamSynchronize(H->stream);
     if (H->own_stream) cudaStreamSynchronize(H->own_stream);
-    DBuf* bufs[] = {&H->d_A, &H->d_samp, &H->d_tcB, &H->amps_owned, &H->d_levels, &H->d_tw, &H->d_harms, &H->d_wtab, &H->d_atab, &H->d_amax,
+    DBuf* bufs[] = {&H->d_A, &H->d_samp, &H->d_tcB, &H->amps_owned, &H->d_levels, &H->d_tw, &H->d_harms, &H->d_wtab, &H->d_atab, &H->d_amax, &H->d_bmap,
                     &H->d_ctab, &H->d_nvalid, &H->d_X, &H->d_Q0, &H->d_sigma,
                     &H->d_tmetric, &H->d_items, &H->d_counts, &H->d_cands};
     for (DBuf* b : bufs) b->release();
     H->h_nvalid.release();
+    H->h_bmap.release();
     H->h_io.release();
     H->h_mwin.release();
     H->h_mst.release();
@@ -1013,7 +1032,7 @@ namespace {
 // grid; candidates appended to `outv` in the reference's order.
 cs_status search_core(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
                       double threshold, int32_t exact_all, int64_t block_begin, int64_t block_end,
-                      std::vector<cs_candidate>* outv) {
+                      std::vector<cs_candidate>* outv, const int64_t* blist = nullptr, int64_t nlist = 0) {
     if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");
     CS_CUDA(cudaSetDevice(H->device), "set device");
     const cs_params& p = H->p;
@@ -1035,14 +1054,26 @@ cs_status search_core(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
     // blocks, sigmas and candidates of the whole search.
     const int64_t nblk_all = (total + Nprof - 1) / Nprof;
     const int64_t b1 = block_end < 0 ? nblk_all : std::min(block_end, nblk_all);
-    if (block_begin >= b1) return CS_OK;
+    if (blist) {
+        // a list of the band's blocks: ascending, inside the band
+        for (int64_t i = 0; i < nlist; ++i)
+            if (blist[i] < 0 || blist[i] >= nblk_all || (i > 0 && blist[i] <= blist[i - 1]))
+                return fail(H, CS_ERR_INVALID_ARGUMENT, "block list must ascend strictly within the band's blocks");
+        if (H->ms_on || H->norm_on)
+            return fail(H, CS_ERR_UNSUPPORTED, "metric statistics and normalisation need contiguous blocks");
+        if (nlist == 0) return CS_OK;
+        block_begin = 0;
+    } else if (block_begin >= b1) {
+        return CS_OK;
+    }
     RunSpec R{};
     R.r_lo = r_lo;
     R.lodr = lodr;
     R.Nprof = Nprof;
-    R.nblocks = b1 - block_begin;
+    R.nblocks = blist ? nlist : b1 - block_begin;
     R.t_base = block_begin * Nprof;
-    R.t_end = std::min(total, b1 * Nprof);
+    R.t_end = blist ? total : std::min(total, b1 * Nprof);
+    R.blist = blist;
     R.nlev = (int)H->levels.size();
     R.stats = H->ms_on;
     R.norm = H->norm_on;
@@ -1097,6 +1128,53 @@ cs_status search_core(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
 }  // namespace
 
 extern "C" {
+
+cs_status cs_search_blocks(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
+                           double threshold, const int64_t* blocks, int64_t nblocks, cs_candidate* out, int64_t cap,
+                           int64_t* n_out) {
+    if (!H || !n_out || (cap > 0 && !out) || cap < 0 || nblocks < 0 || (nblocks > 0 && !blocks))
+        return CS_ERR_INVALID_ARGUMENT;
+    *n_out = 0;
+    std::vector<cs_candidate> v;
+    cs_status st = search_core(H, lofreq, hifreq, lobin, blocksize, threshold, 0, 0, -1, &v, blocks, nblocks);
+    if (st != CS_OK) return st;
+    const int64_t n = (int64_t)v.size();
+    std::copy_n(v.begin(), std::min(n, cap), out);
+    *n_out = n;
+    if (n > cap) return fail(H, CS_ERR_CAPACITY, "candidate array too small");
+    return CS_OK;
+}
+
+cs_status cs_block_features(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
+                            float* d_out, int64_t cap_blocks, int64_t* nblocks_out, int32_t* nfeat_out) {
+    if (!H || !nblocks_out || !nfeat_out || cap_blocks < 0 || (cap_blocks > 0 && !d_out))
+        return CS_ERR_INVALID_ARGUMENT;
+    *nblocks_out = 0;
+    int nfeat = 0;
+    for (const DevLevel& L : H->dlev) nfeat += L.Hk;
+    *nfeat_out = nfeat;
+    if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");
+    if (blocksize < 1 || blocksize > (1 << 16)) return fail(H, CS_ERR_UNSUPPORTED, "blocksize must be 1..65536");
+    CS_CUDA(cudaSetDevice(H->device), "set device");
+    // the band's trial grid, as search_core
+    const double T = (double)H->N * H->dt;
+    const double lodr = H->p.hidr / (double)H->p.nharms;
+    double r_lo = lofreq * T;
+    if (lobin != 100) r_lo = (double)lobin;
+    const double span = std::floor((hifreq * T - r_lo) / lodr);
+    if (!(span == span) || span > 4.0e15) return fail(H, CS_ERR_INVALID_ARGUMENT, "band is not finite");
+    const int64_t total = std::max<int64_t>(0, (int64_t)span + 1);
+    const int64_t nb = (total + blocksize - 1) / blocksize;
+    *nblocks_out = nb;
+    if (nb > cap_blocks) return fail(H, CS_ERR_CAPACITY, "feature array too small");
+    if (nb == 0) return CS_OK;
+    const cudaError_t e = launch_features(H->amps, H->namps, r_lo, lodr, blocksize, total,
+                                          H->d_levels.as<DevLevel>(), (int)H->dlev.size(), nfeat, d_out, H->stream);
+    if (e == cudaErrorInvalidValue) return fail(H, CS_ERR_UNSUPPORTED, "more than 512 features per block");
+    CS_CUDA(e, "features launch");
+    CS_CUDA(cudaStreamSynchronize(H->stream), "features");
+    return CS_OK;
+}
 
 cs_status cs_search_range(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
                           double threshold, int32_t exact_all, int64_t block_begin, int64_t block_end,

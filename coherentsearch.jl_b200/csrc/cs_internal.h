@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "cohsearch.h"
+
 #include <vector>
 
 namespace cs {
@@ -79,6 +81,7 @@ struct WaveArgs {
     int64_t total;          // trials in the whole search
     int32_t nblk;           // blocks in this wave
     int32_t blk_base;       // index of the wave's first block in the search
+    const int64_t* blk_map; // search of a block list: wave block -> band block (trial anchor 0), or nullptr
     const DevHarm* harms;
     const float* wtab;
     const float2* atab;
@@ -246,11 +249,16 @@ __device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_
 // Candidates and the medcut test of a gate value (boxcar_metrics!,
 // src/search.jl:825-843), shared by both synthesis kernels' epilogues.
 // ---------------------------------------------------------------------------
+// Global trial of wave block blk's first trial.
+__device__ __forceinline__ int64_t blk_t0(const WaveArgs& a, int blk) {
+    return a.blk_map ? a.blk_map[blk] * (int64_t)a.Nprof : a.t_first + (int64_t)blk * a.Nprof;
+}
+
 __device__ __forceinline__ void push_cand(const WaveArgs& a, int blk, int l, int j, float metric) {
     const int pos = atomicAdd(a.n_cands, 1);
     if (pos < a.cap_cands) {
         DevCand c;
-        c.blk = a.blk_base + blk;
+        c.blk = a.blk_map ? (int32_t)a.blk_map[blk] : a.blk_base + blk;
         c.lev = l;
         c.j = j;
         c.metric = metric;
@@ -311,6 +319,15 @@ cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max
 cudaError_t launch_rescue(const WaveArgs& a, cudaStream_t st, int num_sms);
 cudaError_t launch_mstats(const WaveArgs& a, cudaStream_t st);
 // the largest |Re| or |Im| of the spectrum, as float bits, into *out (zeroed by the caller)
+cudaError_t launch_features(const float2* amps, int64_t namps, double r_lo, double lodr, int64_t Nprof, int64_t total,
+                            const DevLevel* levels, int nlev, int nfeat, float* out, cudaStream_t st);
+cudaError_t launch_mlp_forward(const cs_mlp& net, const float* x, int64_t n, float* h1, float* h2, float* z,
+                               cudaStream_t st);
+cudaError_t launch_mlp_backward(const cs_mlp& net, const float* x, const float* h1, const float* h2, const float* z,
+                                const float* y, int64_t n, float pos_weight, float* dz, float* dh1, float* dh2,
+                                const cs_mlp_grads& g, float* loss, cudaStream_t st);
+cudaError_t launch_adam(const cs_adam_param& p, float lr, float b1, float b2, float eps, int step, cudaStream_t st);
+cudaError_t launch_to_bf16(const float* p, uint16_t* pb, int64_t n, cudaStream_t st);
 cudaError_t launch_amax(const float2* amps, int64_t n, uint32_t* out, cudaStream_t st, int num_sms);
 
 // block_metrics (reference path): per harmonic, the fine-grid origin, its

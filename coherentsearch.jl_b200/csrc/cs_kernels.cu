@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
     const int blk = blockIdx.y;
     const int m = M > 0 ? M : a.m;
     const int m2 = m / 2;
-    const int64_t t0 = a.t_first + (int64_t)blk * a.Nprof;
+    const int64_t t0 = blk_t0(a, blk);
     const int n = (int)min((int64_t)a.Nprof, a.total - t0);
     if (n <= 0) return;
 
@@ -912,7 +912,7 @@ cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max
 // no contraction), its window w = clamp(searchsortedlast(edges, f), 1, nwin),
 // and z = (M - loc[w]) / scale[w] against the threshold.
 __device__ bool norm_pass(const WaveArgs& a, int blk, int l, int k, int j, float metric) {
-    const int64_t i0 = a.t_first + (int64_t)blk * a.Nprof;
+    const int64_t i0 = blk_t0(a, blk);
     const double rstart = __dadd_rn(a.r_lo, __dmul_rn((double)i0, a.lodr));
     const double rf = __dadd_rn(rstart, __dmul_rn((double)j, a.lodr));
     const double r = k == 1 ? rf : __dmul_rn((double)k, rf);
@@ -968,7 +968,7 @@ __global__ void __launch_bounds__(32 * kRescueWarps) k_rescue(WaveArgs a) {
         const int k = L.k, Hk = L.Hk, nbins = L.nbins, np = L.np, nw = L.nw, wmax = L.wmax;
         float metric = 0.0f;
         if (invsig > 0.0f) {
-            const int64_t t0 = a.t_first + (int64_t)blk * a.Nprof;
+            const int64_t t0 = blk_t0(a, blk);
             const int n = (int)min((int64_t)a.Nprof, a.total - t0);
             const int64_t t = t0 + j;
             for (int jh = 1 + lane; jh <= Hk; jh += 32) {

@@ -149,6 +149,83 @@ cs_status cs_search_range(cs_handle* h, double lofreq, double hifreq, int64_t lo
                           double threshold, int32_t exact_all, int64_t block_begin, int64_t block_end,
                           cs_candidate* out, int64_t cap, int64_t* n_out);
 
+/* cs_search restricted to the listed blocks of the band's grid (strictly
+ * ascending indices): each block's sigma and candidates are exactly the whole
+ * search's, as with cs_search_range.  The re-search of the blocks a learned
+ * proposal picks.  No counterpart in the reference (its chunk loop,
+ * src/search.jl:1768-1894, runs over every chunk).  Not with metric
+ * statistics or normalisation. */
+cs_status cs_search_blocks(cs_handle* h, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
+                           double threshold, const int64_t* blocks, int64_t nblocks, cs_candidate* out, int64_t cap,
+                           int64_t* n_out);
+
+/* ---------------------------------------------------------------------------
+ * Learned block proposal.  No counterpart in the reference: a small network
+ * scores the band's blocks from cheap incoherent features, and the coherent
+ * search re-searches the proposed blocks (cs_search_blocks).  All pointers
+ * with a d_ prefix are device memory the caller owns; stream may be null.
+ * ------------------------------------------------------------------------- */
+
+/* Per block of the band (blocks of blocksize trials from the band's start, as
+ * cs_search), one feature per (decimation level k with Hk harmonics, H = 1..Hk),
+ * levels in the handle's order: the incoherent power sum
+ * S(r) = sum_{i<=H} |X[rint(i*k*r)]|^2 of the attached (normalised) spectrum at
+ * every trial r of the block, as z = (S - H)/sqrt(H), and the feature is
+ * asinh(max over the block of z) -- the incoherent counterpart of every sum
+ * the coherent search forms.  d_out [nblocks][nfeat]; *nblocks_out and
+ * *nfeat_out (sum of Hk) get the sizes; CS_ERR_CAPACITY if the block count
+ * exceeds cap_blocks. */
+cs_status cs_block_features(cs_handle* h, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
+                            float* d_out, int64_t cap_blocks, int64_t* nblocks_out, int32_t* nfeat_out);
+
+/* The proposal network: din -> dh -> dh -> 1, ReLU, BF16 weights (bit
+ * patterns), FP32 biases; W[j][i] maps input i to unit j. */
+typedef struct cs_mlp {
+    int32_t din, dh;
+    const uint16_t* w1;   /* [dh][din] */
+    const float* b1;      /* [dh] */
+    const uint16_t* w2;   /* [dh][dh] */
+    const float* b2;      /* [dh] */
+    const uint16_t* w3;   /* [dh] */
+    const float* b3;      /* [1] */
+} cs_mlp;
+
+/* FP32 gradients of every parameter of a cs_mlp, same shapes. */
+typedef struct cs_mlp_grads {
+    float *w1, *b1, *w2, *b2, *w3, *b3;
+} cs_mlp_grads;
+
+/* One Adam-updated tensor: FP32 master, optional BF16 copy refreshed after the
+ * step, moments m and v, gradient. */
+typedef struct cs_adam_param {
+    float* master;
+    uint16_t* bf16;
+    float* m;
+    float* v;
+    const float* grad;
+    int64_t n;
+} cs_adam_param;
+
+/* Forward pass over n rows of d_x [n][din]: d_h1, d_h2 [n][dh] (post-ReLU) and
+ * the logits d_z [n]; FP32 accumulation. */
+cs_status cs_mlp_forward(const cs_mlp* net, const float* d_x, int64_t n, float* d_h1, float* d_h2, float* d_z,
+                         void* stream);
+
+/* Weighted binary cross-entropy with logits against labels d_y (0/1), mean
+ * over n, weight pos_weight on positives: the loss into *d_loss and the
+ * gradients of every parameter into grads (d_dz [n], d_dh1, d_dh2 [n][dh] are
+ * scratch). */
+cs_status cs_mlp_backward(const cs_mlp* net, const float* d_x, const float* d_h1, const float* d_h2,
+                          const float* d_z, const float* d_y, int64_t n, float pos_weight, float* d_dz, float* d_dh1,
+                          float* d_dh2, const cs_mlp_grads* grads, float* d_loss, void* stream);
+
+/* One Adam step (bias-corrected, step >= 1) on each listed tensor. */
+cs_status cs_adam_step(const cs_adam_param* params, int32_t nparams, float lr, float beta1, float beta2, float eps,
+                       int32_t step, void* stream);
+
+/* BF16 (round to nearest even) copies of FP32 weights. */
+cs_status cs_mlp_to_bf16(const float* d_src, uint16_t* d_dst, int64_t n, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Metric statistics and in-situ normalisation (the reference's --metricstats
  * and --normalize: MetricStats, BlockMetricStats, MetricHistogram, MetricNorm,

@@ -213,6 +213,89 @@ def run_dmsweep(args, rank, local_rank):
             "clocks": clk.summary(), "nfiles": len(files), "h2d": h2d, "d2h": d2h}
 
 
+def run_learned(args, local_rank):
+    """The learned block proposal.  Training: separately
+    seeded 2^24-sample spectra with 200 injections each (f 0.1-750 Hz, duty
+    1-20 %, S/N 6-20, frequency-domain synthesis), every block of the survey
+    band labelled by the coherent search's own candidates (S/N > 8; the mixed
+    FP16 search reports exactly the plain candidates), until --train-blocks.
+    The score cut keeps 99.5 % of the positive blocks of 4 validation spectra.
+    Evaluation spectrum: another such spectrum.  Timed (wall clock, each stage
+    ending in a device sync, every arm alike): the plain FP32 full search, the
+    mixed FP16 full search, and the learned path -- features, scores, plain
+    FP32 re-search of the blocks at or above the cut (and its mixed variant)."""
+    import torch
+    from cohsearch import Engine, FFTFile, SearchParams, decimation_set, learned, synth
+    torch.cuda.set_device(local_rank)
+    nsamp, dt = 1 << 24, 64e-6
+    dec = decimation_set(NHARMS, MAXDECIM)
+    plain = Engine(SearchParams(nharms=NHARMS, m=16, decimations=dec, threshold=THR, synth="fp32"), device=local_rank)
+    mixed = Engine(SearchParams(nharms=NHARMS, m=16, decimations=dec, threshold=THR, synth="fp16"), device=local_rank)
+
+    def spectrum(seed):
+        rng = np.random.default_rng(seed)
+        ps = synth.random_pulsars(rng, 200, 0.1, 750.0, 0.01, 0.20, 6.0, 20.0)
+        return synth.make_spectrum_fd(nsamp, dt, ps, seed)
+
+    def labelled(seed):
+        mixed.set_spectrum(FFTFile.from_array(spectrum(seed), nsamp, dt))
+        X = mixed.block_features(LOF, HIF, 100, BLOCK)
+        raw = mixed.search_raw(LOF, HIF, 100, BLOCK, THR)
+        return X, torch.from_numpy(learned.block_labels(raw, X.shape[0], BLOCK, THR))
+
+    t0 = time.perf_counter()
+    xs, ys, seed, nb = [], [], 10_000, 0
+    while nb < args.train_blocks:
+        X, Y = labelled(seed)
+        xs.append(X)
+        ys.append(Y)
+        nb += X.shape[0]
+        seed += 1
+    Xt, Yt = torch.cat(xs), torch.cat(ys)
+    del xs, ys
+    t_data = time.perf_counter() - t0
+    mlp = learned.ProposalMLP(Xt.shape[1], 256, seed=0, device=local_rank)
+    t0 = time.perf_counter()
+    hist = mlp.fit(Xt, Yt, epochs=10, batch=4096, lr=1e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    val = [labelled(s) for s in (20_000, 20_001, 20_002, 20_003)]
+    sv = np.concatenate([mlp.scores(X) for X, _ in val])
+    tau = learned.choose_threshold(sv, np.concatenate([Y.numpy() for _, Y in val]), 0.995)
+
+    ev = spectrum(30_000)
+    for e in (plain, mixed):
+        e.set_spectrum(FFTFile.from_array(ev, nsamp, dt))
+
+    def wall(fn, k):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(k):
+            out = fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t) * 1e3 / k, out
+
+    gc.disable()
+    ms_plain, full = wall(lambda: plain.search_raw(LOF, HIF, 100, BLOCK, THR), args.steps)
+    ms_mixed, _ = wall(lambda: mixed.search_raw(LOF, HIF, 100, BLOCK, THR), args.steps)
+    ms_learn, res = wall(lambda: learned.learned_search(plain, mlp, tau, LOF, HIF, 100, BLOCK, THR), args.steps)
+    ms_learn_mixed, res_m = wall(lambda: learned.learned_search(mixed, mlp, tau, LOF, HIF, 100, BLOCK, THR),
+                                 args.steps)
+    gc.enable()
+    T = nsamp * dt
+    lodr = 0.5 / NHARMS
+    total = int(np.floor((HIF * T - LOF * T) / lodr)) + 1
+    return {"ms_plain": ms_plain, "ms_mixed": ms_mixed, "ms_learned": ms_learn, "ms_learned_mixed": ms_learn_mixed,
+            "recall": learned.recall_of(res.cands, full, THR), "recall_mixed": learned.recall_of(res_m.cands, full, THR),
+            "frac_blocks": len(res.blocks) / res.nblocks, "nblocks": res.nblocks, "trials": total,
+            "stage_ms": {"features": res.ms_features, "scores": res.ms_scores, "research": res.ms_search},
+            "train_blocks": int(Xt.shape[0]), "train_pos": int(Yt.sum().item()), "nfeat": int(Xt.shape[1]),
+            "loss": [round(h, 4) for h in hist], "tau": tau, "t_data_s": t_data, "t_train_s": t_train,
+            "ncand_full": int(np.sum(full["metric"] > THR))}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from cohsearch import Engine, SearchParams, decimation_set, synth
@@ -335,9 +418,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--synth", default="fp16", choices=["fp32", "bf16", "fp16", "bf16_split", "fp16_split"])
     ap.add_argument("--cpu-blocks", type=int, default=None)
-    ap.add_argument("--workload", choices=["survey", "dmsweep"], default="survey",
+    ap.add_argument("--workload", choices=["survey", "dmsweep", "learned"], default="survey",
                     help="survey: one 2^23-sample spectrum (the headline); dmsweep: 64 spectra of "
-                         "2^21..2^24 samples through the batch entry point")
+                         "2^21..2^24 samples through the batch entry point; learned: the learned block "
+                         "proposal on a 2^24-sample spectrum with 200 injections")
+    ap.add_argument("--train-blocks", type=int, default=1_000_000,
+                    help="learned workload: labelled training blocks (separately seeded spectra)")
     ap.add_argument("--band", type=float, nargs=2, default=None,
                     help="search only [LO, HI] Hz (a smaller case of the same kernels, for profiling)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
@@ -380,6 +466,27 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
+    if args.workload == "learned":
+        if world > 1 or rank != 0:
+            return 0
+        r = run_learned(args, local_rank)
+        cfg = {"workload": "learned proposal: 2^24 samples @64us, 200 injections (f 0.1-750 Hz, duty 1-20%, S/N "
+                           "6-20), nharms=60, decimation_set(60,6), 0.1-125 Hz, threshold 8; network "
+                           f"{r['nfeat']}-256-256-1 BF16 weights, trained on {r['train_blocks']} labelled blocks",
+               "trials_per_step": r["trials"], "blocks": r["nblocks"], "blocks_researched": r["frac_blocks"],
+               "recall_vs_plain": r["recall"], "recall_mixed_research": r["recall_mixed"],
+               "plain_fp32_ms": r["ms_plain"], "mixed_fp16_ms": r["ms_mixed"],
+               "learned_plain_research_ms": r["ms_learned"], "learned_mixed_research_ms": r["ms_learned_mixed"],
+               "speedup_vs_plain": r["ms_plain"] / r["ms_learned"],
+               "speedup_mixed_research_vs_plain": r["ms_plain"] / r["ms_learned_mixed"],
+               "learned_stage_ms": r["stage_ms"], "train_positive_blocks": r["train_pos"],
+               "train_loss_per_epoch": r["loss"], "score_cut": r["tau"], "candidates_full": r["ncand_full"],
+               "data_s": r["t_data_s"], "train_s": r["t_train_s"], "timing": "wall clock, device-synced, all arms"}
+        print(json.dumps({
+            "metric": METRIC, "value": r["trials"] / (r["ms_learned"] / 1000.0), "unit": "trials/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_learned"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16", "data": "synthetic", "config": cfg}))
+        return 0
     if args.workload == "dmsweep":
         r = run_dmsweep(args, rank, local_rank)
         if world > 1:

@@ -172,8 +172,11 @@ def run_dmsweep(args, rank, local_rank):
     params = SearchParams(nharms=NHARMS, m=16, decimations=decimation_set(NHARMS, MAXDECIM), threshold=THR,
                           synth=args.synth)
     eng = Engine(params, device=local_rank)
-    stream = torch.cuda.current_stream()
+    # a stream of its own (the legacy default stream cannot be captured):
+    # device-resident batches replay one captured graph (cs_set_batch_graph)
+    stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
+    eng.set_batch_graph(not args.no_graph)
     dev = [torch.from_numpy(a.view(np.float32).copy()).cuda() for a, _, _ in files]
     pin = [torch.from_numpy(a.view(np.float32).copy()).pin_memory() for a, _, _ in files]
     on_dev = [((d.data_ptr(), len(a)), N, dt) for d, (a, N, dt) in zip(dev, files)]
@@ -184,7 +187,8 @@ def run_dmsweep(args, rank, local_rank):
     def timed(spectra, on_device, k):
         tot, launches, trials, ncand, d2h = 0.0, 0, 0, 0, 0
         for _ in range(k):
-            flush.zero_()
+            with torch.cuda.stream(stream):
+                flush.zero_()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -422,6 +426,8 @@ def main():
                     help="survey: one 2^23-sample spectrum (the headline); dmsweep: 64 spectra of "
                          "2^21..2^24 samples through the batch entry point; learned: the learned block "
                          "proposal on a 2^24-sample spectrum with 200 injections")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="dmsweep: search device-resident batches the ordinary way, not by a replayed graph")
     ap.add_argument("--train-blocks", type=int, default=1_000_000,
                     help="learned workload: labelled training blocks (separately seeded spectra)")
     ap.add_argument("--band", type=float, nargs=2, default=None,
@@ -504,6 +510,7 @@ def main():
                            "0-3 injected pulsars each, nharms=60, decimation_set(60,6), 0.1-125 Hz, threshold 8",
                "trials_per_step": r["trials"], "files": r["nfiles"], "synth": args.synth,
                "l2": "flushed (256 MiB write) before each step", "parallelism": "one sweep per GPU (weak)",
+               "batch_graph": not args.no_graph,
                "candidates_per_step": r["ncand"]}
         print(json.dumps({
             "metric": METRIC, "value": world * r["trials"] * K / (r["ms"] / 1000.0), "unit": "trials/s",

@@ -134,6 +134,7 @@ PROTOTYPES = {
     "cs_get_metric_hists": (_i32, [_P, ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(_i32), _P, _P,
                                    _P, _P]),
     "cs_set_metricnorm": (_i32, [_P, _i32, _i32, _P, _P, _P, _P]),
+    "cs_set_batch_graph": (_i32, [_P, _i32]),
     "cs_search_blocks": (_i32, [_P, _f64, _f64, _i64, _i64, _f64, _P, _i64, _P, _i64, ctypes.POINTER(_i64)]),
     "cs_block_features": (_i32, [_P, _f64, _f64, _i64, _i64, _P, _i64, ctypes.POINTER(_i64), ctypes.POINTER(_i32)]),
     "cs_mlp_forward": (_i32, [ctypes.POINTER(cs_mlp), _P, _i64, _P, _P, _P, _P]),

@@ -270,6 +270,12 @@ class Engine:
             _lib.check(st, self._h, "cs_search")
             return out[:n.value].copy()
 
+    def set_batch_graph(self, enable: bool = True):
+        """Replay a captured CUDA graph for repeated batches of device spectra
+        (cs_set_batch_graph); the engine's stream must not be the legacy
+        default stream."""
+        _lib.check(self.lib.cs_set_batch_graph(self._h, int(bool(enable))), self._h, "cs_set_batch_graph")
+
     def search_blocks_raw(self, block_list, lofreq=0.1, hifreq=100.0, lobin=100, blocksize=2048, threshold=None,
                           cap=1 << 16) -> np.ndarray:
         """Raw detections of the listed blocks of the band's grid only

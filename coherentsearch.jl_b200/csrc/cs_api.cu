@@ -14,6 +14,7 @@
 #include <cstdarg>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -250,13 +251,40 @@ struct cs_handle {
     DBuf d_A, d_samp;
     HBuf h_nvalid, h_io;                // pinned: valid counts up; counters + candidate prefix down
     HBuf h_bmap;                        // pinned: a wave's block map (block-list search)
-    DBuf d_levels, d_tw, d_harms, d_wtab, d_atab, d_ctab, d_nvalid, d_X, d_Q0, d_sigma,
+    DBuf d_levels, d_tw, d_nvalid, d_X, d_Q0, d_sigma,
         d_tmetric, d_items, d_counts, d_cands, d_amax, d_bmap;
     // FP64 plan tables of the last anchor r_lo, already on the device
-    bool plan_valid = false;
-    double plan_rlo = 0.0;
-    HostPlans plans;
-    std::vector<std::pair<double, HostPlans>> plan_cache;   // host tables of recent anchors
+    // FP64 plan tables of recent anchors r_lo, each kept on the device too: a
+    // batch of spectra of several lengths alternates between them without
+    // re-uploading, and a captured batch graph reads them in place
+    struct PlanSet {
+        double rlo = 0.0;
+        HostPlans host;
+        DBuf harms, wtab, atab, ctab;
+        void release() {
+            harms.release();
+            wtab.release();
+            atab.release();
+            ctab.release();
+        }
+    };
+    std::vector<std::unique_ptr<PlanSet>> plan_sets;
+    // batch graph (cs_set_batch_graph): one captured graph of a whole batch of
+    // device spectra, replayed while the batch's signature stays the same;
+    // any other search drops it (its buffers and plan tables may move)
+    bool batch_graph = false;
+    bool graph_valid = false;
+    bool graph_failed = false;          // the batch of gkey could not be captured: do not retry
+    cudaGraphExec_t gexec = nullptr;
+    struct GraphSlot {
+        HBuf io;           // counters, then the candidate prefix
+        HBuf nvalid;       // valid counts the graph uploads
+        int64_t launches = 0;
+    };
+    std::vector<GraphSlot> gslots;
+    std::vector<cs_spectrum> gkey;
+    double gkey_d[3] = {0, 0, 0};
+    int64_t gkey_i[2] = {0, 0};
     int64_t plan_bytes = 0;
     // metric statistics (MetricStats) and normalisation (MetricNorm)
     bool ms_on = false;
@@ -426,6 +454,11 @@ struct RunSpec {
     double T = 0.0;       // frequency windows
     double threshold_d = 0.0;
     const int64_t* blist = nullptr;   // search of a block list: band block indices (ascending), nblocks of them
+    // capture into a batch graph: no host syncs; counters and the candidate
+    // prefix go to these pinned slots, valid counts come from h_nvalid
+    bool capture = false;
+    int32_t* cap_io = nullptr;          // 64 bytes of counters, then kCandPrefix DevCands
+    int32_t* cap_nvalid = nullptr;      // pinned [nblocks][nlev], filled here
 };
 
 // _logedges (src/search.jl:1406-1411): nwin+1 log-spaced edges over [a, b].
@@ -445,34 +478,33 @@ int window_index(const double* e, int nwin, double f) {
 
 cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands, float2* x_out) {
     const cs_params& p = H->p;
+    if (!R.capture) H->graph_valid = false;   // buffers and plan tables may move
     // The tables depend on r_lo only (params are fixed per handle): a search
     // repeated on the same band, the common case of a pipeline over many
     // spectra, reuses the device copies.
     int64_t plan_bytes = 0;
-    if (!H->plan_valid || H->plan_rlo != R.r_lo) {
-        H->plan_valid = false;
-        // a few recent anchors stay cached on the host: a batch of spectra of
-        // several lengths alternates between them
-        auto hit = std::find_if(H->plan_cache.begin(), H->plan_cache.end(),
-                                [&](const std::pair<double, HostPlans>& e) { return e.first == R.r_lo; });
-        if (hit != H->plan_cache.end()) {
-            H->plans = hit->second;
-        } else {
-            build_plans(p, R.r_lo, H->plans);
-            if (H->plan_cache.size() >= 8) H->plan_cache.erase(H->plan_cache.begin());
-            H->plan_cache.emplace_back(R.r_lo, H->plans);
+    cs_handle::PlanSet* ps = nullptr;
+    for (auto& e : H->plan_sets)
+        if (e->rlo == R.r_lo) ps = e.get();
+    if (!ps) {
+        if (R.capture) return fail(H, CS_ERR_UNSUPPORTED, "a captured search needs its plan tables on the device");
+        if (H->plan_sets.size() >= 8) {
+            H->plan_sets.front()->release();
+            H->plan_sets.erase(H->plan_sets.begin());
         }
-        const HostPlans& plans = H->plans;
-        CS_CUDA(upload(H->d_harms, plans.harms, H->stream), "upload plans");
-        CS_CUDA(upload(H->d_wtab, plans.w, H->stream), "upload weights");
-        CS_CUDA(upload(H->d_atab, plans.a, H->stream), "upload phases");
-        CS_CUDA(upload(H->d_ctab, plans.c, H->stream), "upload carries");
+        H->plan_sets.push_back(std::make_unique<cs_handle::PlanSet>());
+        ps = H->plan_sets.back().get();
+        ps->rlo = R.r_lo;
+        build_plans(p, R.r_lo, ps->host);
+        const HostPlans& plans = ps->host;
+        CS_CUDA(upload(ps->harms, plans.harms, H->stream), "upload plans");
+        CS_CUDA(upload(ps->wtab, plans.w, H->stream), "upload weights");
+        CS_CUDA(upload(ps->atab, plans.a, H->stream), "upload phases");
+        CS_CUDA(upload(ps->ctab, plans.c, H->stream), "upload carries");
         plan_bytes = (int64_t)(plans.harms.size() * sizeof(DevHarm) + plans.w.size() * sizeof(float) +
                                plans.a.size() * sizeof(float2) + plans.c.size());
-        H->plan_valid = true;
-        H->plan_rlo = R.r_lo;
     }
-    for (const DevHarm& d : H->plans.harms) {
+    for (const DevHarm& d : ps->host.harms) {
         const double lim = 4.6e18;
         if ((double)R.t_end * (double)d.h * (double)d.pnum > lim)
             return fail(H, CS_ERR_UNSUPPORTED, "trial index times harmonic overflows 64-bit phase state");
@@ -506,9 +538,10 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
                            (size_t)nlev * kSampStride * sizeof(float2) +
                            (size_t)nlev * Nprof * sizeof(float) * (R.exact_all ? 2 : 1) +
                            (size_t)nlev * Nprof * (sizeof(DevItem) + sizeof(DevCand)) + 64;
-    // Working set of one wave: up to 8 GiB, and at most half of the free
-    // device memory (a full survey band is one wave on a 180 GB part).
-    size_t budget = (size_t)8 << 30;
+    // Working set of one wave: up to 16 GiB, and at most half of the free
+    // device memory (a full survey band of a 2^24-sample spectrum, ~9 GB, is
+    // one wave on a 180 GB part).
+    size_t budget = (size_t)16 << 30;
     {
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
@@ -519,6 +552,22 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         }
     }
     const int64_t WB = std::max<int64_t>(1, std::min<int64_t>(R.nblocks, (int64_t)(budget / per_blk)));
+    if (R.capture) {
+        // a captured search runs as one wave on buffers an earlier run sized,
+        // without statistics, diagnostics or host round trips
+        if (WB < R.nblocks) return fail(H, CS_ERR_UNSUPPORTED, "a captured search must fit one wave");
+        if (R.stats || R.norm || R.keep_diag || R.interp_only || R.blist || R.exact_all)
+            return fail(H, CS_ERR_UNSUPPORTED, "a captured search carries no statistics, diagnostics or block list");
+        auto small = [](const DBuf& d, size_t n) { return d.bytes < n; };
+        if ((want_x && small(H->d_X, (size_t)WB * p.nharms * Nprof * sizeof(float2))) ||
+            (tensor && small(H->d_A, (size_t)WB * tiles_per_blk * kATileBytes * synth_split(p.synth))) ||
+            small(H->d_samp, (size_t)WB * nlev * kSampStride * sizeof(float2)) ||
+            small(H->d_sigma, (size_t)WB * nlev * sizeof(float)) || small(H->d_nvalid, (size_t)WB * nlev * sizeof(int32_t)) ||
+            small(H->d_items, (size_t)WB * nlev * Nprof * sizeof(DevItem)) ||
+            small(H->d_cands, (size_t)WB * nlev * Nprof * sizeof(DevCand)) || small(H->d_counts, 4 * sizeof(int32_t)) ||
+            (tensor && synth_fp16(p.synth) && small(H->d_amax, 16)))
+            return fail(H, CS_ERR_UNSUPPORTED, "a captured search needs buffers sized by an earlier run");
+    }
 
     if (want_x) CS_CUDA(H->d_X.ensure((size_t)WB * p.nharms * Nprof * sizeof(float2)), "alloc X");
     if (tensor && !R.interp_only) {
@@ -600,14 +649,14 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
     const double nyq = (double)H->N / 2.0;
     // counters, then the first kCandPrefix candidates, come back in one pinned read
     constexpr int kCandPrefix = 4096;
-    CS_CUDA(H->h_io.ensure(64 + (size_t)kCandPrefix * sizeof(DevCand)), "pinned readback");
-    int32_t* counts = H->h_io.as<int32_t>();
-    DevCand* cand_pre = reinterpret_cast<DevCand*>(H->h_io.as<uint8_t>() + 64);
+    if (!R.capture) CS_CUDA(H->h_io.ensure(64 + (size_t)kCandPrefix * sizeof(DevCand)), "pinned readback");
+    int32_t* counts = R.capture ? R.cap_io : H->h_io.as<int32_t>();
+    DevCand* cand_pre = reinterpret_cast<DevCand*>(reinterpret_cast<uint8_t*>(counts) + 64);
 
     // FP16 A tiles: the spectrum's largest component, for their range scale
     const bool fp16_scale = tensor && !R.interp_only && synth_fp16(p.synth);
     if (fp16_scale) {
-        CS_CUDA(H->d_amax.ensure(16), "alloc spectrum maximum");
+        if (!R.capture) CS_CUDA(H->d_amax.ensure(16), "alloc spectrum maximum");
         CS_CUDA(cudaMemsetAsync(H->d_amax.p, 0, sizeof(uint32_t), H->stream), "reset spectrum maximum");
         CS_CUDA(launch_amax(H->amps, H->namps, H->d_amax.as<uint32_t>(), H->stream, H->num_sms), "maximum launch");
         S.launches += 1;
@@ -627,10 +676,10 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         a.total = R.t_end;
         a.nblk = nb;
         a.blk_base = (int32_t)c0;
-        a.harms = H->d_harms.as<DevHarm>();
-        a.wtab = H->d_wtab.as<float>();
-        a.atab = H->d_atab.as<float2>();
-        a.ctab = H->d_ctab.as<uint8_t>();
+        a.harms = ps->harms.as<DevHarm>();
+        a.wtab = ps->wtab.as<float>();
+        a.atab = ps->atab.as<float2>();
+        a.ctab = ps->ctab.as<uint8_t>();
         a.levels = H->d_levels.as<DevLevel>();
         a.tw = H->d_tw.as<float>();
         a.nvalid = H->d_nvalid.as<int32_t>();
@@ -692,8 +741,8 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         }
         int* d_err = H->d_counts.as<int32_t>() + 2;
 
-        CS_CUDA(H->h_nvalid.ensure((size_t)nb * nlev * sizeof(int32_t)), "pinned valid counts");
-        int32_t* nvalid = H->h_nvalid.as<int32_t>();
+        if (!R.capture) CS_CUDA(H->h_nvalid.ensure((size_t)nb * nlev * sizeof(int32_t)), "pinned valid counts");
+        int32_t* nvalid = R.capture ? R.cap_nvalid : H->h_nvalid.as<int32_t>();
         for (int b = 0; b < nb; ++b) {
             const int64_t c = c0 + b;
             // global trial of the block's first trial
@@ -735,16 +784,16 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             S.h2d_bytes += (int64_t)nb * nlev * (int64_t)sizeof(int32_t);
             a.nvalid = H->d_nvalid.as<int32_t>();
         }
-        CS_CUDA(cudaEventRecord(H->ev[0], H->stream), "event");
+        if (!R.capture) CS_CUDA(cudaEventRecord(H->ev[0], H->stream), "event");
         CS_CUDA(launch_interp(a, H->stream, win_max, d_err), "interp launch");
-        CS_CUDA(cudaEventRecord(H->ev[1], H->stream), "event");
+        if (!R.capture) CS_CUDA(cudaEventRecord(H->ev[1], H->stream), "event");
         S.launches += 1;
         if (!R.interp_only) {
             // sigma needs only the samples, so it runs first and the synthesis
             // epilogue applies the medcut test itself (no gate pass over HBM);
             // exact_all scores every trial exactly and needs no gate at all
             CS_CUDA(launch_sigma(a, H->stream, max_hk, max_np, d_err), "sigma launch");
-            CS_CUDA(cudaEventRecord(H->ev[2], H->stream), "event");
+            if (!R.capture) CS_CUDA(cudaEventRecord(H->ev[2], H->stream), "event");
             S.launches += 1;
             if (!R.exact_all) {
                 if (tensor)
@@ -753,7 +802,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
                     CS_CUDA(launch_synth_fp32(a, H->stream, (int)smem_synth), "synth launch");
                 S.launches += 1;
             }
-            CS_CUDA(cudaEventRecord(H->ev[3], H->stream), "event");
+            if (!R.capture) CS_CUDA(cudaEventRecord(H->ev[3], H->stream), "event");
             CS_CUDA(launch_rescue(a, H->stream, H->num_sms), "rescue launch");
             S.launches += 1;
             if (R.stats) {
@@ -763,7 +812,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
                                         cudaMemcpyDeviceToHost, H->stream),
                         "read block stats");
             }
-            CS_CUDA(cudaEventRecord(H->ev[4], H->stream), "event");
+            if (!R.capture) CS_CUDA(cudaEventRecord(H->ev[4], H->stream), "event");
         }
         CS_CUDA(cudaMemcpyAsync(counts, H->d_counts.p, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost,
                                 H->stream),
@@ -773,6 +822,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             CS_CUDA(cudaMemcpyAsync(cand_pre, H->d_cands.p, (size_t)n_pre * sizeof(DevCand),
                                     cudaMemcpyDeviceToHost, H->stream),
                     "read candidates");
+        if (R.capture) return CS_OK;   // one wave: the caller's graph holds the rest
         CS_CUDA(cudaStreamSynchronize(H->stream), "wave");
         S.d2h_bytes += 4 * sizeof(int32_t);
         if (counts[2] == 1) return fail(H, CS_ERR_CUDA, "interpolation window exceeded its bound");
@@ -915,6 +965,13 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
 
 extern "C" {
 
+cs_status cs_set_batch_graph(cs_handle* H, int32_t enable) {
+    if (!H) return CS_ERR_INVALID_ARGUMENT;
+    H->batch_graph = enable != 0;
+    if (!H->batch_graph) H->graph_valid = false;
+    return CS_OK;
+}
+
 const char* cs_version(void) { return CS_VERSION_STRING; }
 
 const char* cs_last_error(const cs_handle* h) { return h ? h->err.c_str() : "null handle"; }
@@ -962,8 +1019,16 @@ cs_status cs_destroy(cs_handle* H) {
     cudaSetDevice(H->device);
     if (H->stream) cudaStreamSynchronize(H->stream);
     if (H->own_stream) cudaStreamSynchronize(H->own_stream);
-    DBuf* bufs[] = {&H->d_A, &H->d_samp, &H->d_tcB, &H->amps_owned, &H->d_levels, &H->d_tw, &H->d_harms, &H->d_wtab, &H->d_atab, &H->d_amax, &H->d_bmap,
-                    &H->d_ctab, &H->d_nvalid, &H->d_X, &H->d_Q0, &H->d_sigma,
+    for (auto& e : H->plan_sets) e->release();
+    H->plan_sets.clear();
+    if (H->gexec) cudaGraphExecDestroy(H->gexec);
+    H->gexec = nullptr;
+    for (auto& g : H->gslots) {
+        g.io.release();
+        g.nvalid.release();
+    }
+    DBuf* bufs[] = {&H->d_A, &H->d_samp, &H->d_tcB, &H->amps_owned, &H->d_levels, &H->d_tw, &H->d_amax, &H->d_bmap,
+                    &H->d_nvalid, &H->d_X, &H->d_Q0, &H->d_sigma,
                     &H->d_tmetric, &H->d_items, &H->d_counts, &H->d_cands};
     for (DBuf* b : bufs) b->release();
     H->h_nvalid.release();
@@ -1030,13 +1095,15 @@ namespace {
 
 // The search of one spectrum over blocks [block_begin, block_end) of the band's
 // grid; candidates appended to `outv` in the reference's order.
-cs_status search_core(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
-                      double threshold, int32_t exact_all, int64_t block_begin, int64_t block_end,
-                      std::vector<cs_candidate>* outv, const int64_t* blist = nullptr, int64_t nlist = 0) {
+// The band bookkeeping of `search` (src/search.jl:2016-2027) into a RunSpec;
+// *empty when there is nothing to search.
+cs_status setup_run(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize, double threshold,
+                    int32_t exact_all, int64_t block_begin, int64_t block_end, const int64_t* blist, int64_t nlist,
+                    RunSpec& R, bool* empty) {
+    *empty = true;
     if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");
     CS_CUDA(cudaSetDevice(H->device), "set device");
     const cs_params& p = H->p;
-    // Band bookkeeping of `search` (src/search.jl:2016-2027).
     const double T = (double)H->N * H->dt;
     const double lodr = p.hidr / (double)p.nharms;
     double r_lo = lofreq * T;
@@ -1066,7 +1133,7 @@ cs_status search_core(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
     } else if (block_begin >= b1) {
         return CS_OK;
     }
-    RunSpec R{};
+    R = RunSpec{};
     R.r_lo = r_lo;
     R.lodr = lodr;
     R.Nprof = Nprof;
@@ -1085,32 +1152,37 @@ cs_status search_core(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
     R.keep_diag = H->diag >= 1;
     R.r_hi = r_hi;
     R.T = T;
-    std::vector<DevCand> raw;
-    cs_status st = run_blocks(H, R, &raw, nullptr);
-    if (st != CS_OK) return st;
-    // Reference order with one task: by block, base fold then each decimation
-    // level in params order, ascending trial (src/search.jl:1809-1859).
+    *empty = false;
+    return CS_OK;
+}
+
+// Device records to candidates: the reference order with one task (by block,
+// base fold then each decimation level in params order, ascending trial:
+// src/search.jl:1809-1859) and its FP64 frequency expressions.
+void emit_candidates(cs_handle* H, const RunSpec& R, std::vector<DevCand>& raw, std::vector<cs_candidate>* outv) {
+    const cs_params& p = H->p;
     std::sort(raw.begin(), raw.end(), [](const DevCand& x, const DevCand& y) {
         if (x.blk != y.blk) return x.blk < y.blk;
         if (x.lev != y.lev) return x.lev < y.lev;
         return x.j < y.j;
     });
+    const int64_t block_begin = R.blist ? 0 : R.t_base / R.Nprof;
     const int64_t n = (int64_t)raw.size();
     outv->reserve(outv->size() + (size_t)n);
     for (int64_t i = 0; i < n; ++i) {
         const DevCand& c = raw[i];
         const LevelHost& L = H->levels[c.lev];
-        const int64_t i0 = (block_begin + (int64_t)c.blk) * Nprof;
-        const double rstart = r_lo + (double)i0 * lodr;
+        const int64_t i0 = (block_begin + (int64_t)c.blk) * R.Nprof;
+        const double rstart = R.r_lo + (double)i0 * R.lodr;
         cs_candidate o{};
         if (L.k == 1) {
-            o.r = rstart + (double)c.j * lodr;           // rf, src/search.jl:1833
+            o.r = rstart + (double)c.j * R.lodr;           // rf, src/search.jl:1833
             o.nharm = p.nharms;
         } else {
-            o.r = (double)L.k * (rstart + (double)c.j * lodr);  // r_dec, src/search.jl:1696
+            o.r = (double)L.k * (rstart + (double)c.j * R.lodr);  // r_dec, src/search.jl:1696
             o.nharm = L.Hk;
         }
-        o.freq = o.r / T;
+        o.freq = o.r / R.T;
         o.metric = (double)c.metric;
         if (R.norm) {
             // z of the normalised test, with the device's FP64 expressions
@@ -1122,8 +1194,97 @@ cs_status search_core(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
         o.trial = i0 + c.j;
         outv->push_back(o);
     }
+}
+
+cs_status search_core(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize,
+                      double threshold, int32_t exact_all, int64_t block_begin, int64_t block_end,
+                      std::vector<cs_candidate>* outv, const int64_t* blist = nullptr, int64_t nlist = 0) {
+    RunSpec R{};
+    bool empty = true;
+    cs_status st = setup_run(H, lofreq, hifreq, lobin, blocksize, threshold, exact_all, block_begin, block_end, blist,
+                             nlist, R, &empty);
+    if (st != CS_OK || empty) return st;
+    std::vector<DevCand> raw;
+    st = run_blocks(H, R, &raw, nullptr);
+    if (st != CS_OK) return st;
+    emit_candidates(H, R, raw, outv);
     return CS_OK;
 }
+
+constexpr int kGraphPrefix = 4096;   // candidates a captured search reads back per spectrum
+
+// Capture one graph of the whole batch (device spectra, after an ordinary run
+// of it sized every buffer): per spectrum the valid-count upload from its
+// own pinned slot, the search's launches and the readback of its counters
+// and candidate prefix into that slot.  Not an error when a spectrum cannot
+// be captured (more than one wave): the batch then stays ordinary.
+void capture_batch(cs_handle* H, const cs_spectrum* files, int nfiles, double lofreq, double hifreq, int64_t lobin,
+                   int64_t blocksize, double threshold) {
+    if (H->gexec) cudaGraphExecDestroy(H->gexec);
+    H->gexec = nullptr;
+    H->graph_valid = false;
+    H->graph_failed = true;   // until the capture below succeeds
+    H->gkey.assign(files, files + nfiles);
+    H->gkey_d[0] = lofreq;
+    H->gkey_d[1] = hifreq;
+    H->gkey_d[2] = threshold;
+    H->gkey_i[0] = lobin;
+    H->gkey_i[1] = blocksize;
+    const cs_stats keep = H->stats;   // the batch's own statistics survive the capture
+    struct Restore {
+        cs_handle* H;
+        cs_stats s;
+        ~Restore() { H->stats = s; }
+    } restore{H, keep};
+    if ((int)H->gslots.size() < nfiles) H->gslots.resize(nfiles);
+    const int nlev = (int)H->levels.size();
+    // slots and run specs first: no allocation while capturing
+    std::vector<RunSpec> specs(nfiles);
+    std::vector<char> empty(nfiles, 1);
+    for (int i = 0; i < nfiles; ++i) {
+        H->amps = reinterpret_cast<const float2*>(files[i].amps);
+        H->namps = files[i].namps;
+        H->N = files[i].N;
+        H->dt = files[i].dt;
+        H->has_spec = true;
+        bool e = true;
+        if (setup_run(H, lofreq, hifreq, lobin, blocksize, threshold, 0, 0, -1, nullptr, 0, specs[i], &e) != CS_OK) return;
+        empty[i] = e ? 1 : 0;
+        if (e) continue;
+        if (H->gslots[i].io.ensure(64 + (size_t)kGraphPrefix * sizeof(DevCand)) != cudaSuccess ||
+            H->gslots[i].nvalid.ensure((size_t)specs[i].nblocks * nlev * sizeof(int32_t)) != cudaSuccess)
+            return;
+    }
+    if (cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) return;
+    bool ok = true;
+    for (int i = 0; i < nfiles && ok; ++i) {
+        if (empty[i]) continue;
+        H->amps = reinterpret_cast<const float2*>(files[i].amps);
+        H->namps = files[i].namps;
+        H->N = files[i].N;
+        H->dt = files[i].dt;
+        RunSpec R = specs[i];
+        R.capture = true;
+        R.keep_diag = false;
+        R.cap_io = H->gslots[i].io.as<int32_t>();
+        R.cap_nvalid = H->gslots[i].nvalid.as<int32_t>();
+        std::vector<DevCand> unused;   // (the candidates come back through the slot)
+        ok = run_blocks(H, R, &unused, nullptr) == CS_OK;
+        H->gslots[i].launches = H->stats.launches;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(H->stream, &g);
+    if (ok && ec == cudaSuccess && g && cudaGraphInstantiate(&H->gexec, g, 0) == cudaSuccess) {
+        H->graph_valid = true;
+        H->graph_failed = false;
+    } else {
+        H->gexec = nullptr;
+    }
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();   // a failed capture leaves no sticky state to report
+    H->err.clear();
+}
+
 
 }  // namespace
 
@@ -1230,6 +1391,68 @@ cs_status cs_search_batch(cs_handle* H, const cs_spectrum* files, int32_t nfiles
     std::vector<cs_candidate> all;
     std::vector<int32_t> owner;
     cs_stats tot{};
+    const bool want_graph = on_device && H->batch_graph && nfiles > 0;
+    auto same_key = [&]() {
+        if ((int)H->gkey.size() != nfiles) return false;
+        if (H->gkey_d[0] != lofreq || H->gkey_d[1] != hifreq || H->gkey_d[2] != threshold ||
+            H->gkey_i[0] != lobin || H->gkey_i[1] != blocksize)
+            return false;
+        for (int i = 0; i < nfiles; ++i)
+            if (H->gkey[i].amps != files[i].amps || H->gkey[i].namps != files[i].namps || H->gkey[i].N != files[i].N ||
+                H->gkey[i].dt != files[i].dt)
+                return false;
+        return true;
+    };
+    const bool key_match = want_graph && same_key();
+    if (key_match && H->graph_valid) {
+        // replay: one launch for the whole batch, one synchronisation
+        CS_CUDA(cudaGraphLaunch(H->gexec, H->stream), "batch graph launch");
+        CS_CUDA(cudaStreamSynchronize(H->stream), "batch graph");
+        for (int i = 0; i < nfiles; ++i) {
+            const cs_spectrum& f = files[i];
+            H->amps = reinterpret_cast<const float2*>(f.amps);
+            H->namps = f.namps;
+            H->N = f.N;
+            H->dt = f.dt;
+            H->has_spec = true;
+            RunSpec R{};
+            bool empty = true;
+            cs_status st = setup_run(H, lofreq, hifreq, lobin, blocksize, threshold, 0, 0, -1, nullptr, 0, R, &empty);
+            if (st != CS_OK) return st;
+            const size_t before = all.size();
+            if (!empty) {
+                const int32_t* counts = H->gslots[i].io.as<int32_t>();
+                if (counts[2] != 0) return fail(H, CS_ERR_TIMEOUT, "a device wait ran out in the batch graph");
+                const int n_c = counts[1];
+                if (n_c > kGraphPrefix) {
+                    // more candidates than the captured prefix: search this one
+                    // again the ordinary way (the graph is dropped and rebuilt)
+                    st = search_core(H, lofreq, hifreq, lobin, blocksize, threshold, 0, 0, -1, &all);
+                    if (st != CS_OK) return st;
+                } else {
+                    const DevCand* pre = reinterpret_cast<const DevCand*>(H->gslots[i].io.as<uint8_t>() + 64);
+                    std::vector<DevCand> raw(pre, pre + n_c);
+                    emit_candidates(H, R, raw, &all);
+                }
+                tot.trials += R.t_end - R.t_base;
+                tot.blocks += R.nblocks;
+                tot.rescued += counts[0];
+                tot.candidates += n_c;
+                tot.waves += 1;
+                tot.launches += H->gslots[i].launches;
+                tot.d2h_bytes += 64 + (int64_t)std::min(n_c, kGraphPrefix) * (int64_t)sizeof(DevCand);
+            }
+            owner.insert(owner.end(), all.size() - before, i);
+        }
+        H->stats = tot;
+        H->has_spec = false;
+        const int64_t n = (int64_t)all.size();
+        std::copy_n(all.begin(), std::min(n, cap), out);
+        std::copy_n(owner.begin(), std::min(n, cap), file_of);
+        *n_out = n;
+        if (n > cap) return fail(H, CS_ERR_CAPACITY, "candidate array too small");
+        return CS_OK;
+    }
     for (int i = 0; i < nfiles; ++i) {
         if (!on_device) {
             if (i + 1 < nfiles) CS_CUDA(issue_copy(i + 1), "copy spectrum");
@@ -1264,6 +1487,8 @@ cs_status cs_search_batch(cs_handle* H, const cs_spectrum* files, int32_t nfiles
         tot.d2h_bytes += S.d2h_bytes;
     }
     H->stats = tot;
+    if (want_graph && !(key_match && H->graph_failed))
+        capture_batch(H, files, nfiles, lofreq, hifreq, lobin, blocksize, threshold);
     H->has_spec = false;   // the batch buffers are not a spectrum of the handle's
     const int64_t n = (int64_t)all.size();
     std::copy_n(all.begin(), std::min(n, cap), out);

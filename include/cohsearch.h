@@ -149,6 +149,18 @@ cs_status cs_search_range(cs_handle* h, double lofreq, double hifreq, int64_t lo
                           double threshold, int32_t exact_all, int64_t block_begin, int64_t block_end,
                           cs_candidate* out, int64_t cap, int64_t* n_out);
 
+/* enable != 0: cs_search_batch over device spectra (on_device = 1) runs the
+ * batch the ordinary way once, captures it into one CUDA graph -- per
+ * spectrum its uploads, launches and readback, no host round trip between
+ * spectra -- and replays that graph while later calls repeat the same batch
+ * (same spectrum addresses, lengths, band and threshold; refill the spectra
+ * in place between calls).  Any other search on the handle drops the graph.
+ * A spectrum needing more than one wave keeps the batch ordinary; one with
+ * more than 4096 candidates is searched again the ordinary way.  No
+ * counterpart in the reference (its batch is a loop over files,
+ * src/cli.jl:237-289). */
+cs_status cs_set_batch_graph(cs_handle* h, int32_t enable);
+
 /* cs_search restricted to the listed blocks of the band's grid (strictly
  * ascending indices): each block's sigma and candidates are exactly the whole
  * search's, as with cs_search_range.  The re-search of the blocks a learned

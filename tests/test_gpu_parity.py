@@ -319,3 +319,49 @@ def test_batch_equals_file_by_file_searches():
         want = single.search_raw(1.0, 60.0, 100, 2048, 7.0)
         assert np.array_equal(raw[owner == i], want)
     assert any(len(raw[owner == i]) > 0 for i in range(len(files)))
+
+
+def test_batch_graph_replays_the_ordinary_batch():
+    """cs_set_batch_graph: the batch of device spectra run once the ordinary
+    way, captured into one graph and replayed -- the same records as the
+    ordinary batch, also after the spectra are refilled in place, and again
+    after an unrelated search drops the graph."""
+    import torch
+    from cohsearch import synth
+    cs = _cs()
+    rng = np.random.default_rng(12)
+    lens = [1 << 20, 1 << 21, 1 << 20]
+    def spectra(seed):
+        out = []
+        for i, n in enumerate(lens):
+            ps = synth.random_pulsars(np.random.default_rng(seed + i), 6, 0.5, 200.0, 0.02, 0.2, 8.0, 20.0)
+            out.append(synth.make_spectrum_fd(n, 64e-6, ps, seed + i))
+        return out
+    first = spectra(500)
+    dev = [torch.from_numpy(a.view(np.float32).copy()).cuda() for a in first]
+    files = [((d.data_ptr(), len(a)), n, 64e-6) for d, a, n in zip(dev, first, lens)]
+    params = cs.SearchParams(nharms=32, m=16, decimations=cs.decimation_set(32, 4), synth="fp16")
+    side = torch.cuda.Stream()
+    ref = cs.Engine(params)
+    want, wown = ref.search_batch_raw(files, 1.0, 60.0, 100, 2048, 8.0, on_device=True)
+    assert len(want) > 0
+    eng = cs.Engine(params)
+    eng.set_stream(side.cuda_stream)
+    eng.set_batch_graph(True)
+    for _ in range(3):                       # capture, then replays
+        got, own = eng.search_batch_raw(files, 1.0, 60.0, 100, 2048, 8.0, on_device=True)
+        side.synchronize()
+        assert np.array_equal(got, want) and np.array_equal(own, wown)
+    # refill in place: the replay searches the new contents
+    second = spectra(900)
+    for d, a in zip(dev, second):
+        d.copy_(torch.from_numpy(a.view(np.float32).copy()).cuda())
+    torch.cuda.synchronize()
+    want2, wown2 = ref.search_batch_raw(files, 1.0, 60.0, 100, 2048, 8.0, on_device=True)
+    got2, own2 = eng.search_batch_raw(files, 1.0, 60.0, 100, 2048, 8.0, on_device=True)
+    assert np.array_equal(got2, want2) and np.array_equal(own2, wown2)
+    # an unrelated search drops the graph; the next batch rebuilds it
+    eng.set_spectrum(cs.FFTFile.from_array(second[0], lens[0], 64e-6))
+    eng.search_raw(1.0, 60.0, 100, 2048, 8.0)
+    got3, own3 = eng.search_batch_raw(files, 1.0, 60.0, 100, 2048, 8.0, on_device=True)
+    assert np.array_equal(got3, want2) and np.array_equal(own3, wown2)

@@ -204,10 +204,11 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// Bounded wait on an mbarrier phase: gives up after kWaitLimit polls or one
-// second of wall time, whichever comes first.
+// Bounded wait on an mbarrier phase: gives up after kWaitLimit polls or about
+// one second of wall time, whichever comes first.  The clock is first read
+// after 1024 polls: a wait that ends sooner (nearly every one) reads no timer.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    const uint64_t t0 = global_ns();
+    uint64_t t0 = 0;
     for (uint32_t it = 0; it < kWaitLimit; ++it) {
         uint32_t done;
         asm volatile(
@@ -218,7 +219,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
             : "r"(smem_u32(bar)), "r"(parity)
             : "memory");
         if (done) return true;
-        if ((it & 1023u) == 1023u && global_ns() - t0 > 1000000000ull) return false;
+        if ((it & 1023u) == 1023u) {
+            const uint64_t now = global_ns();
+            if (t0 == 0) t0 = now;
+            else if (now - t0 > 1000000000ull) return false;
+        }
     }
     return false;
 }

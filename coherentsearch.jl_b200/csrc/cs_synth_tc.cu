@@ -169,29 +169,106 @@ struct Unroll<N, N, G> {
     __device__ __forceinline__ static void run(G&, const float*, int, int) {}
 };
 
+// Streams pw columns out of TMEM through the scan g.
 // pw (the level's padded column count) is a multiple of HM.
-template <int HM, uint32_t MASK>
-__device__ __noinline__ float gate_level(uint32_t tcol, int nbins, int pw, uint32_t wmask,
-                                         const float* __restrict__ rsq) {
-    GateScan<HM, MASK> g;
-    g.init(wmask);
+template <class G>
+__device__ __forceinline__ void scan_cols(G& g, uint32_t tcol, int nbins, int pw) {
     for (int c0 = 0; c0 < pw; c0 += 32) {
         if (c0 + 32 <= pw) {
             float x[32];
             tmem_ld32(tcol + c0, x);
             if (c0 + 32 < nbins)
-                Unroll2<0, 32, true, GateScan<HM, MASK>>::run(g, x, c0, nbins);
+                Unroll2<0, 32, true, G>::run(g, x, c0, nbins);
             else
-                Unroll2<0, 32, false, GateScan<HM, MASK>>::run(g, x, c0, nbins);
+                Unroll2<0, 32, false, G>::run(g, x, c0, nbins);
         } else {
             for (int c1 = c0; c1 < pw; c1 += 8) {   // HM == 8 here: pw is a multiple of 8
                 float x[8];
                 tmem_ld8(tcol + c1, x);
-                Unroll2<0, 8, false, GateScan<HM, MASK>>::run(g, x, c1, nbins);
+                Unroll2<0, 8, false, G>::run(g, x, c1, nbins);
             }
         }
     }
+}
+
+__host__ __device__ constexpr int top_width(uint32_t m) {
+    int w = 0;
+    while (m) { ++w; m >>= 1; }
+    return w;
+}
+
+// Gate value of one unit (its starts [0, nbins), columns [0, pw)).
+//
+// Window-energy bound: a boxcar of width w <= W (the widest of the level) lies
+// inside the width-W window at its start, so by Cauchy-Schwarz
+//   S_w(p) / sqrt(w) <= sqrt(sum of x^2 over [p, p+W)) <= sqrt(L),
+// L the largest width-W sum of squares over the unit's starts -- a one-width
+// scan of x^2, a third of the cost of the full gate scan.  B below adds the
+// rounding of both scans (prefix sums of at most 512 columns: an error of at
+// most 2^-14 of the sum of |x| in the gate, 2^-14 of the sum of x^2 in L) and
+// 2^-16 for the rest, so B >= the gate value the full scan would compute.  When
+// B < cut for every valid trial of the warp (cut: the value below which a gate
+// can neither be flagged for the rescan nor pushed as a candidate; -inf when
+// the exact gate values are wanted), the warp skips the full scan and returns
+// -inf, which leaves the flagged set and the candidates unchanged.
+// The largest sum of squares over W consecutive columns, streamed like
+// GateScan: prefix sums q of x^2 (one fused multiply-add per column) and a ring
+// of them.  Every window that ends inside the pw columns counts, also those
+// starting past the unit's last start: a larger maximum is still a bound, and
+// no column needs a test.
+template <int HM, int W>
+struct EnergyScan {
+    float ring[HM];
+    float q;
+    float mx;
+
+    __device__ __forceinline__ void init() {
+#pragma unroll
+        for (int d = 0; d < HM; ++d) ring[d] = INFINITY;   // no window starts before column 0
+        ring[0] = 0.0f;
+        q = 0.0f;
+        mx = -INFINITY;
+    }
+    template <int SLOT, bool FAST>
+    __device__ __forceinline__ void step2(float x0, float x1, int, int) {
+        const float q0 = fmaf(x0, x0, q);
+        const float q1 = fmaf(x1, x1, q0);
+        const float d0 = q0 - ring[(SLOT - W + HM) % HM];
+        const float d1 = q1 - (W == 1 ? q0 : ring[(SLOT + 1 - W + HM) % HM]);
+        mx = fmax3(mx, d0, d1);
+        ring[SLOT % HM] = q0;
+        ring[(SLOT + 1) % HM] = q1;
+        q = q1;
+    }
+};
+
+template <int HM, int W>
+__device__ __forceinline__ float energy_bound(uint32_t tcol, int nbins, int pw) {
+    EnergyScan<HM, W> e;
+    e.init();
+    scan_cols(e, tcol, nbins, pw);
+    return (sqrtf(e.mx + e.q * 0x1p-13f) + 0x1p-13f * sqrtf((float)pw * e.q)) * (1.0f + 0x1p-16f);
+}
+
+template <int HM, uint32_t MASK>
+__device__ __noinline__ float full_gate(uint32_t tcol, int nbins, int pw, uint32_t wmask,
+                                        const float* __restrict__ rsq) {
+    GateScan<HM, MASK> g;
+    g.init(wmask);
+    scan_cols(g, tcol, nbins, pw);
     return g.finish(rsq);
+}
+
+template <int HM, uint32_t MASK>
+__device__ __noinline__ float gate_level(uint32_t tcol, int nbins, int pw, uint32_t wmask,
+                                         const float* __restrict__ rsq, float cut, bool valid) {
+    if constexpr (MASK != 0u) {
+        if (cut > 0.0f) {   // cut is the level's: warp-uniform
+            const float B = energy_bound<HM, top_width(MASK)>(tcol, nbins, pw);
+            if (__all_sync(0xffffffffu, !valid || B < cut)) return -INFINITY;
+        }
+    }
+    return full_gate<HM, MASK>(tcol, nbins, pw, wmask, rsq);
 }
 
 // Width sets of the decimation ladder and of the plain geometric bank.
@@ -200,15 +277,19 @@ constexpr uint32_t kMaskLadderDeep = 0x2Eu;   // {2,3,4,6}
 
 template <int HM>
 __device__ __forceinline__ float gate_dispatch(uint32_t tcol, int nbins, int pw, uint32_t wmask,
-                                               const float* __restrict__ rsq) {
+                                               const float* __restrict__ rsq, float cut, bool valid) {
     if (HM == 8) {
-        if (wmask == kMaskLadderBase) return gate_level<8, kMaskLadderBase>(tcol, nbins, pw, wmask, rsq);
-        if (wmask == kMaskLadderDeep) return gate_level<8, kMaskLadderDeep>(tcol, nbins, pw, wmask, rsq);
-        return gate_level<8, 0u>(tcol, nbins, pw, wmask, rsq);
+        if (wmask == kMaskLadderBase)
+            return gate_level<8, kMaskLadderBase>(tcol, nbins, pw, wmask, rsq, cut, valid);
+        if (wmask == kMaskLadderDeep)
+            return gate_level<8, kMaskLadderDeep>(tcol, nbins, pw, wmask, rsq, cut, valid);
+        return gate_level<8, 0u>(tcol, nbins, pw, wmask, rsq, cut, valid);
     }
-    if (wmask == 0x4112Fu) return gate_level<32, 0x4112Fu>(tcol, nbins, pw, wmask, rsq);  // {1,..,13,19}
-    if (wmask == 0x804112Fu) return gate_level<32, 0x804112Fu>(tcol, nbins, pw, wmask, rsq);
-    return gate_level<32, 0u>(tcol, nbins, pw, wmask, rsq);
+    if (wmask == 0x4112Fu)   // {1,..,13,19}
+        return gate_level<32, 0x4112Fu>(tcol, nbins, pw, wmask, rsq, cut, valid);
+    if (wmask == 0x804112Fu)
+        return gate_level<32, 0x804112Fu>(tcol, nbins, pw, wmask, rsq, cut, valid);
+    return gate_level<32, 0u>(tcol, nbins, pw, wmask, rsq, cut, valid);
 }
 
 }  // namespace
@@ -234,6 +315,7 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     __shared__ uint8_t lu_start[kMaxLevels + 1], lu_idx[kMaxUnits];
     __shared__ float inv_sh[kMaxLevels];        // 1/sigma of the tile's block, per level
     __shared__ int nv_sh[kMaxLevels];           // valid trials of the tile's block, per level
+    __shared__ float cut_sh[kMaxLevels];        // gate bound for skipping a warp's scan, per level
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
@@ -279,24 +361,50 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     if (tid == 0 && (int)blockIdx.x < ntiles)
         bulk_load(smem_u32(As0), a.Atile + (int64_t)blockIdx.x * abytes, abytes, &lbar[0]);
 
+    // The per-level sigma and valid counts of the first tile's block; each
+    // iteration then loads the next tile's while its own MMA and epilogue run.
+    float sig_next = 0.0f;
+    int nv_next = 0;
+    if (tid < t.nlev && (int)blockIdx.x < ntiles) {
+        const int b0 = (int)blockIdx.x / tiles_per_blk;
+        sig_next = a.sigma[b0 * a.nlev + tid];
+        nv_next = a.nvalid[b0 * a.nlev + tid];
+    }
+
     int it = 0;
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
         const int buf = nbuf == 2 ? (it & 1) : 0;
         const int blk = tile / tiles_per_blk;
         const int j0 = (tile % tiles_per_blk) * kTM;
-        // the block's per-level sigma and valid counts, for the epilogue (ordered
-        // by the barrier below; the previous epilogue finished at the loop's end)
-        if (tid < t.nlev) {
-            // 1/sigma times the A tiles' scale 2^s (exact): the gate in true units
-            inv_sh[tid] = inv_sigma(a.sigma[blk * a.nlev + tid]) * gup;
-            nv_sh[tid] = a.nvalid[blk * a.nlev + tid];
-        }
         // Prefetch the next tile into the other buffer: its previous reader (the
         // MMA of the last iteration) has completed.
         if (nbuf == 2 && tid == 0 && tile + (int)gridDim.x < ntiles)
             bulk_load(smem_u32(As0 + (buf ^ 1) * abytes), a.Atile + (int64_t)(tile + gridDim.x) * abytes,
                       abytes, &lbar[buf ^ 1]);
-        ok = __syncthreads_and(mbar_wait(&lbar[buf], (uint32_t)(nbuf == 2 ? ((it >> 1) & 1) : (it & 1)))) != 0;
+        // the block's per-level sigma and valid counts, for the epilogue (ordered
+        // by the barrier below; the previous epilogue finished at the loop's end)
+        if (tid < t.nlev) {
+            // 1/sigma times the A tiles' scale 2^s (exact): the gate in true units
+            const float inv = inv_sigma(sig_next) * gup;
+            inv_sh[tid] = inv;
+            nv_sh[tid] = nv_next;
+            // a gate g (TMEM units) with g < cut has g*inv below both medcut_gate
+            // and the threshold, so gate_flag would neither flag nor push it
+            float cut = -INFINITY;
+            const float c = fminf(a.medcut_gate, a.threshold);
+            if (!a.Q0 && inv > 0.0f && c > 0.0f) cut = (c / inv) * (1.0f - 0x1p-16f);
+            cut_sh[tid] = cut;
+            const int tn = tile + (int)gridDim.x;
+            if (tn < ntiles) {
+                const int bn = tn / tiles_per_blk;
+                sig_next = a.sigma[bn * a.nlev + tid];
+                nv_next = a.nvalid[bn * a.nlev + tid];
+            }
+        }
+        // Only the MMA (issued by thread 0) reads the A tile: warp 0 waits for
+        // it, and the barrier holds the other warps.
+        ok = __syncthreads_and(warp == 0 ? mbar_wait(&lbar[buf], (uint32_t)(nbuf == 2 ? ((it >> 1) & 1) : (it & 1)))
+                                         : true) != 0;
         if (!ok) {
             if (tid == 0) atomicExch(err, 2);
             break;
@@ -340,16 +448,23 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
             const int wg = warp >> 2;
             const int row = (warp & 3) * 32 + (tid & 31);
             const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+            // need: a gate of the tile may be flagged or pushed.  A -inf gate
+            // whose level could skip (cut > 0, so 1/sigma > 0) is neither, so
+            // a tile whose every unit returned -inf there needs no medcut pass.
+            bool need = false;
             for (int u = 0; u < t.nunit; ++u) {
                 const TcUnit& U = unit_sh[u];
                 if (U.wg != wg) continue;                               // warp-uniform
                 if (j0 >= nv_sh[U.lev]) continue;                       // warp-uniform
                 const TcLevel& L = lev_sh[U.lev];
-                part_sh[u][row] = gate_dispatch<HM>(lane_base + (uint32_t)U.col, U.nstart, U.pw, L.wmask, L.rsq);
+                const float cut = cut_sh[U.lev];
+                const float v = gate_dispatch<HM>(lane_base + (uint32_t)U.col, U.nstart, U.pw, L.wmask, L.rsq, cut,
+                                                  j0 + row < nv_sh[U.lev]);
+                part_sh[u][row] = v;
+                need |= !(cut > 0.0f) || v != -INFINITY;
             }
-            __syncthreads();
             // gate = max over the level's units, then the medcut test
-            for (int idx = tid; idx < t.nlev * kTM; idx += blockDim.x) {
+            if (__syncthreads_or(need)) for (int idx = tid; idx < t.nlev * kTM; idx += blockDim.x) {
                 const int l = idx / kTM, r = idx % kTM;
                 const int j = j0 + r;
                 if (j >= nv_sh[l]) continue;

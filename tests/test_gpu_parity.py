@@ -259,6 +259,26 @@ def test_tensor_candidates_identical_to_plain(synth):
     assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("synth,ladder", [("fp16", True), ("bf16_split", True), ("fp16", False)])
+def test_tensor_gate_skip_keeps_the_flagged_set(synth, ladder):
+    """The tensor epilogue skips a warp's full gate scan when a window-energy
+    bound puts every trial of the warp below the medcut test.  With the exact
+    gate values requested (diagnostics level 2) nothing is skipped; the
+    rescanned trial count and the candidates must be the same either way, on
+    the decimation ladder's widths and on the plain geometric width bank."""
+    amps, N, dt = multi_spectrum()
+    cs = _cs()
+    dec = cs.decimation_set(60, 6) if ladder else [1]
+    out = {}
+    for diag in (2, 0):
+        eng = _engine(cs.SearchParams(nharms=60, m=16, decimations=dec, synth=synth), amps, N, dt, diag=diag)
+        c = eng.search_raw(0.2, 180.0, 100, 2048, 8.0)
+        out[diag] = (c, eng.stats()["rescued"])
+    assert out[2][1] > 0 and len(out[2][0]) > 0
+    assert out[0][1] == out[2][1]
+    assert np.array_equal(out[0][0], out[2][0])
+
+
 @pytest.mark.parametrize("synth", ["bf16", "fp16"])
 def test_tensor_bright_spectrum_scale_invariant(synth):
     """A spectrum scaled by 2^17 (noise amplitudes ~1e5, past FP16's 65504)

@@ -100,10 +100,10 @@ struct GateScan {
         ps = 0.0f;
         wm = MASK ? MASK : runtime_mask;
     }
-    // Two bins at columns e_bin, e_bin+1 (ring slots SLOT, SLOT+1): the same
-    // adds as two single steps, each width's maximum taken over both columns
-    // by one three-input max.  FAST: both columns lie before the profile's
-    // last bin, so the ring takes the prefix sums without a test.
+    // Two bins at columns e_bin, e_bin+1 (ring slots SLOT, SLOT+1): two
+    // sequential prefix adds, each width's maximum taken over both columns by
+    // one three-input max.  FAST: both columns lie before the profile's last
+    // bin, so the ring takes the prefix sums without a test.
     template <int SLOT, bool FAST>
     __device__ __forceinline__ void step2(float x0, float x1, int e_bin, int nbins) {
         const float ps0 = ps + x0;
@@ -122,17 +122,6 @@ struct GateScan {
         ring[SLOT % HM] = r0;
         ring[(SLOT + 1) % HM] = r1;
         ps = ps1;
-    }
-    // One bin at column e_bin, whose ring slot of position e_bin+1 is SLOT.
-    template <int SLOT>
-    __device__ __forceinline__ void step(float x, int e_bin, int nbins) {
-        ps += x;
-#pragma unroll
-        for (int w = 1; w <= HM; ++w) {
-            const bool on = MASK ? ((MASK >> (w - 1)) & 1u) : ((wm >> (w - 1)) & 1u);
-            if (on) mw[w - 1] = fmaxf(mw[w - 1], ps - ring[(SLOT - w + HM) % HM]);
-        }
-        ring[SLOT % HM] = (e_bin + 1 < nbins) ? ps : INFINITY;
     }
     __device__ __forceinline__ float finish(const float* __restrict__ rsq) const {
         float best = -INFINITY;
@@ -154,18 +143,6 @@ struct Unroll2 {
 };
 template <int N, bool FAST, class G>
 struct Unroll2<N, N, FAST, G> {
-    __device__ __forceinline__ static void run(G&, const float*, int, int) {}
-};
-
-template <int U, int N, class G>
-struct Unroll {
-    __device__ __forceinline__ static void run(G& g, const float* x, int base, int nbins) {
-        g.template step<U + 1>(x[U], base + U, nbins);
-        Unroll<U + 1, N, G>::run(g, x, base, nbins);
-    }
-};
-template <int N, class G>
-struct Unroll<N, N, G> {
     __device__ __forceinline__ static void run(G&, const float*, int, int) {}
 };
 

@@ -4,8 +4,9 @@ A small network scores each block of the band from its incoherent power-sum
 features (``Engine.block_features``, cs_block_features).  The blocks whose
 score reaches a threshold -- the proposed ones and the ones the network is
 unsure of -- are re-searched by the coherent search (``Engine.
-search_blocks_raw``, cs_search_blocks), which stays the judge: recall is
-measured against the full search's candidates.
+search_blocks_raw``, cs_search_blocks), which keeps the final word: every
+reported candidate is the coherent search's, and recall is measured against
+the full search's candidates.
 
 The network (2*nharms -> 256 -> 256 -> 1, ReLU, BF16 weights, FP32
 accumulation) runs and trains through the library's own kernels

@@ -1,8 +1,8 @@
 // cs_mlp.cu -- the learned block proposal: per-block incoherent power-sum
 // features and a small MLP (features -> 256 -> 256 -> 1, BF16 weights, FP32
 // accumulation) with its training kernels.  No counterpart in the reference:
-// it scores frequency blocks so that the coherent search (the judge of
-// recall) re-searches only the proposed ones.
+// it scores frequency blocks so that the coherent search, which reports
+// every candidate, re-searches only the proposed ones.
 //
 // The network is tiny (147*256 + 256*256 + 256 weights): a training batch is
 // a few MFLOP, so the layers are plain tiled SIMT products (FP32 accumulation

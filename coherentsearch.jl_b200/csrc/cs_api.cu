@@ -1429,6 +1429,10 @@ cs_status cs_search_batch(cs_handle* H, const cs_spectrum* files, int32_t nfiles
                     // again the ordinary way (the graph is dropped and rebuilt)
                     st = search_core(H, lofreq, hifreq, lobin, blocksize, threshold, 0, 0, -1, &all);
                     if (st != CS_OK) return st;
+                    // the re-search's own launches and copies count too
+                    tot.launches += H->stats.launches;
+                    tot.h2d_bytes += H->stats.h2d_bytes;
+                    tot.d2h_bytes += H->stats.d2h_bytes;
                 } else {
                     const DevCand* pre = reinterpret_cast<const DevCand*>(H->gslots[i].io.as<uint8_t>() + 64);
                     std::vector<DevCand> raw(pre, pre + n_c);

@@ -341,6 +341,36 @@ def test_batch_equals_file_by_file_searches():
     assert any(len(raw[owner == i]) > 0 for i in range(len(files)))
 
 
+def test_batch_graph_prefix_overflow_searches_again():
+    """A replayed spectrum with more candidates than the captured 4096-record
+    prefix is searched again the ordinary way: the records still equal the
+    ordinary batch's, replay after replay."""
+    import torch
+    from cohsearch import synth
+    cs = _cs()
+    lens = [1 << 18, 1 << 12]
+    arrs = [synth.make_spectrum_fd(n, 64e-6, [], 40 + i) for i, n in enumerate(lens)]
+    dev = [torch.from_numpy(a.view(np.float32).copy()).cuda() for a in arrs]
+    files = [((d.data_ptr(), len(a)), n, 64e-6) for d, a, n in zip(dev, arrs, lens)]
+    # the first threshold (noise only) that puts the long spectrum past the prefix
+    for thr in (3.0, 2.5, 2.0, 1.5):
+        params = cs.SearchParams(nharms=32, m=16, decimations=cs.decimation_set(32, 4), threshold=thr,
+                                 synth="fp16")
+        ref = cs.Engine(params)
+        want, wown = ref.search_batch_raw(files, 1.0, 60.0, 100, 2048, thr, on_device=True)
+        if np.bincount(wown, minlength=len(lens))[0] > 4096:
+            break
+    assert np.bincount(wown, minlength=len(lens))[0] > 4096
+    side = torch.cuda.Stream()
+    eng = cs.Engine(params)
+    eng.set_stream(side.cuda_stream)
+    eng.set_batch_graph(True)
+    for _ in range(3):
+        got, own = eng.search_batch_raw(files, 1.0, 60.0, 100, 2048, thr, on_device=True)
+        side.synchronize()
+        assert np.array_equal(got, want) and np.array_equal(own, wown)
+
+
 def test_batch_graph_replays_the_ordinary_batch():
     """cs_set_batch_graph: the batch of device spectra run once the ordinary
     way, captured into one graph and replayed -- the same records as the

@@ -1,11 +1,16 @@
 # CohSearchB200.jl -- Julia binding of libcohsearch_cuda.so (include/cohsearch.h).
 #
 # Drop-in device dispatch for CoherentSearch.jl: `device_search_region` has the
-# inputs and result of `_search_region!` (src/search.jl:1768-1894), and
-# `device_chunk_metrics` those of `chunk_metrics` (src/search.jl:1740-1755).
-# A maintainer wires them in as shown in INTEGRATION.md.  No Julia is
-# installed where this library is built, so this file is exercised through
-# the identical C ABI by the Python binding (coherentsearch.jl_b200/cohsearch).
+# inputs and result of `_search_region!` (src/search.jl:1768-1894),
+# `device_chunk_metrics` those of `chunk_metrics` (src/search.jl:1740-1755);
+# then block ranges (`device_search_range`), the batch over files
+# (`device_search_batch`, `set_batch_graph!`), `block_metrics`
+# (`device_block_metrics`), `candidate_profile` / `measure_ducy`
+# (`device_refold`) and MetricStats / MetricNorm (`set_metricstats!`,
+# `block_stats`, `metric_hists`, `set_metricnorm!`).  A maintainer wires them
+# in as shown in INTEGRATION.md.  No Julia is installed where this library is
+# built: every ccall is checked against include/cohsearch.h by a host test, and
+# the same C calls run through the Python binding (coherentsearch.jl_b200/cohsearch).
 module CohSearchB200
 
 const LIB = joinpath(@__DIR__, "..", "lib", "libcohsearch_cuda.so")

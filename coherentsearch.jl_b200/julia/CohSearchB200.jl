@@ -7,9 +7,10 @@
 # (`device_search_batch`, `set_batch_graph!`), `block_metrics`
 # (`device_block_metrics`), `candidate_profile` / `measure_ducy`
 # (`device_refold`) and MetricStats / MetricNorm (`set_metricstats!`,
-# `block_stats`, `metric_hists`, `set_metricnorm!`).  A maintainer wires them
-# in as shown in INTEGRATION.md.  No Julia is installed where this library is
-# built: every ccall is checked against include/cohsearch.h by a host test, and
+# `block_stats`, `metric_hists`, `set_metricnorm!`).  In `search`
+# (src/search.jl:2080-2094) the detection pass's `_search_region!` call becomes
+# `set_spectrum!` + `device_search_region` on a handle cached per params.  No
+# Julia is installed where this library is built: every ccall is checked against include/cohsearch.h by a host test, and
 # the same C calls run through the Python binding (coherentsearch.jl_b200/cohsearch).
 module CohSearchB200
 

@@ -10,8 +10,9 @@
 # `block_stats`, `metric_hists`, `set_metricnorm!`).  In `search`
 # (src/search.jl:2080-2094) the detection pass's `_search_region!` call becomes
 # `set_spectrum!` + `device_search_region` on a handle cached per params.  No
-# Julia is installed where this library is built: every ccall is checked against include/cohsearch.h by a host test, and
-# the same C calls run through the Python binding (coherentsearch.jl_b200/cohsearch).
+# Julia is installed where this library is built: a host test checks every
+# ccall against include/cohsearch.h, and the same C calls run through the
+# Python binding (coherentsearch.jl_b200/cohsearch).
 module CohSearchB200
 
 const LIB = joinpath(@__DIR__, "..", "lib", "libcohsearch_cuda.so")

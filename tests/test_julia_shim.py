@@ -5,6 +5,10 @@ include/cohsearch.h declares, with as many argument types as the prototype has
 parameters."""
 import os
 import re
+import shutil
+import subprocess
+
+import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 JL = os.path.join(ROOT, "coherentsearch.jl_b200", "julia", "CohSearchB200.jl")
@@ -72,3 +76,69 @@ def test_julia_binding_covers_the_reference_facing_calls():
             "cs_set_batch_graph", "cs_chunk_metrics", "cs_block_metrics", "cs_refold", "cs_set_metricstats",
             "cs_get_block_stats", "cs_get_metric_hists", "cs_set_metricnorm", "cs_last_error"}
     assert want <= names, sorted(want - names)
+
+
+_JL_SIZES = {"Int32": (4, 4), "Int64": (8, 8), "Float32": (4, 4), "Float64": (8, 8), "UInt32": (4, 4)}
+
+
+def _jl_field_layout(tname):
+    """(size, align) of a Julia field type as Julia lays isbits structs out
+    for C: natural alignment, NTuple{n,T} as an array, pointers 8 bytes."""
+    if tname.startswith("Ptr{"):
+        return 8, 8
+    m = re.fullmatch(r"NTuple\{(\d+),\s*(\w+)\}", tname)
+    if m:
+        sz, al = _JL_SIZES[m.group(2)]
+        return int(m.group(1)) * sz, al
+    return _JL_SIZES[tname]
+
+
+def _jl_structs():
+    text = open(JL).read()
+    out = {}
+    for m in re.finditer(r"^struct (CS\w+)\n(.*?)^end", text, re.S | re.M):
+        fields, off, align = [], 0, 1
+        for ln in m.group(2).splitlines():
+            fm = re.match(r"\s*(\w+)::(\S+)", ln)
+            if not fm:
+                continue
+            sz, al = _jl_field_layout(fm.group(2))
+            off = (off + al - 1) // al * al
+            fields.append((fm.group(1), off))
+            off += sz
+            align = max(align, al)
+        out[m.group(1)] = (fields, (off + align - 1) // align * align)
+    return out
+
+
+def test_julia_structs_match_the_c_layout():
+    """CSParams, CSCandidate, CSSpectrum and CSBlockStats against the header
+    as gcc lays it out: same field names, offsets and sizes."""
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    pairs = {"CSParams": "cs_params", "CSCandidate": "cs_candidate", "CSSpectrum": "cs_spectrum",
+             "CSBlockStats": "cs_block_stats"}
+    jl = _jl_structs()
+    assert set(pairs) <= set(jl)
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "cohsearch.h"', "int main(void) {"]
+    for js, cs in pairs.items():
+        lines.append(f'    printf("{cs} sizeof %zu\\n", sizeof({cs}));')
+        for fname, _ in jl[js][0]:
+            lines.append(f'    printf("{cs} {fname} %zu\\n", offsetof({cs}, {fname}));')
+    lines += ["    return 0;", "}"]
+    out = os.path.join(ROOT, "_build", "julia_layout")
+    os.makedirs(out, exist_ok=True)
+    src, exe = os.path.join(out, "probe.c"), os.path.join(out, "probe")
+    with open(src, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    subprocess.run([gcc, "-std=c11", "-I", os.path.join(ROOT, "include"), "-o", exe, src], check=True)
+    got = {}
+    for ln in subprocess.run([exe], check=True, capture_output=True, text=True).stdout.splitlines():
+        name, field, val = ln.split()
+        got[(name, field)] = int(val)
+    for js, cs in pairs.items():
+        fields, size = jl[js]
+        assert got[(cs, "sizeof")] == size, js
+        for fname, off in fields:
+            assert got[(cs, fname)] == off, (js, fname)

@@ -9,10 +9,12 @@
 // level followed by that level's first wmax bins again (the wrapped tail of
 // the boxcar prefix sums, src/search.jl:571-578).  tcgen05.mma (M=128, K=16
 // per instruction, FP32 accumulation in TMEM) computes D; each epilogue thread
-// owns one trial's TMEM row and streams its bins through a register ring of
-// prefix sums to the zero-baseline gate value (src/search.jl:743-779) and the
-// block-sigma samples.  The gate only selects the trials that take the exact
-// FP32 rescan, so the reported S/N never depends on the reduced precision.
+// owns one trial's TMEM row.  It first bounds its gate by the largest window
+// energy of its bins (a one-width scan of x^2); a warp whose trials all stay
+// below the medcut test skips the rest.  Otherwise it streams its bins through
+// a register ring of prefix sums to the zero-baseline gate value
+// (src/search.jl:743-779).  The gate only selects the trials that take the
+// exact FP32 rescan, so the reported S/N never depends on the reduced precision.
 //
 // Layout: SWIZZLE_NONE K-major canonical UMMA layout -- 8-row x 16-byte core
 // matrices, K-adjacent core matrices 128 B apart (LBO), 8-row groups 2048 B

@@ -137,14 +137,26 @@ def interp_flops_per_trial(m=16):
     return NHARMS * (4 * m + 6)   # m real-times-complex FMAs + one complex product
 
 
+def tensor_flops_per_trial():
+    """Dense contraction of the Re/Im amplitude stack against every level's
+    cos/sin rows: 2 * sum_k (2 Hk)^2 flops."""
+    return sum(2 * (2 * Hk) ** 2 for _, Hk in level_list())
+
+
+# boxcar gate per trial (prefix sums + a subtract and a max per start and width, all levels)
+GATE_OPS_PER_TRIAL = 2922
+
+
+def sigma_flops_per_block():
+    """FP32 synthesis of the pooled sigma columns of one block, all levels: per
+    level min(2048, 8192 // nbins) columns of 4(Hk+1)(Hk-1) flops."""
+    return sum(min(BLOCK, 8192 // (2 * Hk)) * 4.0 * (Hk + 1) * (Hk - 1) for _, Hk in level_list())
+
+
 # DRAM bytes (read + write) per trial of one launch, from the ncu captures
 # summarised under profiles/ (small survey case, 1,282,048 trials; the traffic
 # of these kernels grows in proportion to the trial count).
 NCU_BYTES_PER_TRIAL = {"k_interp": 295.3, "k_synth_tc": 259.2, "k_sigma": 98.9, "k_rescue": 0.44}
-# Algorithmic DRAM bytes per trial: k_interp writes 240 B of FP16 A-tile chunks
-# and 96 B of sigma samples and reads ~4 B of spectrum; k_sigma reads the 96 B
-# of samples.
-ALG_BYTES_PER_TRIAL = {"k_interp": 340.0, "k_sigma": 96.0}
 
 
 def load_peaks():
@@ -218,7 +230,7 @@ def run_dmsweep(args, rank, local_rank):
 
 
 def run_learned(args, local_rank):
-    """The learned block proposal.  Training: separately
+    """The learned block proposal on a 2^24-sample spectrum.  Training: separately
     seeded 2^24-sample spectra with 200 injections each (f 0.1-750 Hz, duty
     1-20 %, S/N 6-20, frequency-domain synthesis), every block of the survey
     band labelled by the coherent search's own candidates (S/N > 8; the mixed
@@ -389,7 +401,7 @@ def run_ours(args, rank, world, local_rank):
         t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, ms_e2e = float(t[0]), float(t[1])
-    res = {"ms": ms, "ms_e2e": ms_e2e, "stage": stage, "launches": launches, "h2d": h2d, "d2h": d2h,
+    res = {"ms": ms, "ms_e2e": ms_e2e, "namps": namps, "stage": stage, "launches": launches, "h2d": h2d, "d2h": d2h,
            "trials": trials, "ncand": ncand, "clocks": clk.summary(), "stats": st, "plain": plain}
     del eng
     return res
@@ -398,20 +410,36 @@ def run_ours(args, rank, world, local_rank):
 # ---------------------------------------------------------------------------
 # CPU restatement (reference arm and cpu_baseline)
 # ---------------------------------------------------------------------------
-def cpu_sample_run(nthreads, nblocks, seed=2):
-    """Time the C port of the reference search on `nblocks` blocks of the
-    survey workload (mid-band, every harmonic and decimation valid)."""
-    from cohsearch import synth
+_CPU_SPECTRUM = {}
+
+
+def cpu_band_run(nthreads, nblocks=None, seed=2, first_block=None):
+    """Time the C port of the reference search (oracle/cs_cpu.c, all given
+    threads, blocks dealt round-robin as the reference's tasks take chunks) on
+    the survey workload: the whole band by default, else `nblocks` blocks from
+    `first_block` (mid-band when not given).  The port's c2r transform is a
+    direct FP64 DFT where the reference calls FFTW."""
     from oracle import cs_cpu
-    amps, N, dt = synth.survey_config(seed=seed)
+    if seed not in _CPU_SPECTRUM:
+        from cohsearch import synth
+        _CPU_SPECTRUM[seed] = synth.survey_config(seed=seed)
+    amps, N, dt = _CPU_SPECTRUM[seed]
     T = N * dt
     lodr = 0.5 / NHARMS
     r_lo = LOF * T
     total = int(math.floor((HIF * T - r_lo) / lodr)) + 1
-    first_block = (total // BLOCK) // 2
-    res = cs_cpu.search_blocks(amps, N, dt, NHARMS, 16, 0.5, [k for k, _ in level_list()], r_lo, total,
-                               BLOCK, first_block, nblocks, THR, nthreads)
-    return res
+    nblk_all = -(-total // BLOCK)
+    if nblocks is None:
+        first_block, nblocks = 0, nblk_all
+    elif first_block is None:
+        first_block = max(0, nblk_all // 2 - nblocks // 2)
+    return cs_cpu.search_blocks(amps, N, dt, NHARMS, 16, 0.5, [k for k, _ in level_list()], r_lo, total,
+                                BLOCK, first_block, nblocks, THR, nthreads)
+
+
+CPU_PORT_NOTE = ("C restatement of the reference's production search (Float32-weight interpolation, FP64 "
+                 "profiles, block sigma, batched FP32 gate, exact rescan); its c2r transform is a direct FP64 "
+                 "DFT where the reference calls FFTW")
 
 
 def main():
@@ -421,7 +449,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--synth", default="fp16", choices=["fp32", "bf16", "fp16", "bf16_split", "fp16_split"])
-    ap.add_argument("--cpu-blocks", type=int, default=None)
+    ap.add_argument("--cpu-blocks", type=int, default=None,
+                    help="CPU port legs: N mid-band blocks per step instead of the whole band (a quick check)")
     ap.add_argument("--workload", choices=["survey", "dmsweep", "learned"], default="survey",
                     help="survey: one 2^23-sample spectrum (the headline); dmsweep: 64 spectra of "
                          "2^21..2^24 samples through the batch entry point; learned: the learned block "
@@ -445,21 +474,27 @@ def main():
         if rank != 0:
             return 0
         nthreads = os.cpu_count() or 1
-        nblocks = args.cpu_blocks or max(8, 2 * nthreads)
+        # warm-up on a sliver of the band (the reference's own timing method,
+        # bench/thread_scaling.jl:83-97), then every timed step searches the
+        # whole band, as the GPU arm's step does
         for _ in range(args.warmup):
-            cpu_sample_run(nthreads, max(1, nthreads // 4))
-        times, trials = [], 0
+            cpu_band_run(nthreads, nblocks=2 * nthreads)
+        times, trials, nblk = [], 0, 0
         for _ in range(args.steps):
-            r = cpu_sample_run(nthreads, nblocks)
+            r = cpu_band_run(nthreads, nblocks=args.cpu_blocks)
             times.append(r["seconds"])
-            trials = r["trials"]
+            trials, nblk = r["trials"], r["blocks"]
         v = trials * len(times) / sum(times)
-        sample = f"{nblocks} blocks x {BLOCK} trials mid-band of the survey workload per step"
+        what = "whole band" if args.cpu_blocks is None else "mid-band sample"
+        sample = (f"{what} per step ({nblk} blocks x {BLOCK} trials, {trials} trials), {nthreads} threads; "
+                  + CPU_PORT_NOTE)
+        cfg = workload_config("cpu")
+        cfg["trials_per_step"] = trials
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": v, "unit": "trials/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": workload_config("cpu"),
+            "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": v, "unit": "trials/s", "cores": nthreads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": v, "unit": "trials/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
@@ -536,52 +571,72 @@ def main():
     peaks, psrc = load_peaks()
     stage = {k: v / K for k, v in res["stage"].items()}
     st = res["stats"]
-    frac_valid = {1: 1.0}
-    prof_per_trial = st["profiles"] / max(1, trials)
-    # roofline of the dominant kernel
+    # Roofline of the dominant kernel, on the algorithmic work per trial of the
+    # hot path (one fundamental trial through every harmonic and level):
+    #   interpolation  nharms*(4m+6) = 4,200 FP32 flops (FP32 SIMT pipe);
+    #   profiles       2*sum_k (2 Hk)^2 = 42,952 dense-contraction flops (tensor pipe);
+    #   gate scan      ~2,922 FP32 ops (boxcar prefix sums and maxima);
+    #   spectrum       the 32 MiB spectrum read once: ~4.2 B per trial (L2-resident).
+    # `traffic` is the kernel's measured DRAM bytes (ncu), and
+    # `traffic_over_algorithmic` how far it lies above that one spectrum read.
     dom = max(stage, key=stage.get)
-    fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12   # TFLOP/s, nominal
-    # dense product per trial: 2 * K(128) * N(352 columns), twice over hi and lo when split
-    tc_flops = trials * 2.0 * 128 * 352 * (2 if args.synth.endswith("_split") else 1)
+    mhz = peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12   # TFLOP/s, nominal (no measured FP32 figure exists)
+    tc_peak = peaks["bf16_tflops"]
     kname = {"ms_interp": "k_interp", "ms_synth": "k_synth_tc" if args.synth != "fp32" else "k_synth_fp32",
              "ms_sigma": "k_sigma", "ms_rescue": "k_rescue"}[dom]
+    alg_bytes = 8.0 * res["namps"] / trials        # the spectrum, read once, per trial
     traffic = NCU_BYTES_PER_TRIAL.get(kname)
     traffic = traffic * trials if traffic is not None else None
-    if kname == "k_synth_tc":
-        achieved = tc_flops / (stage[dom] / 1000.0) / 1e12
-        roof = {"kernel": kname, "bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
-                "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"], "traffic": traffic,
-                "work": "2*128*352 flops per trial (dense 16-bit product, all levels)"}
+    f_interp = interp_flops_per_trial()
+    f_tc = tensor_flops_per_trial()
+    f_box = GATE_OPS_PER_TRIAL
+    fp32_src = (f"nominal FP32 rate 148 SM x 128 lanes x 2 flops x {mhz:.0f} MHz (no measured FP32 peak); "
+                "of nominal")
+    if kname in ("k_synth_tc",):
+        work, unit, peak, bound = f_tc, "TFLOP/s", tc_peak, "tensor"
+        wnote = "2*sum_k (2 Hk)^2 = %d tensor flops per trial (dense profile contraction)" % f_tc
+        psrc_k = f"MEASURED_PEAKS.json bf16_tflops ({psrc}); of measured" if psrc == "measured" else \
+            "fallback 1,590 TFLOP/s; of fallback"
     elif kname == "k_synth_fp32":
-        fl = trials * synth_flops_per_trial({1: 1.0})
-        achieved = fl / (stage[dom] / 1000.0) / 1e12
-        roof = {"kernel": kname, "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
-                "peak_source": "nominal FP32 FMA rate 148 SM x 128 lanes x 2 x max SM clock "
-                               "(no measured FP32 peak exists)",
-                "work": "4(Hk+1)(Hk-1) flops per trial per level"}
-    else:
-        # (a stage without an algorithmic count is rated on its measured bytes)
-        alg_b = ALG_BYTES_PER_TRIAL.get(kname, NCU_BYTES_PER_TRIAL.get(kname, 0.0))
-        alg = alg_b * trials
-        achieved = alg / (stage[dom] / 1000.0) / 1e9
-        roof = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                "work": f"{alg_b:.0f} algorithmic DRAM bytes per trial"}
-        if kname == "k_interp":
-            fl = trials * interp_flops_per_trial()
-            roof["fp32"] = {"achieved_tflops": fl / (stage[dom] / 1000.0) / 1e12, "peak_tflops": fp32_peak,
-                            "work": "nharms*(4m+6) flops per trial",
-                            "note": "limited by shared-memory tap loads, not DRAM or FMA"}
-    roof["peak_source"] = roof.get("peak_source", f"MEASURED_PEAKS.json ({psrc})")
+        work, unit, peak, bound = synth_flops_per_trial({1: 1.0}) + f_box, "TFLOP/s", fp32_peak, "fp32"
+        wnote = "symmetric real DFT 4(Hk+1)(Hk-1) per level + gate scan, FP32 flops per trial"
+        psrc_k = fp32_src
+    elif kname == "k_interp":
+        work, unit, peak, bound = f_interp, "TFLOP/s", fp32_peak, "fp32"
+        wnote = "nharms*(4m+6) = %d FP32 flops per trial (16-tap Eqn-30 sums + phase factor)" % f_interp
+        psrc_k = fp32_src
+    else:   # k_sigma / k_rescue: FP32 profile synthesis of the pooled columns, per trial of the step
+        work = sigma_flops_per_block() / BLOCK
+        unit, peak, bound = "TFLOP/s", fp32_peak, "fp32"
+        wnote = "FP32 synthesis flops of the pooled sigma columns, per trial"
+        psrc_k = fp32_src
+    achieved = work * trials / (stage[dom] / 1000.0) / 1e12
+    roof = {"kernel": kname, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+            "frac": achieved / peak, "traffic": traffic,
+            "traffic_over_algorithmic": (traffic / (alg_bytes * trials)) if traffic else None,
+            "algorithmic_bytes_per_trial": alg_bytes, "work": wnote, "peak_source": psrc_k}
+    # the whole step against the path's bound: the slower of the FP32 SIMT work
+    # (interpolation + gate scan) and the tensor contraction
+    t_bound = max((f_interp + f_box) * trials / (fp32_peak * 1e12), f_tc * trials / (tc_peak * 1e12))
+    roof["step"] = {"bound_ms": t_bound * 1e3, "measured_ms": res["ms"] / K,
+                    "frac": t_bound * 1e3 / (res["ms"] / K),
+                    "work": "max((4,200 + 2,922) FP32 flops / FP32 peak, 42,952 tensor flops / BF16 peak) "
+                            "per trial"}
     roof["stage_ms"] = stage
     cpu = None
     try:
         if args.no_cpu:
             raise RuntimeError("skipped (--no-cpu)")
-        r = cpu_sample_run(os.cpu_count() or 1, args.cpu_blocks or max(8, 2 * (os.cpu_count() or 1)))
-        cpu = {"value": r["trials"] / r["seconds"], "unit": "trials/s", "cores": r["threads"],
-               "kind": "port", "sample": f"{r['blocks']} blocks x {BLOCK} trials mid-band of the workload"}
+        nthreads = os.cpu_count() or 1
+        cpu_band_run(nthreads, nblocks=2 * nthreads)   # warm-up on a sliver of the band
+        runs = [cpu_band_run(nthreads, nblocks=args.cpu_blocks) for _ in range(3)]
+        secs = sorted(r["seconds"] for r in runs)
+        r = runs[0]
+        what = "whole band" if args.cpu_blocks is None else "mid-band sample"
+        cpu = {"value": r["trials"] / secs[1], "unit": "trials/s", "cores": r["threads"], "kind": "port",
+               "sample": f"{what} ({r['blocks']} blocks, {r['trials']} trials), median of 3 runs; "
+                         + CPU_PORT_NOTE}
     except Exception as e:  # the baseline is reported, never required
         cpu = {"value": None, "unit": "trials/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
     cfg = workload_config(args.synth)

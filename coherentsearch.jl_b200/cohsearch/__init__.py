@@ -10,7 +10,8 @@ from .metricstats import (BlockMetricStats, MetricHistogram, MetricNorm, MetricS
 from .search import (Candidate, Engine, SearchCache, SearchParams, block_metrics, boxcar_widths, candidate_profile,
                      chunk_metrics, measure_ducy, rotate_to_peak,
                      decimation_set, ladder_boxcar_widths, proftype, remove_duplicates,
-                     remove_harmonics, search, search_batch, search_block, write_candidates)
+                     remove_harmonics, search, search_batch, search_block, write_candidates, output_path,
+                     search_files)
 
 __all__ = [
     "CohSearchError", "LIB_PATH", "load_library", "FFTFile", "SimpleInf", "freqs", "write_fft",
@@ -18,5 +19,6 @@ __all__ = [
     "decimation_set", "ladder_boxcar_widths", "proftype", "remove_duplicates", "remove_harmonics",
     "search", "write_candidates", "BlockMetricStats", "MetricHistogram", "MetricNorm", "MetricStats",
     "build_metricnorm", "hist_quantile", "metricstats_summary", "metricstats_windows", "block_metrics",
-    "search_block", "search_batch", "candidate_profile", "measure_ducy", "rotate_to_peak",
+    "search_block", "search_batch", "candidate_profile", "measure_ducy", "rotate_to_peak", "output_path",
+    "search_files",
 ]

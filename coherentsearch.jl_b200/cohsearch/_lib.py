@@ -127,6 +127,8 @@ PROTOTYPES = {
     "cs_search_block_values": (_i32, [_P, _P, _P, _i64, ctypes.POINTER(_i64)]),
     "cs_search_trial_metrics": (_i32, [_P, _P, _i64, ctypes.POINTER(_i64)]),
     "cs_set_diagnostics": (_i32, [_P, _i32]),
+    "cs_set_memory_limit": (_i32, [_P, _i64]),
+    "cs_set_wait_test": (_i32, [_P, _i64]),
     "cs_search_gate_values": (_i32, [_P, _P, _i64, ctypes.POINTER(_i64)]),
     "cs_version": (ctypes.c_char_p, []),
     "cs_set_metricstats": (_i32, [_P, _i32, _f64, _f64, _i32, _i32]),

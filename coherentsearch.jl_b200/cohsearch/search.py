@@ -3,7 +3,9 @@
 Same names, argument meaning and error behaviour as the Julia API
 (src/CoherentSearch.jl:17-51): ``SearchParams``, ``decimation_set``,
 ``search``, ``SearchCache``, ``chunk_metrics``, ``Candidate``,
-``remove_duplicates``, ``remove_harmonics``, ``write_candidates``.  The hot
+``remove_duplicates``, ``remove_harmonics``, ``write_candidates``, and the
+command line's per-file loop with its ``.cohout`` naming (``search_files``,
+``output_path``).  The hot
 loop runs in ``libcohsearch_cuda.so`` through the C ABI; only the
 post-processing of the few hundred raw detections (duplicate and harmonic
 collapse, src/search.jl:2148-2214) runs here, as it runs in Julia in the
@@ -351,6 +353,17 @@ class Engine:
                                                    ctypes.byref(n)), self._h)
         return sig, nv
 
+    def set_memory_limit(self, nbytes: int):
+        """Cap the device memory the engine holds (0: no cap); searches split
+        into waves under it, or raise CohSearchError(CS_ERR_OUT_OF_MEMORY)."""
+        _lib.check(self.lib.cs_set_memory_limit(self._h, int(nbytes)), self._h, "cs_set_memory_limit")
+
+    def set_wait_test(self, wait_ns: int):
+        """Test hook of the bounded device waits (cs_set_wait_test): with
+        wait_ns > 0 the next searches end in CS_ERR_TIMEOUT after a device wait
+        of that length that nothing completes; 0 turns it off."""
+        _lib.check(self.lib.cs_set_wait_test(self._h, int(wait_ns)), self._h, "cs_set_wait_test")
+
     def set_diagnostics(self, level: int):
         _lib.check(self.lib.cs_set_diagnostics(self._h, int(level)), self._h, "cs_set_diagnostics")
 
@@ -552,6 +565,55 @@ def search(ft, params: SearchParams = None, lofreq=0.1, hifreq=100.0, lobin=100,
     if harm_remove:
         cands = remove_harmonics(cands, numharm, harm_tol)
     return cands
+
+
+def output_path(fftfile: str, outputfilenm: str = "", outdir: str = "", nfiles: int = 1) -> str:
+    """Where one file's candidates go (output_path, src/cli.jl:263-270): a lone
+    file with neither an output name nor an output directory writes to stdout
+    (''); otherwise ``<fftfile without .fft>.cohout``, beside the input or in
+    ``outdir``."""
+    import os
+    if nfiles == 1 and not outdir:
+        return outputfilenm
+    stem = os.path.splitext(fftfile)[0]
+    if outdir:
+        stem = os.path.join(outdir, os.path.basename(stem))
+    return stem + ".cohout"
+
+
+def search_files(fftfiles: Sequence[str], params: SearchParams = None, lofreq=0.1, hifreq=100.0, lobin=100,
+                 blocksize=2048, threshold=None, ncands=100, outputfilenm: str = "", outdir: str = "",
+                 remove=True, dr_tol=1.0, harm_remove=True, numharm=16, harm_tol=1.0, measure=True,
+                 device: int = 0) -> List[List[Candidate]]:
+    """The per-file loop of the reference's command line (src/cli.jl:237-246
+    with search_one, :279-306): each ``.fft`` opened (FFTFile), searched with
+    one shared SearchCache, its strongest ``ncands`` candidates (best metric
+    first) refolded for their duty cycle and written to ``output_path``.  An
+    output name with several files raises ValueError, as the reference's
+    ArgumentError.  Returns each file's reported candidates."""
+    import os
+    from .fileio import FFTFile
+    nfiles = len(fftfiles)
+    if nfiles > 1 and outputfilenm:
+        raise ValueError(f"an output file name names one output but {nfiles} FFT files were given; omit it "
+                         "(each file gets its own .cohout) or give an output directory")
+    if outdir:
+        os.makedirs(outdir, exist_ok=True)
+    params = SearchParams() if params is None else params
+    thr = params.threshold if threshold is None else threshold
+    cache = SearchCache()
+    out = []
+    for path in fftfiles:
+        ft = FFTFile(path)
+        cands = search(ft, params, lofreq=lofreq, hifreq=hifreq, lobin=lobin, blocksize=blocksize, threshold=thr,
+                       remove=remove, dr_tol=dr_tol, harm_remove=harm_remove, numharm=numharm,
+                       harm_tol=harm_tol, cache=cache, device=device)
+        cands = sorted(cands, key=lambda c: -c.metric)[:ncands]
+        if cands and measure:
+            cands = measure_ducy(ft, cands, params, cache=cache, device=device)
+        write_candidates(cands, output_path(path, outputfilenm, outdir, nfiles), thr)
+        out.append(cands)
+    return out
 
 
 def search_batch(fts, params: SearchParams = None, lofreq=0.1, hifreq=100.0, lobin=100, blocksize=2048,

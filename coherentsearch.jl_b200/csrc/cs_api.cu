@@ -312,6 +312,8 @@ struct cs_handle {
     std::vector<float> last_tmetric;
     std::vector<float> last_gate;
     int diag = 0;
+    size_t mem_limit = 0;   // cs_set_memory_limit: device bytes the handle may hold (0: no cap)
+    int64_t stall_ns = 0;   // cs_set_wait_test
     int last_nlev = 0;
     int last_Nprof = 0;
 };
@@ -551,6 +553,25 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             budget = std::min(budget, std::max<size_t>((size_t)512 << 20, (free_b + held) / 2));
         }
     }
+    if (H->mem_limit) {
+        // the cap covers the wave buffers and everything else the handle holds
+        // (spectrum, plan tables, twiddles, batch buffers, block-metric scratch)
+        size_t fixed = 0;
+        const DBuf* held_fixed[] = {&H->amps_owned, &H->d_tcB, &H->d_levels, &H->d_tw, &H->d_counts, &H->d_amax,
+                                    &H->d_bmap, &H->d_batch[0], &H->d_batch[1], &H->d_mst, &H->d_mwin,
+                                    &H->d_mhist, &H->d_muo, &H->d_norm, &H->d_bm_r, &H->d_bm_h, &H->d_bm_st,
+                                    &H->d_bm_prof, &H->d_bm_w, &H->d_bm_sig, &H->d_bm_out};
+        for (const DBuf* b : held_fixed) fixed += b->bytes;
+        for (const auto& e : H->plan_sets)
+            fixed += e->harms.bytes + e->wtab.bytes + e->atab.bytes + e->ctab.bytes;
+        const size_t room = H->mem_limit > fixed + ((size_t)1 << 16) ? H->mem_limit - fixed - ((size_t)1 << 16) : 0;
+        if (room < per_blk)
+            return fail(H, CS_ERR_OUT_OF_MEMORY,
+                        "memory limit " + std::to_string(H->mem_limit) + " B: the handle holds " +
+                            std::to_string(fixed) + " B and one block's working set needs " +
+                            std::to_string(per_blk) + " B more");
+        budget = std::min(budget, room);
+    }
     const int64_t WB = std::max<int64_t>(1, std::min<int64_t>(R.nblocks, (int64_t)(budget / per_blk)));
     if (R.capture) {
         // a captured search runs as one wave on buffers an earlier run sized,
@@ -718,6 +739,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         a.lodr = R.lodr;
         a.T = R.T;
         a.norm_thr = R.threshold_d;
+        a.stall_ns = H->stall_ns;
         if (R.norm) {
             const int nw = H->norm_nwin;
             const double* nd = H->d_norm.as<double>();
@@ -1595,6 +1617,8 @@ cs_status cs_search_stats(const cs_handle* H, cs_stats* out) {
 
 cs_status cs_chunk_metrics(cs_handle* H, double rstart, int64_t n, double* out) {
     if (!H || !out || n < 1 || n > (1 << 16)) return CS_ERR_INVALID_ARGUMENT;
+    // a NaN, infinite or negative start has no bin (floor() of it is undefined as an integer)
+    if (!(rstart >= 0.0 && std::isfinite(rstart))) return fail(H, CS_ERR_INVALID_ARGUMENT, "rstart must be finite and >= 0");
     if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");
     CS_CUDA(cudaSetDevice(H->device), "set device");
     RunSpec R{};
@@ -1705,6 +1729,7 @@ cs_status cs_refold(cs_handle* H, const double* r, const int32_t* nharm, int64_t
 
 cs_status cs_interp_chunk(cs_handle* H, double r_lo, int64_t t0, int64_t n, float* out) {
     if (!H || !out || n < 1 || n > (1 << 16) || t0 < 0) return CS_ERR_INVALID_ARGUMENT;
+    if (!(r_lo >= 0.0 && std::isfinite(r_lo))) return fail(H, CS_ERR_INVALID_ARGUMENT, "r_lo must be finite and >= 0");
     if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");
     CS_CUDA(cudaSetDevice(H->device), "set device");
     RunSpec R{};
@@ -1727,6 +1752,26 @@ cs_status cs_search_block_values(const cs_handle* H, float* sigma, int32_t* nval
     if (cap < n) return CS_ERR_CAPACITY;
     if (sigma) std::copy(H->last_sigma.begin(), H->last_sigma.end(), sigma);
     if (nvalid) std::copy(H->last_nvalid.begin(), H->last_nvalid.end(), nvalid);
+    return CS_OK;
+}
+
+cs_status cs_set_memory_limit(cs_handle* H, int64_t bytes) {
+    if (!H || bytes < 0) return CS_ERR_INVALID_ARGUMENT;
+    CS_CUDA(cudaSetDevice(H->device), "set device");
+    CS_CUDA(cudaStreamSynchronize(H->stream), "drain");
+    H->mem_limit = (size_t)bytes;
+    // the wave buffers come back at the size the cap allows
+    for (DBuf* b : {&H->d_X, &H->d_A, &H->d_samp, &H->d_Q0, &H->d_items, &H->d_cands, &H->d_tmetric, &H->d_sigma,
+                    &H->d_nvalid})
+        b->release();
+    H->graph_valid = false;
+    return CS_OK;
+}
+
+cs_status cs_set_wait_test(cs_handle* H, int64_t wait_ns) {
+    if (!H || wait_ns < 0) return CS_ERR_INVALID_ARGUMENT;
+    H->stall_ns = wait_ns;
+    H->graph_valid = false;   // a captured graph holds the old kernel arguments
     return CS_OK;
 }
 
@@ -1809,6 +1854,8 @@ extern "C" cs_status cs_chunk_metrics_static(const cs_params* params, const floa
     if ((reinterpret_cast<uintptr_t>(d_amps) & 7u) != 0 || (reinterpret_cast<uintptr_t>(d_out) & 3u) != 0)
         return static_fail(err, err_cap, CS_ERR_INVALID_ARGUMENT,
                            "spectrum must be 8-byte and output 4-byte aligned");
+    if (!(rstart >= 0.0 && std::isfinite(rstart)))
+        return static_fail(err, err_cap, CS_ERR_INVALID_ARGUMENT, "rstart must be finite and >= 0");
     const cs_params& p = *params;
 
     // The base fold (k = 1) only, as cs_chunk_metrics evaluates it.
@@ -1891,11 +1938,15 @@ extern "C" cs_status cs_chunk_metrics_static(const cs_params* params, const floa
     uint8_t* base = static_cast<uint8_t*>(g_static_base[dev]);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int32_t nvalid = Nprof;
+    // Every failed step waits for the stream before the lock is released: work
+    // already queued must not run on the shared array under the next caller.
 #define CS_STATIC_CUDA(call, where)                                                                  \
     do {                                                                                             \
         const cudaError_t e_ = (call);                                                               \
-        if (e_ != cudaSuccess)                                                                       \
+        if (e_ != cudaSuccess) {                                                                     \
+            (void)cudaStreamSynchronize(st);                                                         \
             return static_fail(err, err_cap, CS_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e_)); \
+        }                                                                                            \
     } while (0)
     auto put = [&](size_t o, const void* src, size_t bytes) {
         return bytes ? cudaMemcpyAsync(base + o, src, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;

@@ -131,6 +131,9 @@ struct WaveArgs {
     int32_t norm_nwin;
     double norm_thr;            // the threshold, in FP64
     double r_lo, lodr, T;       // band anchor, trial step and observation time (FP64 frequencies)
+    // Test hook (cs_set_wait_test): > 0 makes thread block 0 of k_sigma wait
+    // this many nanoseconds at most on a barrier nothing completes.
+    int64_t stall_ns;
 };
 
 constexpr int kMstFields = 8;   // n, min, median, mean, std, max, sum, sumsq
@@ -204,10 +207,11 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// Bounded wait on an mbarrier phase: gives up after kWaitLimit polls or about
-// one second of wall time, whichever comes first.  The clock is first read
-// after 1024 polls: a wait that ends sooner (nearly every one) reads no timer.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait on an mbarrier phase: gives up after kWaitLimit polls or
+// limit_ns of wall time (about one second by default), whichever comes first.
+// The clock is first read after 1024 polls: a wait that ends sooner (nearly
+// every one) reads no timer.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns = 1000000000ull) {
     uint64_t t0 = 0;
     for (uint32_t it = 0; it < kWaitLimit; ++it) {
         uint32_t done;
@@ -222,7 +226,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         if ((it & 1023u) == 1023u) {
             const uint64_t now = global_ns();
             if (t0 == 0) t0 = now;
-            else if (now - t0 > 1000000000ull) return false;
+            else if (now - t0 > limit_ns) return false;
         }
     }
     return false;

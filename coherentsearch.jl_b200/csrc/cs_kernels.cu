@@ -771,6 +771,7 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
     __shared__ int wtot[32];
     __shared__ uint32_t red[32];
     __shared__ __align__(8) uint64_t sbar;
+    __shared__ __align__(8) uint64_t never;   // test hook: a barrier no thread or copy completes
     const int bl = blockIdx.x;
     const int l = bl % a.nlev;
     const DevLevel& L = a.levels[l];
@@ -794,6 +795,7 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
     // this (block, level)'s kSampStride slot) instead of dependent loads.
     if (threadIdx.x == 0) {
         mbar_init(&sbar, 1);
+        mbar_init(&never, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -814,6 +816,19 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
             a.sigma[bl] = 0.0f;
         }
         return;
+    }
+    // Test hook of the bounded waits: block 0 waits on a barrier whose phase
+    // never completes (no arrival is ever made on it; the sample copy above has
+    // landed), gives up after stall_ns and takes the error exit.
+    if (a.stall_ns > 0 && bl == 0) {
+        const bool done = mbar_wait(&never, 0, (uint64_t)a.stall_ns);
+        if (__syncthreads_or(!done)) {
+            if (threadIdx.x == 0) {
+                atomicExch(err, 3);
+                a.sigma[bl] = 0.0f;
+            }
+            return;
+        }
     }
     // Two columns per thread share each twiddle load (read through L1) when
     // the pairs fit one pass of the CTA; otherwise one column per thread, so

@@ -311,7 +311,8 @@ cs_status cs_search_stats(const cs_handle* h, cs_stats* out);
 
 /* Equivalence bridge `chunk_metrics` (src/search.jl:1740-1755): the exact
  * metric of each of the n trials rstart + j*lodr (one block, global trial 0
- * at rstart, base fold only), written to out[0..n). */
+ * at rstart, base fold only), written to out[0..n).  rstart must be finite
+ * and >= 0, 1 <= n <= 65536 (else CS_ERR_INVALID_ARGUMENT). */
 cs_status cs_chunk_metrics(cs_handle* h, double rstart, int64_t n, double* out);
 
 /* cs_chunk_metrics for callers that may not allocate device memory.  It has
@@ -328,7 +329,8 @@ cs_status cs_chunk_metrics(cs_handle* h, double rstart, int64_t n, double* out);
  * Inputs and output are device memory on the current device: d_amps holds
  * namps complex64 amplitudes of an N-sample series (8-byte aligned), d_out
  * receives the n float32 metrics that cs_chunk_metrics returns as doubles
- * (trials rstart + j*lodr, base fold), 1 <= n <= 65536.  Work runs on
+ * (trials rstart + j*lodr, base fold), 1 <= n <= 65536, rstart finite and
+ * >= 0.  Work runs on
  * `stream` (NULL = legacy default stream) and the call returns once it has
  * finished.  `err` (may be NULL) receives a message of at most err_cap bytes.
  *
@@ -337,7 +339,8 @@ cs_status cs_chunk_metrics(cs_handle* h, double rstart, int64_t n, double* out);
  * All calls on a device share the array and it keeps the last call's
  * contents; the counters are cleared on every call.  Calls whose GPU work
  * overlapped would race on it: the library serialises its own calls per
- * device with a lock and returns only after its work is done. */
+ * device with a lock and returns, on success and on every error after work
+ * was queued, only once that work is done. */
 cs_status cs_chunk_metrics_static(const cs_params* params, const float* d_amps, int64_t namps, int64_t N,
                                   double rstart, int64_t n, float* d_out, void* stream, char* err,
                                   int64_t err_cap);
@@ -392,6 +395,25 @@ cs_status cs_search_gate_values(const cs_handle* h, float* out, int64_t cap, int
 /* Per-trial metrics of the last cs_search run with exact_all = 1:
  * out[(b * nlev + l) * blocksize + j]. */
 cs_status cs_search_trial_metrics(const cs_handle* h, float* out, int64_t cap, int64_t* n_out);
+
+/* Cap on the device memory this handle holds (bytes; 0 = no cap, the
+ * default).  Searches split their blocks into waves that fit under the cap
+ * beside the handle's fixed tables and spectrum; when even one block's
+ * working set does not fit, the search returns CS_ERR_OUT_OF_MEMORY and the
+ * handle stays usable.  Setting the cap releases the wave buffers (and a
+ * captured batch graph), so that later searches reallocate them at the
+ * size the cap allows.  No counterpart in the reference (its workspaces are
+ * sized per thread, src/search.jl:1170-1265). */
+cs_status cs_set_memory_limit(cs_handle* h, int64_t bytes);
+
+/* Test hook of the bounded device waits.  With wait_ns > 0 the next searches
+ * make one thread block of the block-sigma kernel wait, for at most wait_ns
+ * nanoseconds, on a shared-memory barrier that nothing completes (every
+ * other device wait keeps its limit of about one second); the wait gives up,
+ * the kernel ends with an error flag and the search returns CS_ERR_TIMEOUT
+ * with the handle and the CUDA context still usable.  wait_ns = 0 (the
+ * default) turns it off.  No counterpart in the reference. */
+cs_status cs_set_wait_test(cs_handle* h, int64_t wait_ns);
 
 /* Library version string. */
 const char* cs_version(void);

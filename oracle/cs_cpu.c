@@ -251,6 +251,9 @@ typedef struct {
     int64_t total;
     int Nprof;
     int64_t first_block, nblocks;
+    const int64_t* blist;   /* block indices to search (NULL: first_block ..) */
+    double* sig_out;        /* [idx][level] block sigma, or NULL */
+    int32_t* nv_out;        /* [idx][level] valid trials, or NULL */
     double threshold, medcut;
     plan_t* plans;
     int nthreads;
@@ -331,10 +334,14 @@ static void* worker(void* arg) {
     float* psT = (float*)malloc(sizeof(float) * (size_t)CS_BATCH * (2 * maxbins + 2));
     float mb[CS_BATCH], rs[CS_BATCH];
     double tmp[512], ps[1024];
-    for (int64_t c = J->first_block + wa->tid; c < J->first_block + J->nblocks; c += J->nthreads) {
+    for (int64_t idx = wa->tid; idx < J->nblocks; idx += J->nthreads) {
+        int64_t c = J->blist ? J->blist[idx] : J->first_block + idx;
         int64_t i0 = c * (int64_t)Np;
         int n = (int)((J->total - i0) < Np ? (J->total - i0) : Np);
-        if (n <= 0) break;
+        if (n <= 0) {
+            if (J->blist) continue;
+            break;
+        }
         double rstart = J->r_lo + (double)i0 * J->lodr;
         for (int h = 1; h <= nh; ++h) {
             fill_row(&J->plans[h - 1], J->amps, J->namps, J->N, J->hidr, nh, i0, n, row);
@@ -385,6 +392,8 @@ static void* worker(void* arg) {
                 }
             }
             double sg = ns ? 1.4826 * median_d(sig, ns) : 0.0;
+            if (J->sig_out) J->sig_out[idx * J->nlev + l] = sg;
+            if (J->nv_out) J->nv_out[idx * J->nlev + l] = nvalid;
             double invsig = sg > 0 ? 1.0 / sg : 0.0;
             const int* ws = J->widths[l];
             int nw = J->nw[l], wmax = ws[nw - 1];
@@ -479,10 +488,30 @@ static int boxcar_bank(int nbins, double fsp, double maxfrac, int* out) {
  * first).  Writes up to cap candidates (block, k, j, metric) and returns the
  * number found; *seconds = wall time of the call, *rescued = exact rescans.
  * Default boxcar parameters (fsp 1.5, maxfrac 0.3, medmargin 2.0). */
+int64_t csref_search_blocks_ex(const float* amps, int64_t namps, int64_t N, int nharms, int m, double hidr,
+                               const int* decims, int ndecim, double r_lo, int64_t total, int Nprof,
+                               int64_t first_block, int64_t nblocks, const int64_t* blist, double threshold,
+                               int exact_all, int nthreads, cpu_cand_t* cands, int64_t cap, double* seconds,
+                               int64_t* rescued, double* sig_out, int32_t* nv_out);
+
 int64_t csref_search_blocks(const float* amps, int64_t namps, int64_t N, int nharms, int m, double hidr,
                             const int* decims, int ndecim, double r_lo, int64_t total, int Nprof,
                             int64_t first_block, int64_t nblocks, double threshold, int exact_all,
                             int nthreads, cpu_cand_t* cands, int64_t cap, double* seconds, int64_t* rescued) {
+    return csref_search_blocks_ex(amps, namps, N, nharms, m, hidr, decims, ndecim, r_lo, total, Nprof,
+                                  first_block, nblocks, NULL, threshold, exact_all, nthreads, cands, cap, seconds,
+                                  rescued, NULL, NULL);
+}
+
+/* As csref_search_blocks, over the listed blocks blist[0 .. nblocks) when blist
+ * is not NULL, with each searched block's per-level sigma and valid-trial
+ * count (levels in search order) written to sig_out / nv_out
+ * [idx * nlevels + l] when those are not NULL. */
+int64_t csref_search_blocks_ex(const float* amps, int64_t namps, int64_t N, int nharms, int m, double hidr,
+                               const int* decims, int ndecim, double r_lo, int64_t total, int Nprof,
+                               int64_t first_block, int64_t nblocks, const int64_t* blist, double threshold,
+                               int exact_all, int nthreads, cpu_cand_t* cands, int64_t cap, double* seconds,
+                               int64_t* rescued, double* sig_out, int32_t* nv_out) {
     struct timespec t0, t1;
     clock_gettime(CLOCK_MONOTONIC, &t0);
     job_t J;
@@ -490,6 +519,7 @@ int64_t csref_search_blocks(const float* amps, int64_t namps, int64_t N, int nha
     J.amps = amps; J.namps = namps; J.N = N; J.nharms = nharms; J.m = m; J.hidr = hidr;
     J.lodr = hidr / (double)nharms; J.r_lo = r_lo; J.total = total; J.Nprof = Nprof;
     J.first_block = first_block; J.nblocks = nblocks; J.threshold = threshold;
+    J.blist = blist; J.sig_out = sig_out; J.nv_out = nv_out;
     J.medcut = exact_all ? -INFINITY : threshold - 2.0;
     J.nthreads = nthreads < 1 ? 1 : nthreads;
     J.cands = cands; J.cap = cap;

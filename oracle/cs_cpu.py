@@ -28,6 +28,13 @@ def load():
             ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int64, ctypes.c_int, ctypes.c_int64,
             ctypes.c_int64, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
+        lib.csref_search_blocks_ex.restype = ctypes.c_int64
+        lib.csref_search_blocks_ex.argtypes = [
+            ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+            ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int64, ctypes.c_int, ctypes.c_int64,
+            ctypes.c_int64, ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+            ctypes.c_int64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p,
+            ctypes.c_void_p]
         _lib = lib
     return _lib
 
@@ -76,3 +83,36 @@ def search_blocks(amps, N, dt, nharms, m, hidr, decimations, r_lo, total, blocks
     trials = max(0, min(total, (first_block + nblk_real) * blocksize) - first_block * blocksize)
     return {"cands": out[:min(n, cap)], "ncand": int(n), "seconds": sec.value, "rescued": resc.value,
             "threads": int(nthreads), "blocks": int(nblk_real), "trials": int(trials)}
+
+
+def search_blocks_ex(amps, N, dt, nharms, m, hidr, decimations, r_lo, total, blocksize, threshold, nthreads,
+                     blocks=None, first_block=0, nblocks=None, exact_all=False, cap=1 << 22):
+    """search_blocks over a block range, or over the listed `blocks` (global
+    block indices of the band's grid), also returning each searched block's
+    per-level sigma and valid-trial count: arrays [len(blocks), nlevels],
+    levels in search order (k = 1 first, then the other factors as given)."""
+    lib = load()
+    a = np.ascontiguousarray(amps, dtype=np.complex64)
+    dec = np.ascontiguousarray(decimations, dtype=np.int32)
+    nlev = 1 + sum(1 for k in decimations if k > 1)
+    if blocks is not None:
+        bl = np.ascontiguousarray(blocks, dtype=np.int64)
+        nb = len(bl)
+        bptr = bl.ctypes.data
+    else:
+        nb = -(-total // blocksize) - first_block if nblocks is None else nblocks
+        bl, bptr = None, None
+    out = np.zeros(cap, CAND_DTYPE)
+    sig = np.zeros((max(nb, 1), nlev), np.float64)
+    nv = np.zeros((max(nb, 1), nlev), np.int32)
+    sec = ctypes.c_double()
+    resc = ctypes.c_int64()
+    n = lib.csref_search_blocks_ex(a.ctypes.data, len(a), int(N), int(nharms), int(m), float(hidr),
+                                   dec.ctypes.data, len(dec), float(r_lo), int(total), int(blocksize),
+                                   int(first_block), int(nb), bptr, float(threshold), int(bool(exact_all)),
+                                   int(nthreads), out.ctypes.data, cap, ctypes.byref(sec), ctypes.byref(resc),
+                                   sig.ctypes.data, nv.ctypes.data)
+    if n > cap:
+        raise RuntimeError(f"{n} candidates exceed the oracle's capacity {cap}")
+    return {"cands": out[:n], "ncand": int(n), "seconds": sec.value, "rescued": resc.value,
+            "sigma": sig[:nb], "nvalid": nv[:nb], "threads": int(nthreads)}

@@ -13,14 +13,17 @@ oracle and the device path can be checked against exactly those numbers:
   test/test_search.jl:113-150.
 
 Run once in a checkout that has the reference tree; the JSON it writes is the
-committed fixture.  Usage: ``python make_reference_kats.py [reference_root]``.
+committed fixture.  Usage: ``python make_reference_kats.py <reference_root>``,
+the root of a CoherentSearch.jl checkout (the directory holding ``test/``).
 """
 import json
 import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python make_reference_kats.py <reference_root>")
+REF = sys.argv[1]
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_kats.json")
 
 

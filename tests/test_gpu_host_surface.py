@@ -1,0 +1,102 @@
+"""The drop-in host surface over the device engine, as the reference tests it:
+PRESTO files searched from disk, SearchCache reuse, the multi-file .cohout
+output, and a truncated spectrum against the oracle.
+
+  * SearchCache reuse (test/test_cli.jl:65-85): fresh, cached, reused and
+    reopened-file runs give the same candidates bit for bit;
+  * multi-file run (test/test_cli.jl:179-221): one .cohout per input, each with
+    its own candidates and a measured duty cycle in every row;
+  * a .fft holding fewer than N/2 amplitudes: the range guard uses the file's
+    end (src/directinterp.jl:490-496), checked against the C port of the
+    reference search (same tolerances as test_gpu_configs).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import cohsearch as cs
+from oracle import cs_cpu
+from tests.test_fileio_host import _synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _write(tmp_path, name, bin0=210, N=1 << 15, dt=1.0e-4):
+    return cs.write_fft(str(tmp_path / name), _synthetic(N, bin0), N, dt), N * dt
+
+
+def test_search_cache_reuse_leaves_results_unchanged(tmp_path):
+    path, T = _write(tmp_path, "synth")
+    ft = cs.FFTFile(path)
+    params = cs.SearchParams(nharms=8)
+    kw = dict(lofreq=200 / T, hifreq=240 / T, blocksize=64, threshold=0.0)
+    fresh = cs.search(ft, params, **kw)
+    assert fresh
+    cache = cs.SearchCache()
+    first = cs.search(ft, params, cache=cache, **kw)
+    eng = cache.engine
+    second = cs.search(ft, params, cache=cache, **kw)      # the reuse path
+    assert cache.engine is eng
+    for got in (first, second):
+        assert len(got) == len(fresh)
+        assert all(c.r == f.r and c.metric == f.metric and c.nharm == f.nharm for c, f in zip(got, fresh))
+    reopened = cs.search(cs.FFTFile(path), params, cache=cache, **kw)
+    assert [c.metric for c in reopened] == [c.metric for c in fresh]
+    # other params rebuild the engine (reuse is keyed on the params object)
+    cs.search(ft, cs.SearchParams(nharms=8, hidr=0.25), cache=cache, **kw)
+    assert cache.engine is not eng
+
+
+def test_multi_file_run_writes_one_cohout_per_input(tmp_path):
+    p1, T = _write(tmp_path, "obs_DM10.0")
+    p2, _ = _write(tmp_path, "obs_DM20.0", bin0=214)
+    res = cs.search_files([p1, p2], cs.SearchParams(nharms=8), lofreq=200 / T, hifreq=240 / T, blocksize=64,
+                          threshold=0.0, ncands=3)
+    o1, o2 = str(tmp_path / "obs_DM10.0.cohout"), str(tmp_path / "obs_DM20.0.cohout")
+    assert os.path.isfile(o1) and os.path.isfile(o2)
+    l1, l2 = open(o1).read().splitlines(), open(o2).read().splitlines()
+    assert len(l1) > 1 and len(l2) > 1 and len(l1) <= 4
+    assert l1[0].startswith("#") and "Ducy(%)" in l1[0]
+    f1, f2 = float(l1[1].split()[2]), float(l2[1].split()[2])
+    assert not np.isclose(f1, f2, rtol=1e-3)
+    for line in l1[1:] + l2[1:]:
+        f = line.split()
+        assert len(f) == 6
+        assert 0 < float(f[5]) <= 30.0
+    # the rows are the returned candidates, strongest first
+    assert [c.metric for c in res[0]] == sorted((c.metric for c in res[0]), reverse=True)
+    # an output directory relocates them
+    od = str(tmp_path / "sub" / "dir")
+    cs.search_files([p1], cs.SearchParams(nharms=8), lofreq=200 / T, hifreq=240 / T, blocksize=64,
+                    threshold=0.0, ncands=3, outdir=od)
+    assert os.path.isfile(os.path.join(od, "obs_DM10.0.cohout"))
+
+
+def test_truncated_spectrum_vs_port(tmp_path):
+    """A spectrum cut at 60 % of N/2: harmonics whose window passes the file's
+    end are guarded off, for the device and the port alike."""
+    from cohsearch import synth
+    from tests.test_gpu_configs import BLOCK, THR, check_against_port
+    N, dt = 1 << 21, 64e-6
+    full = synth.make_spectrum(N, dt, [synth.Pulsar(21.3, 0.05, 30.0, 0.4), synth.Pulsar(150.7, 0.1, 25.0, 0.1)], 77)
+    namps = int(0.6 * (N // 2))
+    path = cs.write_fft(str(tmp_path / "cut"), full[:namps], N, dt)
+    ft = cs.FFTFile(path)
+    assert len(ft.amps) == namps
+    dec = cs.decimation_set(32, 4)
+    eng = cs.Engine(cs.SearchParams(nharms=32, m=16, decimations=dec, threshold=THR))
+    eng.set_diagnostics(1)
+    eng.set_spectrum(ft)
+    lo, hi = 5.0, 200.0
+    dev = eng.search_raw(lo, hi, 100, BLOCK, THR)
+    sig, nv = eng.block_values()
+    from tests.test_gpu_configs import _band
+    _, _, r_lo, total = _band(N, dt, 32, lo, hi)
+    port = cs_cpu.search_blocks_ex(np.asarray(ft.amps), N, dt, 32, 16, 0.5, dec, r_lo, total, BLOCK, THR,
+                                   os.cpu_count() or 1)
+    matched, _ = check_against_port(dev, sig, nv, port, N, dt, 32, lo, hi, len(dec))
+    assert matched > 0
+    # the 150.7 Hz pulsar's upper harmonics lie past the cut: the row guard
+    # zeroes them, yet the fundamental is still found
+    assert np.any(np.abs(dev["freq"] - 150.7) < 0.05)

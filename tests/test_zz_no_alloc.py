@@ -67,6 +67,34 @@ def test_static_matches_chunk_metrics_two_calls():
         assert np.all(np.abs(got - want) <= SNR_RTOL * np.maximum(np.abs(want), 1.0))
 
 
+def test_static_call_allocates_no_device_memory():
+    """After a first call (which looks up the array's address), a second call
+    leaves the device's free memory exactly as it was: no cudaMalloc, no
+    allocating library routine on the path."""
+    import torch
+    import cohsearch as cs
+    amps, N, dt = pulsar_spectrum()
+    d_amps = _device_spectrum(amps)
+    params = cs.SearchParams(nharms=60, m=16)
+    cp = params.to_c()
+    out = torch.empty(2048, dtype=torch.float32, device="cuda")
+    err = ctypes.create_string_buffer(512)
+    lib = _lib()
+
+    def call():
+        return lib.cs_chunk_metrics_static(ctypes.byref(cp), d_amps.data_ptr(), len(amps), int(N), 5000.0, 2048,
+                                           out.data_ptr(), torch.cuda.current_stream().cuda_stream, err, len(err))
+
+    assert call() == 0, err.value.decode()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    assert call() == 0, err.value.decode()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert np.all(np.isfinite(out.cpu().numpy()))
+
+
 def test_static_rejects_oversize_requests():
     import cohsearch as cs
     amps, N, dt = pulsar_spectrum()
@@ -78,6 +106,10 @@ def test_static_rejects_oversize_requests():
     assert st == CS_ERR_CAPACITY and "scratch" in msg
     st, _, msg = _static(cs.SearchParams(nharms=32, m=32), d_amps, len(amps), N, 5000.0, (1 << 16) + 1)
     assert st == CS_ERR_INVALID_ARGUMENT
+    # a start with no bin: NaN, infinite or negative
+    for bad in (float("nan"), float("inf"), -1.0):
+        st, _, msg = _static(cs.SearchParams(nharms=32, m=32), d_amps, len(amps), N, bad, 256)
+        assert st == CS_ERR_INVALID_ARGUMENT and "rstart" in msg
     # the array is still usable after a rejected call
     st, got, msg = _static(cs.SearchParams(nharms=32, m=32), d_amps, len(amps), N, 10010.0, 256)
     assert st == 0, msg

@@ -516,6 +516,12 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
     const int win_max = (int)std::ceil((double)(Nprof - 1 + 64) * p.hidr) + p.m + 4;
     if (interp_smem(win_max, Nprof) > 200 * 1024)
         return fail(H, CS_ERR_UNSUPPORTED, "blocksize too large for the shared-memory interpolation row");
+    // the persistent interpolation kernel: 16 taps, every phase cycle 1..256,
+    // two CTAs' staging within an SM's shared memory, 8-byte aligned bins for
+    // its window copies
+    bool interp2 = p.m == 16 && interp2_smem(win_max, Nprof) <= 112 * 1024 &&
+                   (reinterpret_cast<uintptr_t>(H->amps) & 7u) == 0;
+    for (const DevHarm& d : ps->host.harms) interp2 = interp2 && d.P >= 1 && d.P <= 256;
     int maxbins = 0, maxwmax = 0;
     for (int l = 0; l < R.nlev; ++l) {
         maxbins = std::max(maxbins, H->dlev[l].nbins);
@@ -807,7 +813,10 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             a.nvalid = H->d_nvalid.as<int32_t>();
         }
         if (!R.capture) CS_CUDA(cudaEventRecord(H->ev[0], H->stream), "event");
-        CS_CUDA(launch_interp(a, H->stream, win_max, d_err), "interp launch");
+        if (interp2)
+            CS_CUDA(launch_interp2(a, H->stream, win_max, d_err, H->num_sms), "interp launch");
+        else
+            CS_CUDA(launch_interp(a, H->stream, win_max, d_err), "interp launch");
         if (!R.capture) CS_CUDA(cudaEventRecord(H->ev[1], H->stream), "event");
         S.launches += 1;
         if (!R.interp_only) {
@@ -850,6 +859,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         if (counts[2] == 1) return fail(H, CS_ERR_CUDA, "interpolation window exceeded its bound");
         if (counts[2] == 2) return fail(H, CS_ERR_TIMEOUT, "tensor-core completion wait ran out");
         if (counts[2] == 3) return fail(H, CS_ERR_TIMEOUT, "sigma sample copy wait ran out");
+        if (counts[2] == 4) return fail(H, CS_ERR_TIMEOUT, "interpolation window copy wait ran out");
         float ms = 0.0f;
         CS_CUDA(cudaEventElapsedTime(&ms, H->ev[0], H->ev[1]), "timing");
         S.ms_interp += ms;

@@ -19,6 +19,8 @@ constexpr int kTileTrials = 64;    // trials per CTA in the FP32 synthesis kerne
 constexpr int kATileBytes = 128 * 128 * 2;  // one 16-bit A tile: 128 trials x 128 K
 constexpr int kSampStride = kSigmaCap / 2;  // float2 per (block, level) in `samp`
 constexpr int kSigmaThreads = 384;          // k_sigma CTA: one pass over a level's synthesis tasks
+constexpr int kSigmaKeyShift = 19;          // k_sigma median buckets: the top 12 bits of |x| (sign bit 0)
+constexpr int kSigmaBins = 1 << (31 - kSigmaKeyShift);
 
 // One harmonic's rational trial-grid recipe (DirectPlan, src/directinterp.jl:179-204).
 // Global trial t of the search evaluates harmonic h at Fourier frequency
@@ -150,26 +152,42 @@ struct TcLevel {
 };
 
 // One epilogue work unit: the boxcar starts [p0, p0+nstart) of one level,
-// scanned from TMEM column col (= level col + p0) over pw columns.
+// scanned over pw columns from TMEM column col on even tiles, col1 on odd
+// ones (they differ for the double-buffered base level).
 struct TcUnit {
     int16_t lev;
     int16_t wg;        // epilogue warpgroup (0..3)
     int16_t nstart;
     int16_t pw;
     int16_t col;
+    int16_t col1;
+    int16_t phase;     // 0: scanned first (decimated levels); 1: after the next tile's product is issued
     int16_t pad;
 };
 
+// One tcgen05.mma column range: B columns [bcol, bcol + n) into TMEM columns
+// from tcol (even tiles) or tcol1 (odd tiles).
+struct TcMma {
+    int16_t bcol;
+    int16_t n;
+    int16_t tcol;
+    int16_t tcol1;
+};
+
 constexpr int kMaxUnits = 32;
+constexpr int kMaxMma = 8;
 
 struct TcArgs {
     TcLevel lev[kMaxLevels];
     TcUnit unit[kMaxUnits];
+    TcMma mma[kMaxMma];
     int32_t nunit;
+    int32_t nmma;
     int32_t nlev;
     int32_t hm;            // prefix-sum ring size: 8 or 32 (>= widest boxcar)
-    int32_t ncols_total;   // columns of the product (multiple of 16)
-    int32_t n1;            // N of the first MMA (<= 256); the rest is the second
+    int32_t ncols_total;   // B columns of the product (multiple of 16)
+    int32_t dbuf;          // 1: the base level has two TMEM slots, so the next tile's product
+                           // runs while this tile's base level is scanned
     int32_t fp16;          // operand format: 1 = FP16, 0 = BF16
     int32_t split;         // A tiles per 128 trials: 1, or 2 (hi and lo: K runs over both)
 };
@@ -321,6 +339,9 @@ __device__ __forceinline__ void gate_flag(const WaveArgs& a, int blk, int l, int
 #endif  // __CUDACC__
 
 cudaError_t launch_interp(const WaveArgs& a, cudaStream_t st, int win_max, int* err);
+// Persistent interpolation for m = 16 and phase cycles 1 <= P <= 256 (same values as launch_interp).
+cudaError_t launch_interp2(const WaveArgs& a, cudaStream_t st, int win_max, int* err, int num_sms);
+size_t interp2_smem(int win_max, int Nprof);
 cudaError_t launch_synth_fp32(const WaveArgs& a, cudaStream_t st, int smem_bytes);
 size_t sigma_smem(int max_hk, int max_np);
 size_t interp_smem(int win_max, int Nprof);

@@ -19,6 +19,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <math.h>
+
+#include <algorithm>
 #include <math_constants.h>
 
 namespace cs {
@@ -455,6 +457,186 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
     emit_rows(a, xo, Nst, blk, hidx0, ng, n);
 }
 
+// ---------------------------------------------------------------------------
+// Persistent form of k_interp for the common case (m = 16, rational trial
+// grid, every phase cycle P <= 256).  Two CTAs per SM walk the work items
+// (block, group of 4 harmonics), group fastest.  An item's four bin windows
+// arrive by bulk copy (cp.async.bulk, 16-byte aligned body; the odd first and
+// last bins by plain loads) into a staging buffer, issued by warp 0 as soon as
+// the previous item's taps are done, so the copy runs under that item's
+// emission of A tiles and sigma samples.  Two barriers per item: after the
+// taps (the staging buffer and the staged rows are complete) and after the
+// emission (the rows are free, the next windows have landed).  The tap
+// arithmetic is k_interp's, bit for bit.
+// ---------------------------------------------------------------------------
+constexpr int kI2Threads = 256;
+
+struct HarmStage {
+    int ok;             // 1: computed; 0: zero row
+    int head;           // window element 0 sits at stage + head (1 when its address is not 16-byte aligned)
+    int p0, res0, Ub, Tc, chunk, small, Hs;
+    long long base;     // rfloor0 + qint0 - lo + 1 - m2
+};
+
+__device__ __forceinline__ int i2_wstride(int win_max) { return (win_max + 3) & ~1; }
+
+// Warp 0: the per-harmonic state of `item` into st[], its windows' plain-loaded
+// edge bins, and the bulk copies of their bodies, completing on *bar.
+__device__ void i2_prepare(const WaveArgs& a, int item, int ngroups, int win_max, float2* stage, HarmStage* st,
+                           uint64_t* bar, int* err) {
+    const int lane = threadIdx.x & 31;
+    const int blk = item / ngroups, grp = item - blk * ngroups;
+    const int hidx0 = grp * kHG;
+    const int ng = min(kHG, a.nharms - hidx0);
+    const int64_t t0 = blk_t0(a, blk);
+    const int n = (int)min((int64_t)a.Nprof, a.total - t0);
+    const int m2 = 8;
+    const int wstride = i2_wstride(win_max);
+    uint32_t body_bytes = 0;
+    int head = 0, body = 0, tail = 0;
+    int64_t lo = 0;
+    if (lane < ng) {
+        const DevHarm hp = a.harms[hidx0 + lane];
+        const uint8_t* ct = a.ctab + hp.a_off;
+        const int64_t hpn = (int64_t)hp.h * hp.pnum;
+        const int64_t T0 = t0 * hpn;
+        const int64_t qint0 = T0 / hp.q;
+        const int p0 = (int)(t0 % hp.P);
+        const int64_t tl = t0 + n - 1;
+        const int64_t qintl = (tl * hpn) / hp.q;
+        const int pl = (int)(tl % hp.P);
+        const int64_t fl0 = hp.rfloor0 + qint0 + ct[p0];
+        const int64_t fll = hp.rfloor0 + qintl + ct[pl];
+        // range guard on the TRUE trial range (src/directinterp.jl:490-496)
+        const bool ok = (fl0 + 2 - m2 >= 1) && (fll + 1 + m2 <= a.namps) && (hp.rfloor0 + qintl < a.Nhalf) && n > 0;
+        lo = fl0 + 1 - m2;
+        const int64_t nw = fll + m2 - lo + 1;
+        HarmStage h{};
+        h.ok = ok && nw <= win_max ? 1 : 0;
+        if (ok && nw > win_max) atomicExch(err, 1);
+        if (h.ok) {
+            head = (reinterpret_cast<uintptr_t>(a.amps + lo) & 15u) ? 1 : 0;
+            body = ((int)nw - head) & ~1;
+            tail = (int)nw - head - body;
+            body_bytes = (uint32_t)body * 8u;
+        }
+        h.head = head;
+        h.p0 = p0;
+        h.res0 = (int)(T0 % hp.q);
+        h.base = hp.rfloor0 + qint0 - lo + 1 - m2;
+        const int P = hp.P;
+        const int Tc = P >= kI2Threads ? 1 : kI2Threads / P;
+        const int Ub = n / P;                       // classes jc < n - Ub*P get Ub+1 trials
+        h.Ub = Ub;
+        h.Tc = Tc;
+        h.chunk = (Ub + 1 + Tc - 1) / Tc;
+        h.small = ((uint64_t)hp.q + (uint64_t)P * (uint64_t)hpn) < 0xFFFFFFFFull;
+        h.Hs = (int)(((int64_t)P * hpn) / hp.q);   // bins between trials t and t+P
+        st[lane] = h;
+    }
+    uint32_t total = body_bytes;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+    if (lane == 0) mbar_expect_tx(bar, total);   // the one arrival of the phase, with every copy's bytes
+    __syncwarp();
+    if (lane < ng && (head | body | tail)) {
+        float2* win = stage + lane * wstride + head;
+        const float2* src = a.amps + lo;
+        if (head) win[0] = src[0];
+        if (tail) win[head + body] = src[head + body];
+        if (body) bulk_copy(smem_u32(win + head), src + head, (uint32_t)body * 8u, bar);
+    }
+}
+
+__global__ void __launch_bounds__(kI2Threads, 2) k_interp2(WaveArgs a, int win_max, int Nst, int nitems, int* err) {
+    extern __shared__ __align__(16) float2 sm_i2[];
+    float2* xo = sm_i2;                                  // [kHG][Nst] staged rows
+    float2* stage = sm_i2 + kHG * Nst;                   // [kHG][wstride] bin windows
+    const int wstride = i2_wstride(win_max);
+    __shared__ HarmStage st[2][kHG];
+    __shared__ __align__(8) uint64_t wbar;
+    const int ngroups = (a.nharms + kHG - 1) / kHG;
+    const int warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        mbar_init(&wbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    int item = blockIdx.x;
+    uint32_t pend = 0;   // parity of the latest phase copies were issued on
+    if (item < nitems && warp == 0) i2_prepare(a, item, ngroups, win_max, stage, st[0], &wbar, err);
+    bool ok = __syncthreads_or(item < nitems && !mbar_wait(&wbar, 0)) == 0;
+    if (!ok && threadIdx.x == 0) atomicExch(err, 4);
+    for (int it = 0; item < nitems && ok; item += gridDim.x, ++it) {
+        const HarmStage* S = st[it & 1];
+        const int blk = item / ngroups, grp = item - blk * ngroups;
+        const int hidx0 = grp * kHG;
+        const int ng = min(kHG, a.nharms - hidx0);
+        const int64_t t0 = blk_t0(a, blk);
+        const int n = (int)min((int64_t)a.Nprof, a.total - t0);
+        for (int g = 0; g < ng; ++g) {
+            float2* xg = xo + g * Nst;
+            const HarmStage h = S[g];
+            if (h.ok != 1) {
+                for (int j = threadIdx.x; j < n; j += blockDim.x) xg[j] = make_float2(0.0f, 0.0f);
+                continue;
+            }
+            const DevHarm& hp = a.harms[hidx0 + g];
+            const float* __restrict__ wt = a.wtab + hp.w_off;
+            const float2* __restrict__ at = a.atab + hp.a_off;
+            const uint8_t* __restrict__ ct = a.ctab + hp.a_off;
+            const float2* __restrict__ win = stage + g * wstride + h.head;
+            const int64_t hpn = (int64_t)hp.h * hp.pnum;
+            const int P = hp.P, q = hp.q, Hs = h.Hs;
+            const int Tc = h.Tc, Ub = h.Ub, chunk = h.chunk;
+            const int ntask = P >= kI2Threads ? P : P * Tc;
+            const int nlong = n - Ub * P;
+            const float invP = 1.0f / (float)P;
+            for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
+                // task < 256 when Tc > 1: (task + 0.5)/P is >= 0.5/P from an integer,
+                // far above the float error, so the quotient is exact.
+                const int part = Tc > 1 ? (int)(((float)task + 0.5f) * invP) : 0;
+                const int jc = task - part * P;
+                if (jc >= n) continue;
+                const int U = Ub + (jc < nlong ? 1 : 0);
+                const int u0 = part * chunk, u1 = min(U, u0 + chunk);
+                if (u0 >= u1) continue;
+                int p = h.p0 + jc;
+                if (p >= P) p -= P;
+                const int64_t qv = h.small ? (int64_t)(((uint32_t)h.res0 + (uint32_t)jc * (uint32_t)hpn) / (uint32_t)q)
+                                           : ((int64_t)h.res0 + (int64_t)jc * hpn) / q;
+                const int b0 = (int)(h.base + qv + ct[p]);
+                const float2 A = __ldg(at + p);
+                if (u1 - u0 >= 2 && slide_dispatch(Hs, wt, P, p, A, win, b0, jc, u0, u1, xg)) continue;
+                class_run<16>(wt, P, p, A, win, b0, Hs, jc, u0, u1, xg, 16);
+            }
+        }
+        __syncthreads();   // taps done: the staging buffer is free, the rows complete
+        const int nxt = item + (int)gridDim.x;
+        if (nxt < nitems && warp == 0) i2_prepare(a, nxt, ngroups, win_max, stage, st[(it + 1) & 1], &wbar, err);
+        if (nxt < nitems) pend = (uint32_t)((it + 1) & 1);
+        emit_rows(a, xo, Nst, blk, hidx0, ng, n);
+        // rows emitted; the next item's windows have landed (bounded wait)
+        ok = __syncthreads_or(nxt < nitems && !mbar_wait(&wbar, (uint32_t)((it + 1) & 1))) == 0;
+        if (!ok && threadIdx.x == 0) atomicExch(err, 4);
+    }
+    if (!ok && threadIdx.x == 0) mbar_wait(&wbar, pend);   // bounded: lets a late copy land before exit
+}
+
+size_t interp2_smem(int win_max, int Nprof) {
+    return (size_t)(kHG * Nprof + kHG * ((win_max + 3) & ~1)) * sizeof(float2);
+}
+
+cudaError_t launch_interp2(const WaveArgs& a, cudaStream_t st, int win_max, int* err, int num_sms) {
+    const int ngroups = (a.nharms + kHG - 1) / kHG;
+    const int nitems = ngroups * a.nblk;
+    const size_t smem = interp2_smem(win_max, a.Nprof);
+    cudaFuncSetAttribute(k_interp2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int grid = std::min(nitems, 2 * num_sms);
+    k_interp2<<<grid, kI2Threads, smem, st>>>(a, win_max, a.Nprof, nitems, err);
+    return cudaGetLastError();
+}
+
 // The largest |Re| or |Im| of a spectrum (NaN ignored), for the FP16 A-tile
 // scale: grid-stride maximum, warp reduction, one atomicMax on the float bits
 // (non-negative floats order like their bits) per warp.
@@ -759,6 +941,63 @@ __device__ uint32_t radix_select(const uint32_t* vals, int ns, int kth, uint32_t
     return prefix;
 }
 
+// k-th smallest (0-based, k < n) of n values given as bit patterns, by one
+// warp: radix passes of at most 11 bits over bits top..0, in a histogram of
+// 2048 bins that belongs to the warp.  prefix/mask: bits every value is known
+// to share (above `top`).
+__device__ uint32_t warp_select(const uint32_t* vals, int n, int kth, uint32_t* hist, uint32_t prefix, uint32_t mask,
+                                int top) {
+    const int lane = threadIdx.x & 31;
+    int kk = kth;
+    for (int hi = top; hi >= 0;) {
+        const int nbits = hi + 1 < 11 ? hi + 1 : 11;
+        const int shift = hi + 1 - nbits;
+        const int nb = 1 << nbits;
+        for (int i = lane; i < nb; i += 32) hist[i] = 0;
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) {
+            const uint32_t v = vals[i];
+            if ((v & mask) == prefix) atomicAdd(&hist[(v >> shift) & (uint32_t)(nb - 1)], 1u);
+        }
+        __syncwarp();
+        // each lane sums a run of ceil(nb/32) bins; a warp scan locates rank kk
+        const int per = (nb + 31) / 32;
+        const int b0 = min(nb, lane * per), b1 = min(nb, b0 + per);
+        int local = 0;
+        for (int b = b0; b < b1; ++b) local += (int)hist[b];
+        int incl = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int excl = incl - local;
+        const unsigned who = __ballot_sync(0xffffffffu, excl <= kk && kk < incl);
+        const int src = who ? __ffs(who) - 1 : 0;
+        int bsel = 0, knew = 0;
+        if (lane == src && who) {
+            int c = excl;
+            for (int b = b0; b < b1; ++b) {
+                const int hb = (int)hist[b];
+                if (c + hb > kk) {
+                    bsel = b;
+                    knew = kk - c;
+                    break;
+                }
+                c += hb;
+            }
+        }
+        bsel = __shfl_sync(0xffffffffu, bsel, src);
+        knew = __shfl_sync(0xffffffffu, knew, src);
+        prefix |= (uint32_t)bsel << shift;
+        mask |= (uint32_t)(nb - 1) << shift;
+        kk = knew;
+        hi = shift - 1;
+        __syncwarp();
+    }
+    return prefix;
+}
+
 // One CTA per (block, level).  The columns _block_sigma pools
 // (src/search.jl:528-537): every valid column when nbins*nv <= 8192, else ncol
 // whole columns spaced evenly.  k_interp leaves their exact FP32 amplitudes in
@@ -785,9 +1024,10 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
     const int ncs = all ? nv : min(nv, max(1, kSigmaCap / nbins));
     const int ns = ncs * nbins;
     float2* Xs = reinterpret_cast<float2*>(ss4);                    // [Hk][ncs], <= kSampStride
-    uint32_t* hist = reinterpret_cast<uint32_t*>(ss4);              // reuses Xs once profiles exist
+    uint32_t* lst = reinterpret_cast<uint32_t*>(ss4);               // reuses Xs once profiles exist
     uint32_t* vals = reinterpret_cast<uint32_t*>(Xs + kSampStride);  // [ns]
-    float* tws = reinterpret_cast<float*>(vals + kSigmaCap);        // the level's C2 then S2 rows
+    uint32_t* hist = vals + kSigmaCap;                              // [kSigmaBins]
+    float* tws = reinterpret_cast<float*>(hist + kSigmaBins);       // the level's C2 then S2 rows
     const float* C2 = tws;
     const float* S2 = tws + Hk * np;
     const float2* samp = a.samp + (int64_t)bl * kSampStride;
@@ -798,6 +1038,7 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
         mbar_init(&never, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    for (int i = threadIdx.x; i < kSigmaBins; i += blockDim.x) hist[i] = 0;
     __syncthreads();
     if (threadIdx.x == 0) {
         // the level's twiddle rows come along (2*Hk*np floats, a multiple of 64 bytes)
@@ -871,42 +1112,95 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
         }
     }
     __syncthreads();
+    // The exact median (_median!, src/search.jl:295-305: the central value, or
+    // the mean of the two central ones).  |x| >= 0 orders like its bit
+    // pattern.  One pass counts the values per bucket of their top 12 bits
+    // (exponent and 4 mantissa bits; warp-aggregated shared atomics), a scan
+    // finds the buckets of the central ranks, their values are gathered into
+    // a short list, and one warp selects within it.
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int half = ns >> 1;
-    float med;
-    if (ns & 1) {
-        med = __uint_as_float(radix_select(vals, ns, half, hist, sh, wtot));
-    } else {
-        // _median! (src/search.jl:295-305): mean of the two central order statistics.
-        const uint32_t lo = radix_select(vals, ns, half - 1, hist, sh, wtot);
+    const int r0 = (ns & 1) ? half : half - 1;   // the lower central rank; half is the upper
+    // (whole warps run every round of these two loops: the warp intrinsics
+    // see all 32 lanes; blockDim.x is a multiple of 32)
+    for (int i0 = 0; i0 < ns; i0 += blockDim.x) {
+        const int i = i0 + (int)threadIdx.x;
+        const uint32_t key = i < ns ? vals[i] >> kSigmaKeyShift : 0xFFFFFFFFu;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        if (i < ns && lane == __ffs(peers) - 1) atomicAdd(&hist[key], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    {
+        const int per = (kSigmaBins + (int)blockDim.x - 1) / (int)blockDim.x;
+        const int b0 = min(kSigmaBins, (int)threadIdx.x * per), b1 = min(kSigmaBins, b0 + per);
+        int local = 0;
+        for (int b = b0; b < b1; ++b) local += (int)hist[b];
+        const int excl = block_excl_scan(local, wtot, sh + 2);
+        // sh[0] / sh[1]: buckets of ranks r0 / half; red[0]: values below bucket sh[0]
+        for (int q = 0; q < 2; ++q) {
+            const int r = q ? half : r0;
+            if (excl <= r && r < excl + local) {
+                int c = excl;
+                for (int b = b0; b < b1; ++b) {
+                    const int hb = (int)hist[b];
+                    if (c + hb > r) {
+                        sh[q] = b;
+                        if (q == 0) red[0] = (uint32_t)c;
+                        break;
+                    }
+                    c += hb;
+                }
+            }
+        }
+        if (threadIdx.x == 0) red[1] = 0;   // list length
+    }
+    __syncthreads();
+    const uint32_t blo = (uint32_t)sh[0], bhi = (uint32_t)sh[1];
+    for (int i0 = 0; i0 < ns; i0 += blockDim.x) {
+        const int i = i0 + (int)threadIdx.x;
+        const uint32_t v = i < ns ? vals[i] : 0xFFFFFFFFu;
+        const uint32_t key = v >> kSigmaKeyShift;
+        const bool in = i < ns && key >= blo && key <= bhi;
+        const unsigned bal = __ballot_sync(0xffffffffu, in);
+        if (bal) {   // warp-uniform
+            const int leader = __ffs(bal) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(&red[1], (uint32_t)__popc(bal));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (in) lst[base + __popc(bal & ((1u << lane) - 1u))] = v;
+        }
+    }
+    __syncthreads();
+    if (wid != 0) return;
+    const int nl = (int)red[1];
+    const int below = (int)red[0];
+    // one bucket: the list shares bits 31..19 and the select runs over 18..0
+    const bool one = blo == bhi;
+    const uint32_t lo = warp_select(lst, nl, r0 - below, hist, one ? blo << kSigmaKeyShift : 0u,
+                                    one ? ~((1u << kSigmaKeyShift) - 1u) : 0u, one ? kSigmaKeyShift - 1 : 31);
+    float med = __uint_as_float(lo);
+    if (!(ns & 1)) {
+        // the upper central value: lo again, or the least value above it (in the list)
         int le = 0;
         uint32_t above = 0xFFFFFFFFu;
-        for (int i = threadIdx.x; i < ns; i += blockDim.x) {
-            const uint32_t v = vals[i];
+        for (int i = lane; i < nl; i += 32) {
+            const uint32_t v = lst[i];
             le += v <= lo;
             if (v > lo && v < above) above = v;
         }
-        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             le += __shfl_xor_sync(0xffffffffu, le, o);
             above = min(above, __shfl_xor_sync(0xffffffffu, above, o));
         }
-        if (lane == 0) { wtot[wid] = le; red[wid] = above; }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int tle = 0;
-            uint32_t tab = 0xFFFFFFFFu;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tle += wtot[w]; tab = min(tab, red[w]); }
-            sh[3] = (int)(tle >= half + 1 ? lo : tab);
-        }
-        __syncthreads();
-        med = 0.5f * (__uint_as_float(lo) + __uint_as_float((uint32_t)sh[3]));
+        const uint32_t hi = below + le >= half + 1 ? lo : above;
+        med = 0.5f * (__uint_as_float(lo) + __uint_as_float(hi));
     }
-    if (threadIdx.x == 0) a.sigma[bl] = 1.4826f * med;
+    if (lane == 0) a.sigma[bl] = 1.4826f * med;
 }
 
 size_t sigma_smem(int max_hk, int max_np) {
-    return (size_t)kSampStride * sizeof(float2) + (size_t)kSigmaCap * sizeof(uint32_t) +
+    return (size_t)kSampStride * sizeof(float2) + (size_t)(kSigmaCap + kSigmaBins) * sizeof(uint32_t) +
            (size_t)2 * max_hk * max_np * sizeof(float);
 }
 

@@ -25,6 +25,7 @@
 #include <cuda_fp16.h>
 #include <math.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -275,21 +276,28 @@ __device__ __forceinline__ float gate_dispatch(uint32_t tcol, int nbins, int pw,
 
 constexpr int kEpiThreads = 512;   // 4 warpgroups share the epilogue
 
+// One persistent CTA per SM walks the tiles blockIdx.x, +gridDim.x, ...
+// Thread 0 issues each tile's product (one commit per tile) as soon as its A
+// tile has landed and the TMEM columns it writes are free: with two base-level
+// slots that is right after the decimated levels of the current tile have been
+// scanned, so the next product runs under the base level's scan and the
+// medcut pass.  A tiles are double-buffered in shared memory (one buffer for
+// split tiles), each refilled as soon as the product that read it completed.
 template <int HM>
 __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs t, const uint4* __restrict__ Bg,
                                                       int* err) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const int abytes = kABytes * t.split;     // one tile's A bytes (hi, then lo when split)
-    // two A buffers (the next tile arrives during this tile's MMA); split tiles
-    // take one, refilled as soon as the MMA has read it (during the epilogue)
     const int nbuf = t.split == 2 ? 1 : 2;
     uint8_t* As0 = smem;                      // nbuf A buffers, abytes each
     uint8_t* Bs = smem + nbuf * abytes;       // ncols_total * kK * 2
-    __shared__ uint64_t mbar;                 // MMA completion
+    __shared__ uint64_t mbar;                 // product completion, one phase per tile
     __shared__ uint64_t lbar[2];              // A-tile arrival, one per buffer
     __shared__ uint32_t tmem_base_sh;
+    __shared__ int mma_ok_sh;                 // 0 once a product could not be issued
     __shared__ TcLevel lev_sh[kMaxLevels];
     __shared__ TcUnit unit_sh[kMaxUnits];
+    __shared__ TcMma mma_sh[kMaxMma];
     __shared__ float part_sh[kMaxUnits][kTM];   // per-unit gate partials of the tile
     __shared__ uint8_t lu_start[kMaxLevels + 1], lu_idx[kMaxUnits];
     __shared__ float inv_sh[kMaxLevels];        // 1/sigma of the tile's block, per level
@@ -301,12 +309,14 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     const int tiles_per_blk = a.tiles_per_blk;
     const float gup = a.fp16 ? pow2f(ascale_exp(a.amax_bits)) : 1.0f;   // undoes the FP16 tile scale
     const int ntiles = a.nblk * tiles_per_blk;
+    const int my_ntiles = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
     // B once per CTA.
     const int bwords = t.ncols_total * kK * 2 / 16;
     for (int i = tid; i < bwords; i += blockDim.x) reinterpret_cast<uint4*>(Bs)[i] = Bg[i];
     if (tid < t.nlev) lev_sh[tid] = t.lev[tid];
     if (tid < t.nunit) unit_sh[tid] = t.unit[tid];
+    if (tid < t.nmma) mma_sh[tid] = t.mma[tid];
     if (tid == 0) {
         // each level's units, listed contiguously, for the per-level gate maximum
         int c = 0;
@@ -316,8 +326,7 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
                 if (t.unit[u].lev == l) lu_idx[c++] = (uint8_t)u;
         }
         lu_start[t.nlev] = (uint8_t)c;
-    }
-    if (tid == 0) {
+        mma_ok_sh = 1;
         mbar_init(&mbar, 1);
         mbar_init(&lbar[0], 1);
         mbar_init(&lbar[1], 1);
@@ -335,33 +344,79 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     const uint32_t idesc_base = (1u << 4) | ((uint32_t)(t.fp16 ? 0 : 1) << 7) |
                                 ((uint32_t)(t.fp16 ? 0 : 1) << 10) | ((uint32_t)(kTM >> 4) << 24);
     const uint32_t b_addr = smem_u32(Bs);
-    uint32_t phase = 0;
-    bool ok = true;
-    if (tid == 0 && (int)blockIdx.x < ntiles)
-        bulk_load(smem_u32(As0), a.Atile + (int64_t)blockIdx.x * abytes, abytes, &lbar[0]);
 
+    // Thread 0's bookkeeping: loads issued per A buffer, products issued.
+    int nload[2] = {0, 0};
+    int nmma_issued = 0;
+    // Local tile it sits in A buffer it % nbuf; the n-th load into a buffer
+    // completes that buffer's barrier phase n.
+    auto a_buf = [&](int it) { return nbuf == 2 ? (it & 1) : 0; };
+    auto load_a = [&](int it) {
+        const int b = a_buf(it);
+        bulk_load(smem_u32(As0 + b * abytes), a.Atile + (int64_t)((int)blockIdx.x + it * (int)gridDim.x) * abytes,
+                  abytes, &lbar[b]);
+        ++nload[b];
+    };
+    // Product of local tile it: wait for its A tile, then every column range
+    // into TMEM (the base level into the slot of the tile's parity), one commit.
+    auto issue_mma = [&](int it) -> bool {
+        const int b = a_buf(it);
+        const uint32_t par = (uint32_t)((nbuf == 2 ? (it >> 1) : it) & 1);
+        if (!mbar_wait(&lbar[b], par)) return false;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a_addr = smem_u32(As0 + b * abytes);
+        for (int q = 0; q < t.nmma; ++q) {
+            const TcMma M = mma_sh[q];
+            const uint32_t idesc = idesc_base | ((uint32_t)(M.n >> 3) << 17);
+            const uint32_t dcol = (uint32_t)((it & 1) ? M.tcol1 : M.tcol);
+            // split: the hi tile's K steps, then the lo tile's against the
+            // same twiddles, into one FP32 accumulator
+            for (int kk = 0; kk < t.split * (kK / 16); ++kk) {
+                const int sp = kk / (kK / 16), ks = kk - sp * (kK / 16);
+                const uint64_t da = umma_desc(a_addr + sp * kABytes + ks * 256);
+                const uint64_t db = umma_desc(b_addr + (M.bcol / 8) * kSBO + ks * 256);
+                const uint32_t acc = kk > 0;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(tmem + dcol), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     ::"r"(smem_u32(&mbar)) : "memory");
+        ++nmma_issued;
+        return true;
+    };
+
+    bool ok = true;
+    if (tid == 0 && my_ntiles > 0) {
+        load_a(0);
+        if (nbuf == 2 && my_ntiles > 1) load_a(1);
+        if (!issue_mma(0)) mma_ok_sh = 0;
+    }
     // The per-level sigma and valid counts of the first tile's block; each
-    // iteration then loads the next tile's while its own MMA and epilogue run.
+    // iteration then loads the next tile's while its own epilogue runs.
     float sig_next = 0.0f;
     int nv_next = 0;
-    if (tid < t.nlev && (int)blockIdx.x < ntiles) {
+    if (tid < t.nlev && my_ntiles > 0) {
         const int b0 = (int)blockIdx.x / tiles_per_blk;
         sig_next = a.sigma[b0 * a.nlev + tid];
         nv_next = a.nvalid[b0 * a.nlev + tid];
     }
+    ok = __syncthreads_and(mma_ok_sh != 0) != 0;
+    if (!ok && tid == 0) atomicExch(err, 2);
 
-    int it = 0;
-    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
-        const int buf = nbuf == 2 ? (it & 1) : 0;
+    const int wg = warp >> 2;
+    const int row = (warp & 3) * 32 + (tid & 31);
+    const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+
+    for (int it = 0; it < my_ntiles && ok; ++it) {
+        const int tile = (int)blockIdx.x + it * (int)gridDim.x;
         const int blk = tile / tiles_per_blk;
         const int j0 = (tile % tiles_per_blk) * kTM;
-        // Prefetch the next tile into the other buffer: its previous reader (the
-        // MMA of the last iteration) has completed.
-        if (nbuf == 2 && tid == 0 && tile + (int)gridDim.x < ntiles)
-            bulk_load(smem_u32(As0 + (buf ^ 1) * abytes), a.Atile + (int64_t)(tile + gridDim.x) * abytes,
-                      abytes, &lbar[buf ^ 1]);
-        // the block's per-level sigma and valid counts, for the epilogue (ordered
-        // by the barrier below; the previous epilogue finished at the loop's end)
+        // the block's per-level sigma and valid counts, for the epilogue
+        // (the previous tile's epilogue finished at the last barrier)
         if (tid < t.nlev) {
             // 1/sigma times the A tiles' scale 2^s (exact): the gate in true units
             const float inv = inv_sigma(sig_next) * gup;
@@ -373,94 +428,74 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
             const float c = fminf(a.medcut_gate, a.threshold);
             if (!a.Q0 && inv > 0.0f && c > 0.0f) cut = (c / inv) * (1.0f - 0x1p-16f);
             cut_sh[tid] = cut;
-            const int tn = tile + (int)gridDim.x;
-            if (tn < ntiles) {
-                const int bn = tn / tiles_per_blk;
+            if (it + 1 < my_ntiles) {
+                const int bn = (tile + (int)gridDim.x) / tiles_per_blk;
                 sig_next = a.sigma[bn * a.nlev + tid];
                 nv_next = a.nvalid[bn * a.nlev + tid];
             }
         }
-        // Only the MMA (issued by thread 0) reads the A tile: warp 0 waits for
-        // it, and the barrier holds the other warps.
-        ok = __syncthreads_and(warp == 0 ? mbar_wait(&lbar[buf], (uint32_t)(nbuf == 2 ? ((it >> 1) & 1) : (it & 1)))
-                                         : true) != 0;
+        // this tile's product has completed: its accumulators are readable and
+        // its A buffer may be refilled
+        ok = __syncthreads_and(mbar_wait(&mbar, (uint32_t)(it & 1))) != 0;
         if (!ok) {
             if (tid == 0) atomicExch(err, 2);
             break;
         }
-        const uint32_t a_addr = smem_u32(As0 + buf * abytes);
-
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const int nparts = t.ncols_total > t.n1 ? 2 : 1;
-            for (int part = 0; part < nparts; ++part) {
-                const int ncol0 = part ? t.n1 : 0;
-                const int nn = part ? t.ncols_total - t.n1 : t.n1;
-                const uint32_t idesc = idesc_base | ((uint32_t)(nn >> 3) << 17);
-                // split: the hi tile's K steps, then the lo tile's against the
-                // same twiddles, into one FP32 accumulator
-                for (int kk = 0; kk < t.split * (kK / 16); ++kk) {
-                    const int sp = kk / (kK / 16), ks = kk - sp * (kK / 16);
-                    const uint64_t da = umma_desc(a_addr + sp * kABytes + ks * 256);
-                    const uint64_t db = umma_desc(b_addr + (ncol0 / 8) * kSBO + ks * 256);
-                    const uint32_t acc = kk > 0;
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "setp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                        ::"r"(tmem + (uint32_t)ncol0), "l"(da), "l"(db), "r"(idesc), "r"(acc));
-                }
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                         ::"r"(smem_u32(&mbar)) : "memory");
-        }
-        ok = __syncthreads_and(mbar_wait(&mbar, phase)) != 0;
-        if (!ok && tid == 0) atomicExch(err, 2);
-        if (ok) phase ^= 1u;
-        // one buffer: the MMA has read it, so the next tile may land now
-        if (ok && nbuf == 1 && tid == 0 && tile + (int)gridDim.x < ntiles)
-            bulk_load(smem_u32(As0), a.Atile + (int64_t)(tile + gridDim.x) * abytes, abytes, &lbar[0]);
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-
-        if (ok) {
-            // Epilogue: warpgroup g scans its units; thread owns TMEM row (warp%4)*32 + lane.
-            const int wg = warp >> 2;
-            const int row = (warp & 3) * 32 + (tid & 31);
-            const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-            // need: a gate of the tile may be flagged or pushed.  A -inf gate
-            // whose level could skip (cut > 0, so 1/sigma > 0) is neither, so
-            // a tile whose every unit returned -inf there needs no medcut pass.
-            bool need = false;
+        if (tid == 0) {
+            if (nbuf == 2 && it + 2 < my_ntiles) load_a(it + 2);
+            if (nbuf == 1 && it + 1 < my_ntiles) load_a(it + 1);
+        }
+        const int par = it & 1;
+        // Epilogue: warpgroup wg scans its units of a phase; the thread owns TMEM
+        // row (warp%4)*32 + lane.  need: a gate of the tile may be flagged or
+        // pushed.  A -inf gate whose level could skip (cut > 0, so 1/sigma > 0)
+        // is neither, so a tile whose every unit returned -inf there needs no
+        // medcut pass.
+        auto scan_units = [&](int ph) -> bool {
+            bool nd = false;
             for (int u = 0; u < t.nunit; ++u) {
                 const TcUnit& U = unit_sh[u];
-                if (U.wg != wg) continue;                               // warp-uniform
+                if (U.wg != wg || U.phase != ph) continue;              // warp-uniform
                 if (j0 >= nv_sh[U.lev]) continue;                       // warp-uniform
                 const TcLevel& L = lev_sh[U.lev];
                 const float cut = cut_sh[U.lev];
-                const float v = gate_dispatch<HM>(lane_base + (uint32_t)U.col, U.nstart, U.pw, L.wmask, L.rsq, cut,
+                const uint32_t col = (uint32_t)(par ? U.col1 : U.col);
+                const float v = gate_dispatch<HM>(lane_base + col, U.nstart, U.pw, L.wmask, L.rsq, cut,
                                                   j0 + row < nv_sh[U.lev]);
                 part_sh[u][row] = v;
-                need |= !(cut > 0.0f) || v != -INFINITY;
+                nd |= !(cut > 0.0f) || v != -INFINITY;
             }
-            // gate = max over the level's units, then the medcut test
-            if (__syncthreads_or(need)) for (int idx = tid; idx < t.nlev * kTM; idx += blockDim.x) {
-                const int l = idx / kTM, r = idx % kTM;
-                const int j = j0 + r;
-                if (j >= nv_sh[l]) continue;
-                float g = -INFINITY;
-                for (int i = lu_start[l]; i < lu_start[l + 1]; ++i) g = fmaxf(g, part_sh[lu_idx[i]][r]);
-                if (a.Q0) a.Q0[((int64_t)blk * a.nlev + l) * a.Nprof + j] = g * gup;
-                gate_flag(a, blk, l, j, g, inv_sh[l]);
-            }
-        }
+            return nd;
+        };
+        bool need = scan_units(0);
+        // The columns phase 0 read are free: the next tile's product may land
+        // in them (and in the other base-level slot) while phase 1 and the
+        // medcut pass run.
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
+        if (tid == 0 && it + 1 < my_ntiles && !issue_mma(it + 1)) mma_ok_sh = 0;
+        if (t.dbuf) need |= scan_units(1);
+        // gate = max over the level's units, then the medcut test
+        if (__syncthreads_or(need)) for (int idx = tid; idx < t.nlev * kTM; idx += blockDim.x) {
+            const int l = idx / kTM, r = idx % kTM;
+            const int j = j0 + r;
+            if (j >= nv_sh[l]) continue;
+            float g = -INFINITY;
+            for (int i = lu_start[l]; i < lu_start[l + 1]; ++i) g = fmaxf(g, part_sh[lu_idx[i]][r]);
+            if (a.Q0) a.Q0[((int64_t)blk * a.nlev + l) * a.Nprof + j] = g * gup;
+            gate_flag(a, blk, l, j, g, inv_sh[l]);
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        ok = __syncthreads_and(mma_ok_sh != 0) != 0;
+        if (!ok && tid == 0) atomicExch(err, 2);
     }
-    if (!ok) {
-        // bounded: let an in-flight MMA and prefetch land before TMEM and smem go away
-        mbar_wait(&mbar, phase);
-        mbar_wait(&lbar[0], 0);
-        mbar_wait(&lbar[1], 0);
+    if (tid == 0) {
+        // bounded: let every product and A-tile copy this CTA issued land
+        // before its TMEM and shared memory go away (all have on the normal path)
+        if (nmma_issued > 0) mbar_wait(&mbar, (uint32_t)((nmma_issued - 1) & 1));
+        for (int b = 0; b < 2; ++b)
+            if (nload[b] > 0) mbar_wait(&lbar[b], (uint32_t)((nload[b] - 1) & 1));
     }
     __syncthreads();
     if (warp == 0) {
@@ -483,7 +518,7 @@ static uint16_t to_half_bits(float v, int fp16) {
 }
 
 int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, TcPlanHost* out) {
-    if (2 * nharms > kK) return -1;
+    if (2 * nharms > kK || nlev < 1) return -1;
     TcArgs& t = out->args;
     t = TcArgs{};
     t.nlev = nlev;
@@ -493,13 +528,19 @@ int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, Tc
     for (int l = 0; l < nlev; ++l) wmax = wmax > dl[l].wmax ? wmax : dl[l].wmax;
     t.hm = wmax <= 8 ? 8 : (wmax <= 32 ? 32 : 0);
     if (!t.hm) return -2;
-    int col = 0;
+    auto pad16 = [](int x) { return (x + 15) / 16 * 16; };
+    auto pad32 = [](int x) { return (x + 31) / 32 * 32; };
+    // Each level's columns: its bins followed by its first wmax bins.  The
+    // decimated levels lie one after another (offsets relative to the first);
+    // the base level's B columns come first, their count fixed below.
+    int rcol = 0;
     for (int l = 0; l < nlev; ++l) {
         TcLevel& L = t.lev[l];
         L.nbins = dl[l].nbins;
         L.ncol = dl[l].nbins + dl[l].wmax;
         L.pw = (L.ncol + t.hm - 1) / t.hm * t.hm;
-        L.col = col;
+        L.col = l == 0 ? 0 : rcol;
+        if (l > 0) rcol += L.pw;
         L.wmask = 0;
         for (int i = 0; i < 32; ++i) L.rsq[i] = 0.0f;
         for (int i = 0; i < dl[l].nw; ++i) {
@@ -507,55 +548,141 @@ int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, Tc
             L.wmask |= 1u << (w - 1);
             L.rsq[w - 1] = dl[l].rsqrtw[i];
         }
-        col += L.pw;
     }
-    const int total = (col + 15) / 16 * 16;
-    if (total > 512) return -3;
-    // Epilogue units: split each level's boxcar starts into segments of about
-    // equal scan cost (every segment re-reads wmax columns), then place them on
-    // the 4 warpgroups, heaviest first onto the lightest.
-    double tot_cost = 0.0;
-    for (int l = 0; l < nlev; ++l) tot_cost += (double)(dl[l].nbins + dl[l].wmax) * (1 + 2 * dl[l].nw);
-    const double target = tot_cost / 8.0;
-    int nu = 0;
-    struct UC { int lev, p0, nst; double c; } uc[kMaxUnits];
-    for (int l = 0; l < nlev; ++l) {
-        const double c = (double)(dl[l].nbins + dl[l].wmax) * (1 + 2 * dl[l].nw);
-        int nseg = (int)(c / target + 0.5);
-        nseg = nseg < 1 ? 1 : nseg;
-        while (nseg > 1 && dl[l].nbins / nseg < 8) --nseg;
-        if (nu + nseg > kMaxUnits) nseg = 1;
-        if (nu + nseg > kMaxUnits) return -4;
-        t.lev[l].nunits = nseg;
-        for (int sgi = 0; sgi < nseg; ++sgi) {
-            // segment boundaries on multiples of 8 columns
-            const int p0 = (int)(((int64_t)dl[l].nbins * sgi / nseg) / 8 * 8);
-            const int p1 = sgi + 1 == nseg ? dl[l].nbins : (int)(((int64_t)dl[l].nbins * (sgi + 1) / nseg) / 8 * 8);
-            uc[nu++] = {l, p0, p1 - p0, (double)(p1 - p0 + dl[l].wmax) * (1 + 2 * dl[l].nw)};
+    const int g1 = pad16(rcol);          // decimated levels
+    if (g1 + pad16(t.lev[0].pw) > 512) return -3;
+    int try_dbuf = 1;
+    auto phase_of = [&](int l) { return (try_dbuf && l == 0) ? 1 : 0; };
+    struct UC { int lev, p0, nst; double c; };
+    auto seg_cost = [&](int l, int nst) { return (double)(nst + dl[l].wmax) * (1 + 2 * dl[l].nw); };
+    // The units of one phase for a segment target of (phase cost / div), and
+    // their longest-processing-time placement on the 4 warpgroups.
+    auto build_phase = [&](int ph, int div, UC* uc, int* wg_of, double* maxload) -> int {
+        double ph_cost = 0.0;
+        for (int l = 0; l < nlev; ++l)
+            if (phase_of(l) == ph) ph_cost += seg_cost(l, dl[l].nbins);
+        int nu = 0;
+        for (int l = 0; l < nlev; ++l) {
+            if (phase_of(l) != ph) continue;
+            int nseg = (int)(seg_cost(l, dl[l].nbins) / (ph_cost / div) + 0.5);
+            nseg = nseg < 1 ? 1 : nseg;
+            while (nseg > 1 && dl[l].nbins / nseg < 8) --nseg;
+            if (nu + nseg > kMaxUnits) return -1;
+            for (int sgi = 0; sgi < nseg; ++sgi) {
+                // segment boundaries on multiples of 8 columns
+                const int p0 = (int)(((int64_t)dl[l].nbins * sgi / nseg) / 8 * 8);
+                const int p1 =
+                    sgi + 1 == nseg ? dl[l].nbins : (int)(((int64_t)dl[l].nbins * (sgi + 1) / nseg) / 8 * 8);
+                uc[nu++] = {l, p0, p1 - p0, seg_cost(l, p1 - p0)};
+            }
         }
+        double load[4] = {0.0, 0.0, 0.0, 0.0};
+        bool used[kMaxUnits] = {false};
+        for (int k = 0; k < nu; ++k) {
+            int best = -1;
+            for (int i = 0; i < nu; ++i)
+                if (!used[i] && (best < 0 || uc[i].c > uc[best].c)) best = i;
+            used[best] = true;
+            int g = 0;
+            for (int q = 1; q < 4; ++q) if (load[q] < load[g]) g = q;
+            load[g] += uc[best].c;
+            wg_of[best] = g;
+        }
+        *maxload = std::max(std::max(load[0], load[1]), std::max(load[2], load[3]));
+        return nu;
+    };
+    // Epilogue units: each level's boxcar starts split into segments (every
+    // segment re-reads wmax columns), then placed on the 4 warpgroups.  With
+    // two base-level slots the decimated levels are scanned first (phase 0)
+    // and the base level second (phase 1), while the next tile's product
+    // lands in the other slot and in the freed decimated columns.  Per phase,
+    // the segment size that gives the lightest heaviest warpgroup wins.  A
+    // slot spans every column its units read (each unit reads a multiple of
+    // the ring size from its first start), so that no scan reaches into the
+    // other slot, which the next tile's product may be writing.
+    UC all_uc[kMaxUnits];
+    int all_wg[kMaxUnits], all_ph[kMaxUnits];
+    int nall = 0;
+    int slot_w = t.lev[0].pw;
+    for (try_dbuf = 1; try_dbuf >= 0; --try_dbuf) {
+        nall = 0;
+        bool okp = true;
+        for (int ph = 0; ph < 2 && okp; ++ph) {
+            UC best_uc[kMaxUnits], uc[kMaxUnits];
+            int best_wg[kMaxUnits], wg_of[kMaxUnits];
+            int best_nu = 0;
+            double best_load = 0.0;
+            for (int div : {4, 5, 6, 8, 10, 12, 16}) {
+                double ml = 0.0;
+                const int nu = build_phase(ph, div, uc, wg_of, &ml);
+                if (nu < 0 || nall + nu > kMaxUnits) continue;
+                if (best_nu == 0 || ml < best_load) {
+                    best_nu = nu;
+                    best_load = ml;
+                    std::copy(uc, uc + nu, best_uc);
+                    std::copy(wg_of, wg_of + nu, best_wg);
+                }
+            }
+            bool any = false;
+            for (int l = 0; l < nlev; ++l) any |= phase_of(l) == ph;
+            if (any && best_nu == 0) okp = false;
+            for (int i = 0; i < best_nu; ++i) {
+                all_uc[nall] = best_uc[i];
+                all_wg[nall] = best_wg[i];
+                all_ph[nall++] = ph;
+            }
+        }
+        if (!okp) continue;
+        slot_w = t.lev[0].pw;
+        for (int i = 0; i < nall; ++i)
+            if (all_uc[i].lev == 0) {
+                const int upw = (all_uc[i].nst + dl[0].wmax + t.hm - 1) / t.hm * t.hm;
+                slot_w = std::max(slot_w, all_uc[i].p0 + upw);
+            }
+        slot_w = pad16(slot_w);
+        if (!try_dbuf || pad32(g1) + pad32(slot_w) + slot_w <= 512) break;
     }
-    double load[4] = {0.0, 0.0, 0.0, 0.0};
-    bool used[kMaxUnits] = {false};
-    t.nunit = nu;
-    for (int k = 0; k < nu; ++k) {
-        int best = -1;
-        for (int i = 0; i < nu; ++i)
-            if (!used[i] && (best < 0 || uc[i].c > uc[best].c)) best = i;
-        used[best] = true;
-        int g = 0;
-        for (int q = 1; q < 4; ++q) if (load[q] < load[g]) g = q;
-        load[g] += uc[best].c;
-        TcUnit& U = t.unit[best];
-        U.lev = (int16_t)uc[best].lev;
-        U.wg = (int16_t)g;
-        U.nstart = (int16_t)uc[best].nst;
-        U.pw = (int16_t)((uc[best].nst + dl[uc[best].lev].wmax + t.hm - 1) / t.hm * t.hm);
-        U.col = (int16_t)(t.lev[uc[best].lev].col + uc[best].p0);
+    if (try_dbuf < 0) return -4;
+    t.dbuf = try_dbuf;
+    // B columns: the base level's slot width (its bins, its wrapped tail and
+    // zero columns up to the reach of its scans, so that every column a scan
+    // reads is written by the product), then the decimated levels.
+    const int g0 = slot_w;
+    const int total = g0 + g1;
+    if (total > 512) return -3;
+    for (int l = 1; l < nlev; ++l) t.lev[l].col += g0;
+    // TMEM: the decimated levels at [0, g1), then the base level's slot for
+    // even tiles and, with two slots, the one for odd tiles (32-column aligned).
+    const int slot0 = t.dbuf ? pad32(g1) : g1, slot1 = t.dbuf ? slot0 + pad32(slot_w) : slot0;
+    if (slot0 + slot_w > 512) return -3;
+    auto tcol_of = [&](int l, int odd) { return l == 0 ? (odd ? slot1 : slot0) : t.lev[l].col - g0; };
+    t.nmma = 0;
+    for (int c = 0; c < g0; c += 256) {
+        const int n = g0 - c < 256 ? g0 - c : 256;
+        t.mma[t.nmma++] = {(int16_t)c, (int16_t)n, (int16_t)(slot0 + c), (int16_t)(slot1 + c)};
+    }
+    for (int c = 0; c < g1; c += 256) {
+        const int n = g1 - c < 256 ? g1 - c : 256;
+        if (t.nmma >= kMaxMma) return -4;
+        t.mma[t.nmma++] = {(int16_t)(g0 + c), (int16_t)n, (int16_t)c, (int16_t)c};
+    }
+    t.nunit = nall;
+    for (int l = 0; l < nlev; ++l) t.lev[l].nunits = 0;
+    for (int i = 0; i < nall; ++i) {
+        TcUnit& U = t.unit[i];
+        const int l = all_uc[i].lev;
+        t.lev[l].nunits += 1;
+        U.lev = (int16_t)l;
+        U.wg = (int16_t)all_wg[i];
+        U.nstart = (int16_t)all_uc[i].nst;
+        U.pw = (int16_t)((all_uc[i].nst + dl[l].wmax + t.hm - 1) / t.hm * t.hm);
+        U.col = (int16_t)(tcol_of(l, 0) + all_uc[i].p0);
+        U.col1 = (int16_t)(tcol_of(l, 1) + all_uc[i].p0);
+        U.phase = (int16_t)all_ph[i];
         U.pad = 0;
-        if (U.col + U.pw > 512) return -3;
+        if (U.col + U.pw > 512 || U.col1 + U.pw > 512) return -3;
     }
     t.ncols_total = total;
-    t.n1 = total > 256 ? 256 : total;
     out->B.assign((size_t)total * kK, 0);
     for (int l = 0; l < nlev; ++l) {
         const DevLevel& d = dl[l];

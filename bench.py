@@ -330,6 +330,8 @@ def run_ours(args, rank, world, local_rank):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     lof, hif = args.band if args.band else (LOF, HIF)
+    # launch shapes from the autotuner (setup, outside the timed region)
+    tune = None if args.no_tune else eng.autotune(lof, hif, 100, BLOCK, nsample=256)
 
     def step_device():
         return eng.search_raw(lof, hif, 100, BLOCK, THR)
@@ -382,6 +384,8 @@ def run_ours(args, rank, world, local_rank):
                                     threshold=THR, synth="fp32"), device=local_rank)
         eng32.set_stream(stream.cuda_stream)
         eng32.set_spectrum_device(d_amps.data_ptr(), namps, N, dt, keep=d_amps)
+        if not args.no_tune:
+            eng32.autotune(lof, hif, 100, BLOCK, nsample=256)
         c32 = eng32.search_raw(lof, hif, 100, BLOCK, THR)
         ms32 = 0.0
         for _ in range(max(1, args.steps)):
@@ -401,7 +405,7 @@ def run_ours(args, rank, world, local_rank):
         t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, ms_e2e = float(t[0]), float(t[1])
-    res = {"ms": ms, "ms_e2e": ms_e2e, "namps": namps, "stage": stage, "launches": launches, "h2d": h2d, "d2h": d2h,
+    res = {"ms": ms, "ms_e2e": ms_e2e, "namps": namps, "tune": tune, "stage": stage, "launches": launches, "h2d": h2d, "d2h": d2h,
            "trials": trials, "ncand": ncand, "clocks": clk.summary(), "stats": st, "plain": plain}
     del eng
     return res
@@ -463,6 +467,7 @@ def main():
                     help="search only [LO, HI] Hz (a smaller case of the same kernels, for profiling)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison run")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuner)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -644,6 +649,8 @@ def main():
     cfg["profiles_per_step"] = st["profiles"]
     cfg["candidates_per_step"] = res["ncand"]
     cfg["rescued_per_step"] = st["rescued"]
+    if res.get("tune"):
+        cfg["autotuned"] = res["tune"]
     if args.band:
         cfg["band_hz"] = list(args.band)
     if res["plain"]:

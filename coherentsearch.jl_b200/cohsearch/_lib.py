@@ -100,6 +100,14 @@ class cs_adam_param(ctypes.Structure):
                 ("v", ctypes.c_void_p), ("grad", ctypes.c_void_p), ("n", ctypes.c_int64)]
 
 
+class cs_tune_report(ctypes.Structure):
+    _fields_ = [("interp_kernel", ctypes.c_int32), ("tc_double_buffer", ctypes.c_int32),
+                ("tc_div", ctypes.c_int32 * 2), ("nlev", ctypes.c_int32), ("nbins", ctypes.c_int32 * CS_MAX_DECIM),
+                ("units", ctypes.c_int32 * CS_MAX_DECIM), ("ms_interp", ctypes.c_double * 2),
+                ("ms_synth_model", ctypes.c_double), ("ms_synth_tuned", ctypes.c_double),
+                ("sample_blocks", ctypes.c_int64)]
+
+
 _P = ctypes.c_void_p
 _i32 = ctypes.c_int32
 _i64 = ctypes.c_int64
@@ -128,6 +136,7 @@ PROTOTYPES = {
     "cs_search_trial_metrics": (_i32, [_P, _P, _i64, ctypes.POINTER(_i64)]),
     "cs_set_diagnostics": (_i32, [_P, _i32]),
     "cs_set_memory_limit": (_i32, [_P, _i64]),
+    "cs_autotune": (_i32, [_P, _f64, _f64, _i64, _i64, _i64, ctypes.POINTER(cs_tune_report)]),
     "cs_set_wait_test": (_i32, [_P, _i64]),
     "cs_search_gate_values": (_i32, [_P, _P, _i64, ctypes.POINTER(_i64)]),
     "cs_version": (ctypes.c_char_p, []),

@@ -353,6 +353,23 @@ class Engine:
                                                    ctypes.byref(n)), self._h)
         return sig, nv
 
+    def autotune(self, lofreq=0.1, hifreq=100.0, lobin=100, blocksize=2048, nsample=256) -> dict:
+        """Time the launch-shape candidates on `nsample` blocks from the middle
+        of the band (cs_autotune) and keep the fastest: the interpolation
+        kernel, and in the tensor modes the epilogue segment size per profile
+        bin count and the base level's TMEM double buffer.  Returns what was
+        chosen and measured."""
+        r = _lib.cs_tune_report()
+        _lib.check(self.lib.cs_autotune(self._h, float(lofreq), float(hifreq), int(lobin), int(blocksize),
+                                        int(nsample), ctypes.byref(r)), self._h, "cs_autotune")
+        n = r.nlev
+        return {"interp_kernel": "persistent" if r.interp_kernel else "per-item",
+                "tc_double_buffer": bool(r.tc_double_buffer), "tc_div": list(r.tc_div),
+                "units_per_level": {int(r.nbins[i]): int(r.units[i]) for i in range(n)},
+                "ms_interp": {"per-item": r.ms_interp[0], "persistent": r.ms_interp[1]},
+                "ms_synth_model": r.ms_synth_model, "ms_synth_tuned": r.ms_synth_tuned,
+                "sample_blocks": int(r.sample_blocks)}
+
     def set_memory_limit(self, nbytes: int):
         """Cap the device memory the engine holds (0: no cap); searches split
         into waves under it, or raise CohSearchError(CS_ERR_OUT_OF_MEMORY)."""

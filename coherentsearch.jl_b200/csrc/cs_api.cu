@@ -313,6 +313,13 @@ struct cs_handle {
     std::vector<float> last_gate;
     int diag = 0;
     size_t mem_limit = 0;   // cs_set_memory_limit: device bytes the handle may hold (0: no cap)
+    // launch shapes (cs_autotune): interpolation kernel (-1: by applicability,
+    // 0: one CTA per item, 1: persistent), the tensor epilogue's segment
+    // divisors per phase (0: cost model) and its base-level double buffer
+    int tune_interp = -1;
+    int tune_div[2] = {0, 0};
+    int tune_dbuf = 1;
+    bool interp2_used = false, interp2_ok = false;   // the last search's interpolation kernel / its applicability
     int64_t stall_ns = 0;   // cs_set_wait_test
     int last_nlev = 0;
     int last_Nprof = 0;
@@ -360,6 +367,19 @@ cs_status validate(const cs_params* p) {
 
 // Levels: the base fold k = 1, then every k > 1 of params.decimations in
 // order (Workspace.decims, src/search.jl:1251-1254).
+// The tensor synthesis plan with the handle's launch shapes, and its twiddles on the device.
+cs_status build_tc(cs_handle* H) {
+    const cs_params& p = H->p;
+    const int rc = prepare_tc(H->dlev.data(), (int)H->dlev.size(), p.nharms, synth_fp16(p.synth) ? 1 : 0,
+                              synth_split(p.synth), &H->tc, H->tune_div[0], H->tune_div[1], H->tune_dbuf);
+    if (rc != 0)
+        return fail(H, CS_ERR_UNSUPPORTED,
+                    "tensor-core synthesis needs nharms <= 64, boxcar widths <= 32 and <= 512 TMEM columns");
+    CS_CUDA(upload(H->d_tcB, H->tc.B, H->stream), "upload tensor twiddles");
+    H->graph_valid = false;   // a captured graph holds the old plan
+    return CS_OK;
+}
+
 cs_status build_levels(cs_handle* H) {
     const cs_params& p = H->p;
     std::vector<int> ks{1};
@@ -411,14 +431,7 @@ cs_status build_levels(cs_handle* H) {
     }
     CS_CUDA(upload(H->d_levels, H->dlev, H->stream), "upload levels");
     CS_CUDA(upload(H->d_tw, tw, H->stream), "upload twiddles");
-    if (p.synth != CS_SYNTH_FP32) {
-        const int rc = prepare_tc(H->dlev.data(), (int)H->dlev.size(), p.nharms, synth_fp16(p.synth) ? 1 : 0,
-                                  synth_split(p.synth), &H->tc);
-        if (rc != 0)
-            return fail(H, CS_ERR_UNSUPPORTED,
-                        "tensor-core synthesis needs nharms <= 64, boxcar widths <= 32 and <= 512 TMEM columns");
-        CS_CUDA(upload(H->d_tcB, H->tc.B, H->stream), "upload tensor twiddles");
-    }
+    if (p.synth != CS_SYNTH_FP32) return build_tc(H);
     return CS_OK;
 }
 
@@ -522,6 +535,10 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
     bool interp2 = p.m == 16 && interp2_smem(win_max, Nprof) <= 112 * 1024 &&
                    (reinterpret_cast<uintptr_t>(H->amps) & 7u) == 0;
     for (const DevHarm& d : ps->host.harms) interp2 = interp2 && d.P >= 1 && d.P <= 256;
+    const bool interp2_ok = interp2;
+    if (H->tune_interp == 0) interp2 = false;
+    H->interp2_used = interp2;
+    H->interp2_ok = interp2_ok;
     int maxbins = 0, maxwmax = 0;
     for (int l = 0; l < R.nlev; ++l) {
         maxbins = std::max(maxbins, H->dlev[l].nbins);
@@ -1008,6 +1025,37 @@ const char* cs_version(void) { return CS_VERSION_STRING; }
 
 const char* cs_last_error(const cs_handle* h) { return h ? h->err.c_str() : "null handle"; }
 
+namespace {
+// Launch shapes cs_autotune chose, per device and cs_params (bytewise).
+struct TuneEntry {
+    int device;
+    cs_params p;
+    int interp, div0, div1, dbuf;
+};
+std::mutex g_tune_mu;
+std::vector<TuneEntry> g_tune_cache;
+
+bool tune_lookup(int device, const cs_params& p, TuneEntry* out) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (const TuneEntry& e : g_tune_cache)
+        if (e.device == device && std::memcmp(&e.p, &p, sizeof(cs_params)) == 0) {
+            *out = e;
+            return true;
+        }
+    return false;
+}
+
+void tune_store(const TuneEntry& t) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (TuneEntry& e : g_tune_cache)
+        if (e.device == t.device && std::memcmp(&e.p, &t.p, sizeof(cs_params)) == 0) {
+            e = t;
+            return;
+        }
+    g_tune_cache.push_back(t);
+}
+}  // namespace
+
 cs_status cs_create(cs_handle** out, const cs_params* params, int32_t device) {
     if (!out) return CS_ERR_INVALID_ARGUMENT;
     *out = nullptr;
@@ -1032,6 +1080,15 @@ cs_status cs_create(cs_handle** out, const cs_params* params, int32_t device) {
         return CS_ERR_CUDA;
     }
     st = build_levels(H);
+    TuneEntry te{};
+    if (st == CS_OK && tune_lookup(device, H->p, &te)) {
+        // launch shapes an earlier cs_autotune chose for these parameters here
+        H->tune_interp = te.interp;
+        H->tune_div[0] = te.div0;
+        H->tune_div[1] = te.div1;
+        H->tune_dbuf = te.dbuf;
+        if (H->p.synth != CS_SYNTH_FP32) st = build_tc(H);
+    }
     if (st != CS_OK) {
         cs_destroy(H);
         return st;
@@ -1762,6 +1819,114 @@ cs_status cs_search_block_values(const cs_handle* H, float* sigma, int32_t* nval
     if (cap < n) return CS_ERR_CAPACITY;
     if (sigma) std::copy(H->last_sigma.begin(), H->last_sigma.end(), sigma);
     if (nvalid) std::copy(H->last_nvalid.begin(), H->last_nvalid.end(), nvalid);
+    return CS_OK;
+}
+
+cs_status cs_autotune(cs_handle* H, double lofreq, double hifreq, int64_t lobin, int64_t blocksize, int64_t nsample,
+                      cs_tune_report* out) {
+    if (!H || nsample < 1 || blocksize < 1) return CS_ERR_INVALID_ARGUMENT;
+    if (!H->has_spec) return fail(H, CS_ERR_NO_SPECTRUM, "no spectrum attached");
+    CS_CUDA(cudaSetDevice(H->device), "set device");
+    RunSpec R{};
+    bool empty = true;
+    cs_status st = setup_run(H, lofreq, hifreq, lobin, blocksize, H->p.threshold, 0, 0, -1, nullptr, 0, R, &empty);
+    if (st != CS_OK) return st;
+    if (empty) return fail(H, CS_ERR_INVALID_ARGUMENT, "the band holds no trials");
+    const int64_t ns = std::min(nsample, R.nblocks);
+    const int64_t b0 = (R.nblocks - ns) / 2;
+    // the sample is searched plainly: no statistics, normalisation or diagnostics
+    const bool ms_on = H->ms_on, norm_on = H->norm_on;
+    const int diag = H->diag;
+    H->ms_on = H->norm_on = false;
+    H->diag = 0;
+    // stage times of one configuration: the least of 3 runs after a warm-up
+    auto timed = [&](double* ms_i, double* ms_s) -> cs_status {
+        std::vector<cs_candidate> c;
+        double bi = 1e300, bs = 1e300;
+        for (int r = 0; r < 4; ++r) {
+            c.clear();
+            const cs_status e = search_core(H, lofreq, hifreq, lobin, blocksize, H->p.threshold, 0, b0, b0 + ns, &c);
+            if (e != CS_OK) return e;
+            if (r > 0) {
+                bi = std::min(bi, H->stats.ms_interp);
+                bs = std::min(bs, H->stats.ms_synth);
+            }
+        }
+        *ms_i = bi;
+        *ms_s = bs;
+        return CS_OK;
+    };
+    cs_tune_report rep{};
+    rep.sample_blocks = ns;
+    rep.ms_interp[0] = rep.ms_interp[1] = -1.0;
+    const bool tensor = H->p.synth != CS_SYNTH_FP32;
+    double msi = 0.0, mss = 0.0;
+    // 1. the interpolation kernel
+    H->tune_interp = 1;
+    H->tune_div[0] = H->tune_div[1] = 0;
+    H->tune_dbuf = 1;
+    if (tensor) st = build_tc(H);
+    if (st == CS_OK) st = timed(&msi, &mss);
+    if (st == CS_OK && H->interp2_ok) rep.ms_interp[1] = msi;
+    double ms_model = mss;
+    if (st == CS_OK) {
+        H->tune_interp = 0;
+        st = timed(&msi, &mss);
+        rep.ms_interp[0] = msi;
+    }
+    if (st == CS_OK) H->tune_interp = (rep.ms_interp[1] >= 0.0 && rep.ms_interp[1] < rep.ms_interp[0]) ? 1 : 0;
+    // 2. tensor epilogue: segment divisor of each phase, then one or two base-level slots
+    if (st == CS_OK && tensor) {
+        int best[3] = {0, 0, 1};   // div0, div1, dbuf
+        double best_ms = ms_model;
+        auto trial = [&](int d0, int d1, int db) -> cs_status {
+            H->tune_div[0] = d0;
+            H->tune_div[1] = d1;
+            H->tune_dbuf = db;
+            if (build_tc(H) != CS_OK) return CS_OK;   // this shape does not fit: skip it
+            double a = 0.0, b = 0.0;
+            const cs_status e = timed(&a, &b);
+            if (e != CS_OK) return e;
+            if (b < best_ms) {
+                best_ms = b;
+                best[0] = d0;
+                best[1] = d1;
+                best[2] = db;
+            }
+            return CS_OK;
+        };
+        const int divs[] = {4, 5, 6, 8, 10, 12, 16};
+        if (H->dlev.size() > 1)
+            for (int d : divs)
+                if (st == CS_OK) st = trial(d, best[1], best[2]);
+        for (int d : divs)
+            if (st == CS_OK) st = trial(best[0], d, best[2]);
+        if (st == CS_OK) st = trial(best[0], best[1], 0);
+        H->tune_div[0] = best[0];
+        H->tune_div[1] = best[1];
+        H->tune_dbuf = best[2];
+        const cs_status e = build_tc(H);
+        if (st == CS_OK) st = e;
+        rep.ms_synth_model = ms_model;
+        rep.ms_synth_tuned = best_ms;
+    } else {
+        rep.ms_synth_model = rep.ms_synth_tuned = mss;
+    }
+    H->ms_on = ms_on;
+    H->norm_on = norm_on;
+    H->diag = diag;
+    if (st != CS_OK) return st;
+    rep.interp_kernel = H->tune_interp;
+    rep.tc_double_buffer = tensor ? H->tc.args.dbuf : 0;
+    rep.tc_div[0] = tensor ? H->tune_div[0] : 0;
+    rep.tc_div[1] = tensor ? H->tune_div[1] : 0;
+    rep.nlev = (int32_t)H->dlev.size();
+    for (int l = 0; l < rep.nlev && l < CS_MAX_DECIM; ++l) {
+        rep.nbins[l] = H->dlev[l].nbins;
+        rep.units[l] = tensor ? H->tc.args.lev[l].nunits : 0;
+    }
+    tune_store({H->device, H->p, H->tune_interp, H->tune_div[0], H->tune_div[1], H->tune_dbuf});
+    if (out) *out = rep;
     return CS_OK;
 }
 

@@ -199,7 +199,11 @@ struct TcPlanHost {
 };
 
 // Returns 0, or < 0 when the configuration does not fit the tensor path.
-int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, TcPlanHost* out);
+// div0/div1 (> 0): the epilogue segment divisor of phase 0 / 1 instead of the
+// cost model's choice (one of 4, 5, 6, 8, 10, 12, 16); allow_dbuf = 0: one
+// base-level TMEM slot.
+int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, TcPlanHost* out, int div0 = 0,
+               int div1 = 0, int allow_dbuf = 1);
 cudaError_t launch_synth_tc(const WaveArgs& a, const TcPlanHost& tp, const void* dB, int* err,
                             cudaStream_t st, int num_sms);
 

@@ -517,7 +517,8 @@ static uint16_t to_half_bits(float v, int fp16) {
     return *reinterpret_cast<uint16_t*>(&b);
 }
 
-int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, TcPlanHost* out) {
+int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, TcPlanHost* out, int div0, int div1,
+               int allow_dbuf) {
     if (2 * nharms > kK || nlev < 1) return -1;
     TcArgs& t = out->args;
     t = TcArgs{};
@@ -604,7 +605,7 @@ int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, Tc
     int all_wg[kMaxUnits], all_ph[kMaxUnits];
     int nall = 0;
     int slot_w = t.lev[0].pw;
-    for (try_dbuf = 1; try_dbuf >= 0; --try_dbuf) {
+    for (try_dbuf = allow_dbuf ? 1 : 0; try_dbuf >= 0; --try_dbuf) {
         nall = 0;
         bool okp = true;
         for (int ph = 0; ph < 2 && okp; ++ph) {
@@ -613,6 +614,8 @@ int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, Tc
             int best_nu = 0;
             double best_load = 0.0;
             for (int div : {4, 5, 6, 8, 10, 12, 16}) {
+                const int forced = ph ? div1 : div0;   // a tuned divisor replaces the search
+                if (forced > 0 && div != forced) continue;
                 double ml = 0.0;
                 const int nu = build_phase(ph, div, uc, wg_of, &ml);
                 if (nu < 0 || nall + nu > kMaxUnits) continue;

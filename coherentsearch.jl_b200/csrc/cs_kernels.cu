@@ -782,12 +782,65 @@ __device__ __forceinline__ void synth_chunk8x2(const float2* __restrict__ xa, co
     }
 }
 
+// Window-energy bound of the gate (the FP32 form of the tensor epilogue's
+// skip).  Over the stored prefix rows ps[0 .. nbins+W] of trial column t,
+// with y_e = ps[e+1] - ps[e], every gate term ps[p+w] - ps[p] (w <= W) is a
+// sum of w of the y, so by Cauchy-Schwarz (ps[p+w] - ps[p]) / sqrt(w) is at
+// most the root of the largest sum of y^2 over W consecutive columns from a
+// start p < nbins.  Returned: that largest sum (FP32, fused multiply-add
+// prefix of y^2 and a W-slot ring of it) and the total of y^2 for the
+// rounding slack.
+template <int W>
+__device__ __forceinline__ float ps_window_energy(const float* buf, int TT, int t, int nbins, float* qtot) {
+    float ring[W];
+#pragma unroll
+    for (int d = 0; d < W; ++d) ring[d] = INFINITY;   // no window starts before column 0
+    ring[0] = 0.0f;
+    float q = 0.0f, mx = -INFINITY, prev = buf[t];
+    const int ne = nbins + W - 1;   // columns e whose window [e+1-W, e+1) starts at p < nbins
+    for (int e0 = 0; e0 < ne; e0 += W) {
+#pragma unroll
+        for (int u = 0; u < W; ++u) {
+            if (e0 + u < ne) {
+                const float cur = buf[(e0 + u + 1) * TT + t];
+                const float y = cur - prev;
+                prev = cur;
+                q = fmaf(y, y, q);
+                // Q[e+1] and Q[e+1-W] share ring slot (u+1) mod W
+                mx = fmaxf(mx, q - ring[(u + 1) % W]);
+                ring[(u + 1) % W] = q;
+            }
+        }
+    }
+    *qtot = q;
+    return mx;
+}
+
+__device__ __forceinline__ float ps_energy_bound(const float* buf, int TT, int t, int nbins, int W) {
+    float q = 0.0f, mx;
+    switch (W) {
+        case 1: mx = ps_window_energy<1>(buf, TT, t, nbins, &q); break;
+        case 2: mx = ps_window_energy<2>(buf, TT, t, nbins, &q); break;
+        case 3: mx = ps_window_energy<3>(buf, TT, t, nbins, &q); break;
+        case 4: mx = ps_window_energy<4>(buf, TT, t, nbins, &q); break;
+        case 5: mx = ps_window_energy<5>(buf, TT, t, nbins, &q); break;
+        case 6: mx = ps_window_energy<6>(buf, TT, t, nbins, &q); break;
+        case 7: mx = ps_window_energy<7>(buf, TT, t, nbins, &q); break;
+        case 8: mx = ps_window_energy<8>(buf, TT, t, nbins, &q); break;
+        default: return INFINITY;   // wider boxcars: no bound, the full scan runs
+    }
+    // slack: 2^-13 of the total for the prefix roundings of both scans and the
+    // differences of the stored rows, then a relative 2^-16 for the rest
+    return (sqrtf(mx + q * 0x1p-13f) + 0x1p-13f * sqrtf((float)(nbins + W) * q)) * (1.0f + 0x1p-16f);
+}
+
 __global__ void __launch_bounds__(2 * kTileTrials) k_synth_fp32(WaveArgs a) {
     constexpr int TT = kTileTrials;
     extern __shared__ float4 smem4[];
     float2* Xs = reinterpret_cast<float2*>(smem4);               // [nharms][TT]
     float* buf = reinterpret_cast<float*>(Xs + a.nharms * TT);   // [nbuf][TT]
     __shared__ float red[2][TT];
+    __shared__ int skip_sh[TT];
 
     const int tile = blockIdx.x;
     const int blk = blockIdx.y;
@@ -834,10 +887,19 @@ __global__ void __launch_bounds__(2 * kTileTrials) k_synth_fp32(WaveArgs a) {
                 buf[(i + 1) * TT + t] = s;
             }
             for (int u = 1; u <= wmax; ++u) buf[(nbins + u) * TT + t] = s + buf[u * TT + t];
+            // skip the full gate scan when the window-energy bound keeps this
+            // trial's gate below both the medcut test and the threshold (its
+            // gate is then -inf: neither flagged nor a candidate); never with
+            // the exact gate values requested
+            const float c = fminf(a.medcut_gate, a.threshold);
+            bool skip = false;
+            if (!a.Q0 && invsig > 0.0f && c > 0.0f)
+                skip = ps_energy_bound(buf, TT, t, nbins, wmax) < (c / invsig) * (1.0f - 0x1p-16f);
+            skip_sh[t] = skip;
         }
         __syncthreads();
         float best = -INFINITY;
-        for (int wi = half; wi < nw; wi += 2) {
+        if (!skip_sh[t]) for (int wi = half; wi < nw; wi += 2) {
             const int w = L.widths[wi];
             float mm = buf[w * TT + t] - buf[t];
             for (int p = 1; p < nbins; ++p) mm = fmaxf(mm, buf[(p + w) * TT + t] - buf[p * TT + t]);

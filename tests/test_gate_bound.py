@@ -104,3 +104,63 @@ def test_energy_bound_prunes_noise():
     B = _bound_fp32(x, 6)
     cut = 6.0 - (0.02 * 6.0 + 0.05)
     assert np.mean(B < cut) > 0.999
+
+
+# ---------------------------------------------------------------------------
+# The plain FP32 synthesis (k_synth_fp32) bounds its gate from the stored
+# wrapped prefix rows themselves: y_e = ps[e+1] - ps[e] over the nbins + W - 1
+# columns whose width-W window starts below nbins, an FMA prefix of y^2 with a
+# W-slot ring, and the same margins.  Its gate is max over widths w and starts
+# p < nbins of (ps[p+w] - ps[p]) * rsqrt(w) with ps[nbins+u] = ps[nbins] + ps[u].
+# ---------------------------------------------------------------------------
+def _wrapped_ps(x, wmax):
+    n, nbins = x.shape
+    ps = np.zeros((n, nbins + wmax + 1), F)
+    ps[:, 1:nbins + 1] = np.cumsum(x, axis=1, dtype=F)
+    for u in range(1, wmax + 1):
+        ps[:, nbins + u] = (ps[:, nbins] + ps[:, u]).astype(F)
+    return ps
+
+
+def _plain_gate(ps, nbins, widths):
+    best = np.full(ps.shape[0], -np.inf, F)
+    for w in widths:
+        d = (ps[:, w:w + nbins] - ps[:, :nbins]).astype(F)
+        best = np.maximum(best, (d.max(axis=1) * F(1.0 / np.sqrt(w))).astype(F))
+    return best
+
+
+def _plain_bound(ps, nbins, W):
+    n = ps.shape[0]
+    ne = nbins + W - 1
+    y = (ps[:, 1:ne + 1] - ps[:, :ne]).astype(F)
+    q = np.zeros((n, ne + 1), F)
+    for e in range(ne):
+        q[:, e + 1] = _fma32(y[:, e], y[:, e], q[:, e])
+    d = (q[:, W:] - q[:, :-W]).astype(F)     # windows starting at p = 0 .. nbins - 1
+    mx = d.max(axis=1)
+    qt = q[:, ne]
+    a = np.sqrt((mx + qt * F(2.0 ** -13)).astype(F)).astype(F)
+    b = (F(2.0 ** -13) * np.sqrt((F(nbins + W) * qt).astype(F)).astype(F)).astype(F)
+    return ((a + b).astype(F) * F(1.0 + 2.0 ** -16)).astype(F)
+
+
+@pytest.mark.parametrize("kind", ["noise", "pulse", "offset", "alternating", "tiny", "huge"])
+@pytest.mark.parametrize("widths,nbins", [(LADDER_BASE, 120), (LADDER_DEEP, 60), (LADDER_DEEP, 20),
+                                          ([1, 2, 3, 4, 6, 8], 64)])
+def test_plain_energy_bound_covers_the_fp32_gate(kind, widths, nbins):
+    rng = np.random.default_rng(zlib.crc32(f"plain-{kind}-{nbins}".encode()))
+    x = _profiles(kind, 4000, nbins, rng)
+    W = max(widths)
+    ps = _wrapped_ps(x, W)
+    g = _plain_gate(ps, nbins, widths)
+    B = _plain_bound(ps, nbins, W)
+    assert np.all(np.isfinite(B))
+    assert np.all(g <= B), (kind, float(np.max(g - B)))
+
+
+def test_plain_energy_bound_prunes_noise():
+    rng = np.random.default_rng(8)
+    x = _profiles("noise", 20000, 120, rng)
+    B = _plain_bound(_wrapped_ps(x, 6), 120, 6)
+    assert np.mean(B < 6.0) > 0.99

@@ -100,3 +100,20 @@ def test_truncated_spectrum_vs_port(tmp_path):
     # the 150.7 Hz pulsar's upper harmonics lie past the cut: the row guard
     # zeroes them, yet the fundamental is still found
     assert np.any(np.abs(dev["freq"] - 150.7) < 0.05)
+
+
+def test_batch_of_fft_files_from_disk(tmp_path):
+    """Several PRESTO files of uneven length, opened as memory maps and
+    searched as one batch (copies from the maps overlapped with the searches):
+    each file's candidates equal its own search's."""
+    from cohsearch import synth
+    params = cs.SearchParams(nharms=32, m=16, decimations=cs.decimation_set(32, 4), threshold=7.0, synth="fp16")
+    fts = []
+    for i, nsamp in enumerate([1 << 19, 1 << 20, 1 << 18]):
+        amps = synth.make_spectrum(nsamp, 64e-6, [synth.Pulsar(9.0 + 5.0 * i, 0.05, 30.0, 0.3)], 300 + i)
+        fts.append(cs.FFTFile(cs.write_fft(str(tmp_path / f"dm{i}"), amps, nsamp, 64e-6)))
+    assert all(isinstance(ft.amps, np.memmap) for ft in fts)
+    batch = cs.search_batch(fts, params, lofreq=1.0, hifreq=60.0, threshold=7.0)
+    for ft, got in zip(fts, batch):
+        want = cs.search(ft, params, lofreq=1.0, hifreq=60.0, threshold=7.0)
+        assert want and [(c.r, c.metric, c.nharm) for c in got] == [(c.r, c.metric, c.nharm) for c in want]

@@ -97,8 +97,20 @@ def _numpy_stats(eng, N, dt, ms, params, lofreq, hifreq, blocksize):
     tm = tm.reshape(nblk, nlev, blocksize)
     nv = nv.reshape(nblk, nlev)
     total = int(math.floor((hifreq * T - r_lo) / lodr)) + 1
-    edges = {h.k: [w.flo for w in sorted([x for x in ms.whists if x.k == h.k], key=lambda x: x.win)] + [h.fhi]
-             for h in ms.hists}
+    # window edges by the reference rule (_logedges, src/search.jl:1405-1411),
+    # restated here; the device's histograms must carry the same edges
+    r_hi = hifreq * T
+
+    def logedges(a, b, nwin):
+        a = max(float(a), np.finfo(np.float64).tiny)
+        b = max(float(b), a * (1 + 1e-9))
+        la, lb = math.log10(a), math.log10(b)
+        return [10.0 ** (la + (lb - la) * i / nwin) for i in range(nwin + 1)]
+
+    edges = {h.k: logedges(h.k * r_lo / T, h.k * r_hi / T, ms.nwin) for h in ms.hists}
+    for h in ms.hists:
+        dev = [w.flo for w in sorted([x for x in ms.whists if x.k == h.k], key=lambda x: x.win)] + [h.fhi]
+        assert np.allclose(dev, edges[h.k], rtol=1e-13, atol=0.0)
     invw = ms.hist_nb / (ms.hist_hi - ms.hist_lo)
     blocks, hist = [], {}
     for c in range(nblk):

@@ -19,8 +19,6 @@ constexpr int kTileTrials = 64;    // trials per CTA in the FP32 synthesis kerne
 constexpr int kATileBytes = 128 * 128 * 2;  // one 16-bit A tile: 128 trials x 128 K
 constexpr int kSampStride = kSigmaCap / 2;  // float2 per (block, level) in `samp`
 constexpr int kSigmaThreads = 384;          // k_sigma CTA: one pass over a level's synthesis tasks
-constexpr int kSigmaKeyShift = 19;          // k_sigma median buckets: the top 12 bits of |x| (sign bit 0)
-constexpr int kSigmaBins = 1 << (31 - kSigmaKeyShift);
 
 // One harmonic's rational trial-grid recipe (DirectPlan, src/directinterp.jl:179-204).
 // Global trial t of the search evaluates harmonic h at Fourier frequency

@@ -1003,63 +1003,6 @@ __device__ uint32_t radix_select(const uint32_t* vals, int ns, int kth, uint32_t
     return prefix;
 }
 
-// k-th smallest (0-based, k < n) of n values given as bit patterns, by one
-// warp: radix passes of at most 11 bits over bits top..0, in a histogram of
-// 2048 bins that belongs to the warp.  prefix/mask: bits every value is known
-// to share (above `top`).
-__device__ uint32_t warp_select(const uint32_t* vals, int n, int kth, uint32_t* hist, uint32_t prefix, uint32_t mask,
-                                int top) {
-    const int lane = threadIdx.x & 31;
-    int kk = kth;
-    for (int hi = top; hi >= 0;) {
-        const int nbits = hi + 1 < 11 ? hi + 1 : 11;
-        const int shift = hi + 1 - nbits;
-        const int nb = 1 << nbits;
-        for (int i = lane; i < nb; i += 32) hist[i] = 0;
-        __syncwarp();
-        for (int i = lane; i < n; i += 32) {
-            const uint32_t v = vals[i];
-            if ((v & mask) == prefix) atomicAdd(&hist[(v >> shift) & (uint32_t)(nb - 1)], 1u);
-        }
-        __syncwarp();
-        // each lane sums a run of ceil(nb/32) bins; a warp scan locates rank kk
-        const int per = (nb + 31) / 32;
-        const int b0 = min(nb, lane * per), b1 = min(nb, b0 + per);
-        int local = 0;
-        for (int b = b0; b < b1; ++b) local += (int)hist[b];
-        int incl = local;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        const int excl = incl - local;
-        const unsigned who = __ballot_sync(0xffffffffu, excl <= kk && kk < incl);
-        const int src = who ? __ffs(who) - 1 : 0;
-        int bsel = 0, knew = 0;
-        if (lane == src && who) {
-            int c = excl;
-            for (int b = b0; b < b1; ++b) {
-                const int hb = (int)hist[b];
-                if (c + hb > kk) {
-                    bsel = b;
-                    knew = kk - c;
-                    break;
-                }
-                c += hb;
-            }
-        }
-        bsel = __shfl_sync(0xffffffffu, bsel, src);
-        knew = __shfl_sync(0xffffffffu, knew, src);
-        prefix |= (uint32_t)bsel << shift;
-        mask |= (uint32_t)(nb - 1) << shift;
-        kk = knew;
-        hi = shift - 1;
-        __syncwarp();
-    }
-    return prefix;
-}
-
 // One CTA per (block, level).  The columns _block_sigma pools
 // (src/search.jl:528-537): every valid column when nbins*nv <= 8192, else ncol
 // whole columns spaced evenly.  k_interp leaves their exact FP32 amplitudes in
@@ -1086,10 +1029,9 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
     const int ncs = all ? nv : min(nv, max(1, kSigmaCap / nbins));
     const int ns = ncs * nbins;
     float2* Xs = reinterpret_cast<float2*>(ss4);                    // [Hk][ncs], <= kSampStride
-    uint32_t* lst = reinterpret_cast<uint32_t*>(ss4);               // reuses Xs once profiles exist
+    uint32_t* hist = reinterpret_cast<uint32_t*>(ss4);              // reuses Xs once profiles exist
     uint32_t* vals = reinterpret_cast<uint32_t*>(Xs + kSampStride);  // [ns]
-    uint32_t* hist = vals + kSigmaCap;                              // [kSigmaBins]
-    float* tws = reinterpret_cast<float*>(hist + kSigmaBins);       // the level's C2 then S2 rows
+    float* tws = reinterpret_cast<float*>(vals + kSigmaCap);        // the level's C2 then S2 rows
     const float* C2 = tws;
     const float* S2 = tws + Hk * np;
     const float2* samp = a.samp + (int64_t)bl * kSampStride;
@@ -1100,7 +1042,6 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
         mbar_init(&never, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = threadIdx.x; i < kSigmaBins; i += blockDim.x) hist[i] = 0;
     __syncthreads();
     if (threadIdx.x == 0) {
         // the level's twiddle rows come along (2*Hk*np floats, a multiple of 64 bytes)
@@ -1174,95 +1115,42 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
         }
     }
     __syncthreads();
-    // The exact median (_median!, src/search.jl:295-305: the central value, or
-    // the mean of the two central ones).  |x| >= 0 orders like its bit
-    // pattern.  One pass counts the values per bucket of their top 12 bits
-    // (exponent and 4 mantissa bits; warp-aggregated shared atomics), a scan
-    // finds the buckets of the central ranks, their values are gathered into
-    // a short list, and one warp selects within it.
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int half = ns >> 1;
-    const int r0 = (ns & 1) ? half : half - 1;   // the lower central rank; half is the upper
-    // (whole warps run every round of these two loops: the warp intrinsics
-    // see all 32 lanes; blockDim.x is a multiple of 32)
-    for (int i0 = 0; i0 < ns; i0 += blockDim.x) {
-        const int i = i0 + (int)threadIdx.x;
-        const uint32_t key = i < ns ? vals[i] >> kSigmaKeyShift : 0xFFFFFFFFu;
-        const unsigned peers = __match_any_sync(0xffffffffu, key);
-        if (i < ns && lane == __ffs(peers) - 1) atomicAdd(&hist[key], (uint32_t)__popc(peers));
-    }
-    __syncthreads();
-    {
-        const int per = (kSigmaBins + (int)blockDim.x - 1) / (int)blockDim.x;
-        const int b0 = min(kSigmaBins, (int)threadIdx.x * per), b1 = min(kSigmaBins, b0 + per);
-        int local = 0;
-        for (int b = b0; b < b1; ++b) local += (int)hist[b];
-        const int excl = block_excl_scan(local, wtot, sh + 2);
-        // sh[0] / sh[1]: buckets of ranks r0 / half; red[0]: values below bucket sh[0]
-        for (int q = 0; q < 2; ++q) {
-            const int r = q ? half : r0;
-            if (excl <= r && r < excl + local) {
-                int c = excl;
-                for (int b = b0; b < b1; ++b) {
-                    const int hb = (int)hist[b];
-                    if (c + hb > r) {
-                        sh[q] = b;
-                        if (q == 0) red[0] = (uint32_t)c;
-                        break;
-                    }
-                    c += hb;
-                }
-            }
-        }
-        if (threadIdx.x == 0) red[1] = 0;   // list length
-    }
-    __syncthreads();
-    const uint32_t blo = (uint32_t)sh[0], bhi = (uint32_t)sh[1];
-    for (int i0 = 0; i0 < ns; i0 += blockDim.x) {
-        const int i = i0 + (int)threadIdx.x;
-        const uint32_t v = i < ns ? vals[i] : 0xFFFFFFFFu;
-        const uint32_t key = v >> kSigmaKeyShift;
-        const bool in = i < ns && key >= blo && key <= bhi;
-        const unsigned bal = __ballot_sync(0xffffffffu, in);
-        if (bal) {   // warp-uniform
-            const int leader = __ffs(bal) - 1;
-            uint32_t base = 0;
-            if (lane == leader) base = atomicAdd(&red[1], (uint32_t)__popc(bal));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (in) lst[base + __popc(bal & ((1u << lane) - 1u))] = v;
-        }
-    }
-    __syncthreads();
-    if (wid != 0) return;
-    const int nl = (int)red[1];
-    const int below = (int)red[0];
-    // one bucket: the list shares bits 31..19 and the select runs over 18..0
-    const bool one = blo == bhi;
-    const uint32_t lo = warp_select(lst, nl, r0 - below, hist, one ? blo << kSigmaKeyShift : 0u,
-                                    one ? ~((1u << kSigmaKeyShift) - 1u) : 0u, one ? kSigmaKeyShift - 1 : 31);
-    float med = __uint_as_float(lo);
-    if (!(ns & 1)) {
-        // the upper central value: lo again, or the least value above it (in the list)
+    float med;
+    if (ns & 1) {
+        med = __uint_as_float(radix_select(vals, ns, half, hist, sh, wtot));
+    } else {
+        // _median! (src/search.jl:295-305): mean of the two central order statistics.
+        const uint32_t lo = radix_select(vals, ns, half - 1, hist, sh, wtot);
         int le = 0;
         uint32_t above = 0xFFFFFFFFu;
-        for (int i = lane; i < nl; i += 32) {
-            const uint32_t v = lst[i];
+        for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+            const uint32_t v = vals[i];
             le += v <= lo;
             if (v > lo && v < above) above = v;
         }
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             le += __shfl_xor_sync(0xffffffffu, le, o);
             above = min(above, __shfl_xor_sync(0xffffffffu, above, o));
         }
-        const uint32_t hi = below + le >= half + 1 ? lo : above;
-        med = 0.5f * (__uint_as_float(lo) + __uint_as_float(hi));
+        if (lane == 0) { wtot[wid] = le; red[wid] = above; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int tle = 0;
+            uint32_t tab = 0xFFFFFFFFu;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tle += wtot[w]; tab = min(tab, red[w]); }
+            sh[3] = (int)(tle >= half + 1 ? lo : tab);
+        }
+        __syncthreads();
+        med = 0.5f * (__uint_as_float(lo) + __uint_as_float((uint32_t)sh[3]));
     }
-    if (lane == 0) a.sigma[bl] = 1.4826f * med;
+    if (threadIdx.x == 0) a.sigma[bl] = 1.4826f * med;
 }
 
 size_t sigma_smem(int max_hk, int max_np) {
-    return (size_t)kSampStride * sizeof(float2) + (size_t)(kSigmaCap + kSigmaBins) * sizeof(uint32_t) +
+    return (size_t)kSampStride * sizeof(float2) + (size_t)kSigmaCap * sizeof(uint32_t) +
            (size_t)2 * max_hk * max_np * sizeof(float);
 }
 

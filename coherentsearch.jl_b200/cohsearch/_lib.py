@@ -101,9 +101,11 @@ class cs_adam_param(ctypes.Structure):
 
 
 class cs_tune_report(ctypes.Structure):
-    _fields_ = [("interp_kernel", ctypes.c_int32), ("tc_double_buffer", ctypes.c_int32),
+    _fields_ = [("interp_kernel", ctypes.c_int32), ("sigma_kernel", ctypes.c_int32),
+                ("tc_double_buffer", ctypes.c_int32),
                 ("tc_div", ctypes.c_int32 * 2), ("nlev", ctypes.c_int32), ("nbins", ctypes.c_int32 * CS_MAX_DECIM),
                 ("units", ctypes.c_int32 * CS_MAX_DECIM), ("ms_interp", ctypes.c_double * 2),
+                ("ms_sigma", ctypes.c_double * 2),
                 ("ms_synth_model", ctypes.c_double), ("ms_synth_tuned", ctypes.c_double),
                 ("sample_blocks", ctypes.c_int64)]
 

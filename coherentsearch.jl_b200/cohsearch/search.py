@@ -364,6 +364,8 @@ class Engine:
                                         int(nsample), ctypes.byref(r)), self._h, "cs_autotune")
         n = r.nlev
         return {"interp_kernel": "persistent" if r.interp_kernel else "per-item",
+                "sigma_kernel": "256 threads, twiddles via L1" if r.sigma_kernel else "384 threads, twiddles in smem",
+                "ms_sigma": list(r.ms_sigma),
                 "tc_double_buffer": bool(r.tc_double_buffer), "tc_div": list(r.tc_div),
                 "units_per_level": {int(r.nbins[i]): int(r.units[i]) for i in range(n)},
                 "ms_interp": {"per-item": r.ms_interp[0], "persistent": r.ms_interp[1]},

@@ -319,6 +319,8 @@ struct cs_handle {
     int tune_interp = -1;
     int tune_div[2] = {0, 0};
     int tune_dbuf = 1;
+    int tune_sigma = 0;
+    double stats_sigma_min = 0.0;   // cs_autotune: least sigma-stage time of its last timed configuration     // block-sigma kernel: 0 = 384 threads, twiddles in shared memory; 1 = 256, through L1
     bool interp2_used = false, interp2_ok = false;   // the last search's interpolation kernel / its applicability
     int64_t stall_ns = 0;   // cs_set_wait_test
     int last_nlev = 0;
@@ -840,7 +842,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             // sigma needs only the samples, so it runs first and the synthesis
             // epilogue applies the medcut test itself (no gate pass over HBM);
             // exact_all scores every trial exactly and needs no gate at all
-            CS_CUDA(launch_sigma(a, H->stream, max_hk, max_np, d_err), "sigma launch");
+            CS_CUDA(launch_sigma(a, H->stream, max_hk, max_np, d_err, H->tune_sigma), "sigma launch");
             if (!R.capture) CS_CUDA(cudaEventRecord(H->ev[2], H->stream), "event");
             S.launches += 1;
             if (!R.exact_all) {
@@ -1030,7 +1032,7 @@ namespace {
 struct TuneEntry {
     int device;
     cs_params p;
-    int interp, div0, div1, dbuf;
+    int interp, div0, div1, dbuf, sigma;
 };
 std::mutex g_tune_mu;
 std::vector<TuneEntry> g_tune_cache;
@@ -1087,6 +1089,7 @@ cs_status cs_create(cs_handle** out, const cs_params* params, int32_t device) {
         H->tune_div[0] = te.div0;
         H->tune_div[1] = te.div1;
         H->tune_dbuf = te.dbuf;
+        H->tune_sigma = te.sigma;
         if (H->p.synth != CS_SYNTH_FP32) st = build_tc(H);
     }
     if (st != CS_OK) {
@@ -1842,7 +1845,7 @@ cs_status cs_autotune(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
     // stage times of one configuration: the least of 3 runs after a warm-up
     auto timed = [&](double* ms_i, double* ms_s) -> cs_status {
         std::vector<cs_candidate> c;
-        double bi = 1e300, bs = 1e300;
+        double bi = 1e300, bs = 1e300, bg = 1e300;
         for (int r = 0; r < 4; ++r) {
             c.clear();
             const cs_status e = search_core(H, lofreq, hifreq, lobin, blocksize, H->p.threshold, 0, b0, b0 + ns, &c);
@@ -1850,8 +1853,10 @@ cs_status cs_autotune(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
             if (r > 0) {
                 bi = std::min(bi, H->stats.ms_interp);
                 bs = std::min(bs, H->stats.ms_synth);
+                bg = std::min(bg, H->stats.ms_sigma);
             }
         }
+        H->stats_sigma_min = bg;
         *ms_i = bi;
         *ms_s = bs;
         return CS_OK;
@@ -1875,7 +1880,16 @@ cs_status cs_autotune(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
         rep.ms_interp[0] = msi;
     }
     if (st == CS_OK) H->tune_interp = (rep.ms_interp[1] >= 0.0 && rep.ms_interp[1] < rep.ms_interp[0]) ? 1 : 0;
-    // 2. tensor epilogue: segment divisor of each phase, then one or two base-level slots
+    // 2. the block-sigma kernel
+    rep.ms_sigma[0] = rep.ms_sigma[1] = -1.0;
+    for (int v = 0; v < 2 && st == CS_OK; ++v) {
+        H->tune_sigma = v;
+        double a_ = 0.0, b_ = 0.0;
+        st = timed(&a_, &b_);
+        rep.ms_sigma[v] = H->stats_sigma_min;
+    }
+    if (st == CS_OK) H->tune_sigma = rep.ms_sigma[1] < rep.ms_sigma[0] ? 1 : 0;
+    // 3. tensor epilogue: segment divisor of each phase, then one or two base-level slots
     if (st == CS_OK && tensor) {
         int best[3] = {0, 0, 1};   // div0, div1, dbuf
         double best_ms = ms_model;
@@ -1895,7 +1909,7 @@ cs_status cs_autotune(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
             }
             return CS_OK;
         };
-        const int divs[] = {4, 5, 6, 8, 10, 12, 16};
+        const int divs[] = {2, 3, 4, 5, 6, 8, 10, 12, 16};
         if (H->dlev.size() > 1)
             for (int d : divs)
                 if (st == CS_OK) st = trial(d, best[1], best[2]);
@@ -1917,6 +1931,7 @@ cs_status cs_autotune(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
     H->diag = diag;
     if (st != CS_OK) return st;
     rep.interp_kernel = H->tune_interp;
+    rep.sigma_kernel = H->tune_sigma;
     rep.tc_double_buffer = tensor ? H->tc.args.dbuf : 0;
     rep.tc_div[0] = tensor ? H->tune_div[0] : 0;
     rep.tc_div[1] = tensor ? H->tune_div[1] : 0;
@@ -1925,7 +1940,7 @@ cs_status cs_autotune(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
         rep.nbins[l] = H->dlev[l].nbins;
         rep.units[l] = tensor ? H->tc.args.lev[l].nunits : 0;
     }
-    tune_store({H->device, H->p, H->tune_interp, H->tune_div[0], H->tune_div[1], H->tune_dbuf});
+    tune_store({H->device, H->p, H->tune_interp, H->tune_div[0], H->tune_div[1], H->tune_dbuf, H->tune_sigma});
     if (out) *out = rep;
     return CS_OK;
 }

@@ -198,7 +198,7 @@ struct TcPlanHost {
 
 // Returns 0, or < 0 when the configuration does not fit the tensor path.
 // div0/div1 (> 0): the epilogue segment divisor of phase 0 / 1 instead of the
-// cost model's choice (one of 4, 5, 6, 8, 10, 12, 16); allow_dbuf = 0: one
+// cost model's choice (one of 2, 3, 4, 5, 6, 8, 10, 12, 16); allow_dbuf = 0: one
 // base-level TMEM slot.
 int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, TcPlanHost* out, int div0 = 0,
                int div1 = 0, int allow_dbuf = 1);
@@ -345,9 +345,10 @@ cudaError_t launch_interp(const WaveArgs& a, cudaStream_t st, int win_max, int* 
 cudaError_t launch_interp2(const WaveArgs& a, cudaStream_t st, int win_max, int* err, int num_sms);
 size_t interp2_smem(int win_max, int Nprof);
 cudaError_t launch_synth_fp32(const WaveArgs& a, cudaStream_t st, int smem_bytes);
-size_t sigma_smem(int max_hk, int max_np);
+// variant 0: 384 threads, twiddles in shared memory; 1: 256 threads, twiddles through L1
+size_t sigma_smem(int max_hk, int max_np, int variant = 0);
 size_t interp_smem(int win_max, int Nprof);
-cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np, int* err);
+cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np, int* err, int variant = 0);
 cudaError_t launch_rescue(const WaveArgs& a, cudaStream_t st, int num_sms);
 cudaError_t launch_mstats(const WaveArgs& a, cudaStream_t st);
 // the largest |Re| or |Im| of the spectrum, as float bits, into *out (zeroed by the caller)

@@ -1009,7 +1009,12 @@ __device__ uint32_t radix_select(const uint32_t* vals, int ns, int kth, uint32_t
 // `samp`; their profiles are built here with synth_chunk8 -- the arithmetic of
 // the FP32 synthesis and of the rescan -- so sigma is identical in every
 // synthesis mode.  sigma = 1.4826 * median(|x|), _median! semantics.
-__global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err) {
+// Two forms, picked by the autotuner: NT = 384 threads with the level's
+// twiddle rows copied into shared memory beside the samples (two CTAs per SM),
+// or NT = 256 with the twiddles read through L1 from global memory (less
+// shared memory: three CTAs per SM).  Same arithmetic, same sigma.
+template <int NT, bool TWS>
+__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 2) k_sigma(WaveArgs a, int* err) {
     extern __shared__ float4 ss4[];
     __shared__ int sh[4];
     __shared__ int wtot[32];
@@ -1031,9 +1036,9 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
     float2* Xs = reinterpret_cast<float2*>(ss4);                    // [Hk][ncs], <= kSampStride
     uint32_t* hist = reinterpret_cast<uint32_t*>(ss4);              // reuses Xs once profiles exist
     uint32_t* vals = reinterpret_cast<uint32_t*>(Xs + kSampStride);  // [ns]
-    float* tws = reinterpret_cast<float*>(vals + kSigmaCap);        // the level's C2 then S2 rows
-    const float* C2 = tws;
-    const float* S2 = tws + Hk * np;
+    float* tws = reinterpret_cast<float*>(vals + kSigmaCap);        // the level's C2 then S2 rows (TWS)
+    const float* C2 = TWS ? tws : a.tw + L.tw_off;
+    const float* S2 = C2 + Hk * np;
     const float2* samp = a.samp + (int64_t)bl * kSampStride;
     // The samples arrive by one bulk copy (rounded up to 16 bytes, still inside
     // this (block, level)'s kSampStride slot) instead of dependent loads.
@@ -1046,10 +1051,10 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
     if (threadIdx.x == 0) {
         // the level's twiddle rows come along (2*Hk*np floats, a multiple of 64 bytes)
         const uint32_t xb = (uint32_t)((Hk * ncs * (int)sizeof(float2) + 15) & ~15);
-        const uint32_t tb = (uint32_t)(2 * Hk * np * (int)sizeof(float));
+        const uint32_t tb = TWS ? (uint32_t)(2 * Hk * np * (int)sizeof(float)) : 0u;
         mbar_expect_tx(&sbar, xb + tb);
         bulk_copy(smem_u32(Xs), samp, xb, &sbar);
-        bulk_copy(smem_u32(tws), a.tw + L.tw_off, tb, &sbar);
+        if (TWS) bulk_copy(smem_u32(tws), a.tw + L.tw_off, tb, &sbar);
     }
     if (__syncthreads_or(!mbar_wait(&sbar, 0))) {
         // give up (every thread alike) with an error status, after the copy in
@@ -1149,15 +1154,20 @@ __global__ void __launch_bounds__(kSigmaThreads, 2) k_sigma(WaveArgs a, int* err
     if (threadIdx.x == 0) a.sigma[bl] = 1.4826f * med;
 }
 
-size_t sigma_smem(int max_hk, int max_np) {
+size_t sigma_smem(int max_hk, int max_np, int variant) {
     return (size_t)kSampStride * sizeof(float2) + (size_t)kSigmaCap * sizeof(uint32_t) +
-           (size_t)2 * max_hk * max_np * sizeof(float);
+           (variant == 1 ? 0 : (size_t)2 * max_hk * max_np * sizeof(float));
 }
 
-cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np, int* err) {
-    const size_t smem = sigma_smem(max_hk, max_np);
-    cudaFuncSetAttribute(k_sigma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_sigma<<<a.nblk * a.nlev, kSigmaThreads, smem, st>>>(a, err);
+cudaError_t launch_sigma(const WaveArgs& a, cudaStream_t st, int max_hk, int max_np, int* err, int variant) {
+    const size_t smem = sigma_smem(max_hk, max_np, variant);
+    if (variant == 1) {
+        cudaFuncSetAttribute(k_sigma<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_sigma<256, false><<<a.nblk * a.nlev, 256, smem, st>>>(a, err);
+    } else {
+        cudaFuncSetAttribute(k_sigma<kSigmaThreads, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_sigma<kSigmaThreads, true><<<a.nblk * a.nlev, kSigmaThreads, smem, st>>>(a, err);
+    }
     return cudaGetLastError();
 }
 

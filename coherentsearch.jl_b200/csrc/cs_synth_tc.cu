@@ -613,7 +613,7 @@ int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, Tc
             int best_wg[kMaxUnits], wg_of[kMaxUnits];
             int best_nu = 0;
             double best_load = 0.0;
-            for (int div : {4, 5, 6, 8, 10, 12, 16}) {
+            for (int div : {2, 3, 4, 5, 6, 8, 10, 12, 16}) {
                 const int forced = ph ? div1 : div0;   // a tuned divisor replaces the search
                 if (forced > 0 && div != forced) continue;
                 double ml = 0.0;

@@ -399,12 +399,14 @@ cs_status cs_search_trial_metrics(const cs_handle* h, float* out, int64_t cap, i
 /* What cs_autotune chose, and the stage times it measured on its sample. */
 typedef struct cs_tune_report {
     int32_t interp_kernel;        /* 1: persistent kernel with bulk-copied windows; 0: one CTA per item */
+    int32_t sigma_kernel;         /* block sigma: 0 = 384 threads, twiddles in shared memory; 1 = 256, via L1 */
     int32_t tc_double_buffer;     /* tensor modes: 1 = base level in two TMEM slots */
     int32_t tc_div[2];            /* epilogue segment divisor of each phase (0: FP32 synthesis) */
     int32_t nlev;                 /* decimation levels */
     int32_t nbins[CS_MAX_DECIM];  /* profile bins of each level, in level order */
     int32_t units[CS_MAX_DECIM];  /* epilogue work units (start segments) of each level */
     double ms_interp[2];          /* interpolation stage time of kernel 0 / 1 (-1: not applicable) */
+    double ms_sigma[2];           /* block-sigma stage time of kernel 0 / 1 */
     double ms_synth_model;        /* synthesis stage time with the cost model's plan */
     double ms_synth_tuned;        /* ... with the chosen plan */
     int64_t sample_blocks;        /* blocks of the timed sample */
@@ -412,8 +414,8 @@ typedef struct cs_tune_report {
 
 /* Autotune the handle's launch shapes on its attached spectrum: a sample of
  * nsample blocks from the middle of the band [lofreq, hifreq] (arguments as
- * cs_search) is searched with each candidate -- the interpolation kernel, and
- * in the tensor modes the epilogue segment size of each phase per profile bin
+ * cs_search) is searched with each candidate -- the interpolation kernel, the
+ * block-sigma kernel, and in the tensor modes the epilogue segment size of each phase per profile bin
  * count and the base level's TMEM double buffer -- timed with CUDA events
  * (the least of 3 runs after a warm-up), and the fastest kept on the handle.
  * Every candidate computes the same values, so candidates are unchanged.  The

@@ -138,6 +138,7 @@ PROTOTYPES = {
     "cs_search_trial_metrics": (_i32, [_P, _P, _i64, ctypes.POINTER(_i64)]),
     "cs_set_diagnostics": (_i32, [_P, _i32]),
     "cs_set_memory_limit": (_i32, [_P, _i64]),
+    "cs_set_launch_shapes": (_i32, [_P, ctypes.POINTER(cs_tune_report)]),
     "cs_autotune": (_i32, [_P, _f64, _f64, _i64, _i64, _i64, ctypes.POINTER(cs_tune_report)]),
     "cs_set_wait_test": (_i32, [_P, _i64]),
     "cs_search_gate_values": (_i32, [_P, _P, _i64, ctypes.POINTER(_i64)]),

@@ -372,6 +372,16 @@ class Engine:
                 "ms_synth_model": r.ms_synth_model, "ms_synth_tuned": r.ms_synth_tuned,
                 "sample_blocks": int(r.sample_blocks)}
 
+    def set_launch_shapes(self, interp_kernel=0, sigma_kernel=0, tc_double_buffer=1, tc_div=(0, 0)):
+        """Pin the launch shapes (cs_set_launch_shapes): interpolation kernel 0
+        (one CTA per item) or 1 (persistent), block-sigma kernel 0 (384 threads)
+        or 1 (256), the base level's TMEM double buffer, and the epilogue
+        segment divisor per phase (0: cost model)."""
+        r = _lib.cs_tune_report()
+        r.interp_kernel, r.sigma_kernel, r.tc_double_buffer = int(interp_kernel), int(sigma_kernel), int(tc_double_buffer)
+        r.tc_div[0], r.tc_div[1] = int(tc_div[0]), int(tc_div[1])
+        _lib.check(self.lib.cs_set_launch_shapes(self._h, ctypes.byref(r)), self._h, "cs_set_launch_shapes")
+
     def set_memory_limit(self, nbytes: int):
         """Cap the device memory the engine holds (0: no cap); searches split
         into waves under it, or raise CohSearchError(CS_ERR_OUT_OF_MEMORY)."""

@@ -1945,6 +1945,23 @@ cs_status cs_autotune(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
     return CS_OK;
 }
 
+cs_status cs_set_launch_shapes(cs_handle* H, const cs_tune_report* sh) {
+    if (!H || !sh) return CS_ERR_INVALID_ARGUMENT;
+    auto div_ok = [](int d) { return d == 0 || d == 2 || d == 3 || d == 4 || d == 5 || d == 6 || d == 8 || d == 10 ||
+                                     d == 12 || d == 16; };
+    if ((sh->interp_kernel != 0 && sh->interp_kernel != 1) || (sh->sigma_kernel != 0 && sh->sigma_kernel != 1) ||
+        (sh->tc_double_buffer != 0 && sh->tc_double_buffer != 1) || !div_ok(sh->tc_div[0]) || !div_ok(sh->tc_div[1]))
+        return fail(H, CS_ERR_INVALID_ARGUMENT, "launch shapes out of range");
+    CS_CUDA(cudaSetDevice(H->device), "set device");
+    H->tune_interp = sh->interp_kernel;
+    H->tune_sigma = sh->sigma_kernel;
+    H->tune_dbuf = sh->tc_double_buffer;
+    H->tune_div[0] = sh->tc_div[0];
+    H->tune_div[1] = sh->tc_div[1];
+    H->graph_valid = false;
+    return H->p.synth != CS_SYNTH_FP32 ? build_tc(H) : CS_OK;
+}
+
 cs_status cs_set_memory_limit(cs_handle* H, int64_t bytes) {
     if (!H || bytes < 0) return CS_ERR_INVALID_ARGUMENT;
     CS_CUDA(cudaSetDevice(H->device), "set device");

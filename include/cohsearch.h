@@ -425,6 +425,13 @@ typedef struct cs_tune_report {
 cs_status cs_autotune(cs_handle* h, double lofreq, double hifreq, int64_t lobin, int64_t blocksize, int64_t nsample,
                       cs_tune_report* out);
 
+/* Apply launch shapes chosen earlier (a cs_autotune report, e.g. stored by a
+ * pipeline at its first run): interp_kernel, sigma_kernel, tc_double_buffer
+ * and tc_div are read; the other fields are ignored.  tc_div entries are 0
+ * (the cost model's choice) or one of 2, 3, 4, 5, 6, 8, 10, 12, 16.  Every
+ * shape computes the same values.  No counterpart in the reference. */
+cs_status cs_set_launch_shapes(cs_handle* h, const cs_tune_report* shapes);
+
 /* Cap on the device memory this handle holds (bytes; 0 = no cap, the
  * default).  Searches split their blocks into waves that fit under the cap
  * beside the handle's fixed tables and spectrum; when even one block's

@@ -52,3 +52,26 @@ def test_tuned_search_equals_untuned_and_the_port(synth):
     again = cs.Engine(eng.params)
     again.set_spectrum(cs.FFTFile.from_array(amps, N, dt))
     assert np.array_equal(again.search_raw(band[0], band[1], 100, 2048, 8.0), want)
+
+
+@pytest.mark.parametrize("synth", ["fp16", "bf16_split", "fp32"])
+def test_every_launch_shape_gives_the_same_records(synth):
+    """Each kernel form and epilogue plan the tuner can choose, pinned by
+    cs_set_launch_shapes: identical records and block sigmas."""
+    band = (0.2, 120.0)
+    ref, _, _, _ = _engine(synth)
+    ref.set_launch_shapes(0, 0, 0, (0, 0))
+    want = ref.search_raw(band[0], band[1], 100, 2048, 8.0)
+    wsig, wnv = ref.block_values()
+    assert len(want) > 0
+    shapes = [(1, 0, 1, (0, 0)), (0, 1, 1, (4, 4)), (1, 1, 0, (2, 0)), (0, 0, 1, (16, 3)), (1, 1, 1, (8, 12))]
+    for sh in shapes:
+        eng, _, _, _ = _engine(synth)
+        eng.set_launch_shapes(*sh)
+        got = eng.search_raw(band[0], band[1], 100, 2048, 8.0)
+        sig, nv = eng.block_values()
+        assert np.array_equal(got, want), sh
+        assert np.array_equal(sig, wsig) and np.array_equal(nv, wnv), sh
+    import cohsearch as cs
+    with pytest.raises(ValueError):
+        ref.set_launch_shapes(0, 0, 1, (7, 0))

@@ -185,13 +185,14 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
         }
     }
     if (!a.samp) return;
-    // One warp per (harmonic, level) pair whose level folds this harmonic;
-    // lanes over its pooled columns j_c = (c*nv) div ncs (src/search.jl:528-537),
-    // the division by ncs done as a multiply-high by ceil(2^64/ncs), exact for
-    // every 32-bit dividend.
-    const int lane = threadIdx.x & 31;
-    const int nwarps = blockDim.x >> 5;
-    for (int e = threadIdx.x >> 5; e < ng * a.nlev; e += nwarps) {
+    // The pooled columns j_c = (c*nv) div ncs (src/search.jl:528-537) of every
+    // (harmonic, level) pair whose level folds the harmonic, all pairs' columns
+    // dealt out over the whole CTA as one index space (consecutive threads on
+    // consecutive columns of a pair).  The division by ncs is a multiply-high
+    // by ceil(2^64/ncs), exact for every 32-bit dividend.
+    const int nthr = (int)blockDim.x;
+    int base = 0;
+    for (int e = 0; e < ng * a.nlev; ++e) {
         const int g = e / a.nlev, l = e - g * a.nlev;
         const int h = hidx0 + g + 1;
         const DevLevel& L = a.levels[l];
@@ -202,15 +203,19 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
         const int ncs = all ? nv : min(nv, max(1, kSigmaCap / L.nbins));
         float2* dst = a.samp + ((int64_t)blk * a.nlev + l) * kSampStride + (int64_t)(h / L.k - 1) * ncs;
         const float2* src = xo + g * Nst;
+        // this thread's first column of the pair: (base + c) % nthr == threadIdx.x
+        int c = ((int)threadIdx.x - base) % nthr;
+        if (c < 0) c += nthr;
         if (all || ncs == 1) {
-            for (int c = lane; c < ncs; c += 32) dst[c] = src[all ? c : 0];
+            for (; c < ncs; c += nthr) dst[c] = src[all ? c : 0];
         } else {
             const uint64_t mg = 0xFFFFFFFFFFFFFFFFull / (uint64_t)ncs + 1ull;
-            for (int c = lane; c < ncs; c += 32) {
+            for (; c < ncs; c += nthr) {
                 const uint32_t x = (uint32_t)c * (uint32_t)nv;   // < 4096 * 65536
                 dst[c] = src[(int)__umul64hi((uint64_t)x, mg)];
             }
         }
+        base += ncs;
     }
 }
 
@@ -352,10 +357,13 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
     __shared__ int s_ok[kHG], s_nw[kHG], s_p0[kHG], s_res0[kHG], s_Ub[kHG], s_chunk[kHG], s_Tc[kHG],
         s_small[kHG], s_Hs[kHG];
     __shared__ long long s_lo[kHG], s_base[kHG];   // s_base = rfloor0 + qint0 - lo + 1 - m2
+    __shared__ unsigned long long s_qm[kHG];       // ceil(2^64 / q): (n div q) = mulhi(n, s_qm) for n < 2^32
+    __shared__ unsigned s_pm[kHG];                 // ceil(2^24 / P): (task div P) for task * P < 2^24
 
-    const int hidx0 = blockIdx.x * kHG;
+    // blocks fastest: the CTAs resident on an SM share a group's weight tables in L1
+    const int hidx0 = blockIdx.y * kHG;
     const int ng = min(kHG, a.nharms - hidx0);
-    const int blk = blockIdx.y;
+    const int blk = blockIdx.x;
     const int m = M > 0 ? M : a.m;
     const int m2 = m / 2;
     const int64_t t0 = blk_t0(a, blk);
@@ -399,8 +407,11 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
             s_Tc[g] = Tc;
             s_chunk[g] = (Ub + 1 + Tc - 1) / Tc;
             // res0 + jc*h*pnum < 2^32 for every class: the window start fits 32-bit math
-            s_small[g] = ((uint64_t)hp.q + (uint64_t)P * (uint64_t)hpn) < 0xFFFFFFFFull;
+            // (q > 1: ceil(2^64/q) must fit 64 bits)
+            s_small[g] = ((uint64_t)hp.q + (uint64_t)P * (uint64_t)hpn) < 0xFFFFFFFFull && hp.q > 1;
             s_Hs[g] = (int)(((int64_t)P * hpn) / hp.q);   // bins between trials t and t+P
+            s_qm[g] = hp.q > 1 ? 0xFFFFFFFFFFFFFFFFull / (uint64_t)hp.q + 1ull : 0ull;
+            s_pm[g] = (unsigned)((((uint64_t)1 << 24) + (uint64_t)P - 1) / (uint64_t)P);
         }
     }
     __syncthreads();
@@ -433,11 +444,12 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
         const long long base = s_base[g];
         const int ntask = P >= (int)blockDim.x ? P : P * Tc;
         const int nlong = n - Ub * P;
-        const float invP = 1.0f / (float)P;
+        const unsigned long long qm = s_qm[g];
+        const unsigned pm = s_pm[g];
         for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
-            // task < 256 when Tc > 1: (task + 0.5)/P is >= 0.5/P from an integer,
-            // far above the float error, so the quotient is exact.
-            const int part = Tc > 1 ? (int)(((float)task + 0.5f) * invP) : 0;
+            // task < 256 and P <= 256 when Tc > 1, so task * P < 2^24 and the
+            // multiply by ceil(2^24/P) gives the exact quotient
+            const int part = Tc > 1 ? (int)(((uint64_t)task * pm) >> 24) : 0;
             const int jc = task - part * P;
             if (jc >= n) continue;
             const int U = Ub + (jc < nlong ? 1 : 0);
@@ -445,7 +457,7 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
             if (u0 >= u1) continue;
             int p = p0 + jc;
             if (p >= P) p -= P;
-            const int64_t qv = small ? (int64_t)(((uint32_t)res0 + (uint32_t)jc * (uint32_t)hpn) / (uint32_t)q)
+            const int64_t qv = small ? (int64_t)__umul64hi((uint64_t)((uint32_t)res0 + (uint32_t)jc * (uint32_t)hpn), qm)
                                      : ((int64_t)res0 + (int64_t)jc * hpn) / q;
             const int b0 = (int)(base + qv + ct[p]);
             const float2 A = __ldg(at + p);
@@ -475,7 +487,9 @@ struct HarmStage {
     int ok;             // 1: computed; 0: zero row
     int head;           // window element 0 sits at stage + head (1 when its address is not 16-byte aligned)
     int p0, res0, Ub, Tc, chunk, small, Hs;
+    unsigned pm;        // ceil(2^24 / P)
     long long base;     // rfloor0 + qint0 - lo + 1 - m2
+    unsigned long long qm;   // ceil(2^64 / q), q > 1
 };
 
 __device__ __forceinline__ int i2_wstride(int win_max) { return (win_max + 3) & ~1; }
@@ -485,7 +499,7 @@ __device__ __forceinline__ int i2_wstride(int win_max) { return (win_max + 3) & 
 __device__ void i2_prepare(const WaveArgs& a, int item, int ngroups, int win_max, float2* stage, HarmStage* st,
                            uint64_t* bar, int* err) {
     const int lane = threadIdx.x & 31;
-    const int blk = item / ngroups, grp = item - blk * ngroups;
+    const int grp = item / a.nblk, blk = item - grp * a.nblk;   // blocks fastest
     const int hidx0 = grp * kHG;
     const int ng = min(kHG, a.nharms - hidx0);
     const int64_t t0 = blk_t0(a, blk);
@@ -530,8 +544,10 @@ __device__ void i2_prepare(const WaveArgs& a, int item, int ngroups, int win_max
         h.Ub = Ub;
         h.Tc = Tc;
         h.chunk = (Ub + 1 + Tc - 1) / Tc;
-        h.small = ((uint64_t)hp.q + (uint64_t)P * (uint64_t)hpn) < 0xFFFFFFFFull;
+        h.small = ((uint64_t)hp.q + (uint64_t)P * (uint64_t)hpn) < 0xFFFFFFFFull && hp.q > 1;
         h.Hs = (int)(((int64_t)P * hpn) / hp.q);   // bins between trials t and t+P
+        h.qm = hp.q > 1 ? 0xFFFFFFFFFFFFFFFFull / (uint64_t)hp.q + 1ull : 0ull;
+        h.pm = (unsigned)((((uint64_t)1 << 24) + (uint64_t)P - 1) / (uint64_t)P);
         st[lane] = h;
     }
     uint32_t total = body_bytes;
@@ -569,7 +585,7 @@ __global__ void __launch_bounds__(kI2Threads, 2) k_interp2(WaveArgs a, int win_m
     if (!ok && threadIdx.x == 0) atomicExch(err, 4);
     for (int it = 0; item < nitems && ok; item += gridDim.x, ++it) {
         const HarmStage* S = st[it & 1];
-        const int blk = item / ngroups, grp = item - blk * ngroups;
+        const int grp = item / a.nblk, blk = item - grp * a.nblk;
         const int hidx0 = grp * kHG;
         const int ng = min(kHG, a.nharms - hidx0);
         const int64_t t0 = blk_t0(a, blk);
@@ -591,11 +607,9 @@ __global__ void __launch_bounds__(kI2Threads, 2) k_interp2(WaveArgs a, int win_m
             const int Tc = h.Tc, Ub = h.Ub, chunk = h.chunk;
             const int ntask = P >= kI2Threads ? P : P * Tc;
             const int nlong = n - Ub * P;
-            const float invP = 1.0f / (float)P;
             for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
-                // task < 256 when Tc > 1: (task + 0.5)/P is >= 0.5/P from an integer,
-                // far above the float error, so the quotient is exact.
-                const int part = Tc > 1 ? (int)(((float)task + 0.5f) * invP) : 0;
+                // task < 256 and P <= 256 when Tc > 1: task * P < 2^24, exact quotient
+                const int part = Tc > 1 ? (int)(((uint64_t)task * h.pm) >> 24) : 0;
                 const int jc = task - part * P;
                 if (jc >= n) continue;
                 const int U = Ub + (jc < nlong ? 1 : 0);
@@ -603,7 +617,7 @@ __global__ void __launch_bounds__(kI2Threads, 2) k_interp2(WaveArgs a, int win_m
                 if (u0 >= u1) continue;
                 int p = h.p0 + jc;
                 if (p >= P) p -= P;
-                const int64_t qv = h.small ? (int64_t)(((uint32_t)h.res0 + (uint32_t)jc * (uint32_t)hpn) / (uint32_t)q)
+                const int64_t qv = h.small ? (int64_t)__umul64hi((uint64_t)((uint32_t)h.res0 + (uint32_t)jc * (uint32_t)hpn), h.qm)
                                            : ((int64_t)h.res0 + (int64_t)jc * hpn) / q;
                 const int b0 = (int)(h.base + qv + ct[p]);
                 const float2 A = __ldg(at + p);
@@ -659,7 +673,7 @@ cudaError_t launch_amax(const float2* amps, int64_t n, uint32_t* out, cudaStream
 size_t interp_smem(int win_max, int Nprof) { return (size_t)(win_max + kHG * Nprof) * sizeof(float2); }
 
 cudaError_t launch_interp(const WaveArgs& a, cudaStream_t st, int win_max, int* err) {
-    dim3 grid((a.nharms + kHG - 1) / kHG, a.nblk);
+    dim3 grid(a.nblk, (a.nharms + kHG - 1) / kHG);
     const size_t smem = interp_smem(win_max, a.Nprof);
     const int Nst = a.Nprof;
     switch (a.m) {
@@ -1003,6 +1017,78 @@ __device__ uint32_t radix_select(const uint32_t* vals, int ns, int kth, uint32_t
     return prefix;
 }
 
+// radix_select with fewer barriers, for the block sigma: two histogram
+// buffers (the next pass's is cleared while this pass counts) and two slots
+// for the scan's warp totals and the pass result, so that nothing written in
+// one pass is overwritten before every thread has read it.  Four barriers per
+// pass.  hist2 holds 2 x 2048 bins; wtot2 2 x 32 ints; sh2 2 x 4 ints.
+__device__ uint32_t radix_select_2buf(const uint32_t* vals, int ns, int kth, uint32_t* hist2, int* sh2, int* wtot2) {
+    uint32_t prefix = 0, mask = 0;
+    int kk = kth;
+    const int shifts[3] = {21, 10, 0};
+    const int bits[3] = {11, 11, 10};
+    const int nthr = (int)blockDim.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < 2048; i += nthr) hist2[i] = 0;
+    __syncthreads();
+    for (int pass = 0; pass < 3; ++pass) {
+        const int shift = shifts[pass], nb = 1 << bits[pass];
+        uint32_t* hist = hist2 + (pass & 1) * 2048;
+        uint32_t* hnext = hist2 + ((pass + 1) & 1) * 2048;
+        int* wtot = wtot2 + (pass & 1) * 32;
+        int* sh = sh2 + (pass & 1) * 4;
+        for (int i = threadIdx.x; i < ns; i += nthr) {
+            const uint32_t v = vals[i];
+            if ((v & mask) == prefix) atomicAdd(&hist[(v >> shift) & (uint32_t)(nb - 1)], 1u);
+        }
+        if (pass < 2)
+            for (int i = threadIdx.x; i < 2048; i += nthr) hnext[i] = 0;
+        __syncthreads();
+        const int per = (nb + nthr - 1) / nthr;
+        const int b0 = min(nb, (int)threadIdx.x * per), b1 = min(nb, b0 + per);
+        int local = 0;
+        for (int b = b0; b < b1; ++b) local += (int)hist[b];
+        // block exclusive scan of `local`
+        int x = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wtot[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            const int w = lane < (nthr >> 5) ? wtot[lane] : 0;
+            int incl = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane < (nthr >> 5)) wtot[lane] = incl - w;
+        }
+        __syncthreads();
+        const int excl = wtot[wid] + x - local;
+        if (excl <= kk && kk < excl + local) {
+            int c = excl;
+            for (int b = b0; b < b1; ++b) {
+                const int hb = (int)hist[b];
+                if (c + hb > kk) {
+                    sh[0] = b;
+                    sh[1] = kk - c;
+                    break;
+                }
+                c += hb;
+            }
+        }
+        __syncthreads();
+        prefix |= (uint32_t)sh[0] << shift;
+        mask |= (uint32_t)(nb - 1) << shift;
+        kk = sh[1];
+    }
+    return prefix;
+}
+
 // One CTA per (block, level).  The columns _block_sigma pools
 // (src/search.jl:528-537): every valid column when nbins*nv <= 8192, else ncol
 // whole columns spaced evenly.  k_interp leaves their exact FP32 amplitudes in
@@ -1018,6 +1104,8 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 2) k_sigma(WaveArgs a, int
     extern __shared__ float4 ss4[];
     __shared__ int sh[4];
     __shared__ int wtot[32];
+    __shared__ int sh2[8];      // radix_select_2buf's two result slots
+    __shared__ int wtot2[64];   // and its two scan slots
     __shared__ uint32_t red[32];
     __shared__ __align__(8) uint64_t sbar;
     __shared__ __align__(8) uint64_t never;   // test hook: a barrier no thread or copy completes
@@ -1034,7 +1122,7 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 2) k_sigma(WaveArgs a, int
     const int ncs = all ? nv : min(nv, max(1, kSigmaCap / nbins));
     const int ns = ncs * nbins;
     float2* Xs = reinterpret_cast<float2*>(ss4);                    // [Hk][ncs], <= kSampStride
-    uint32_t* hist = reinterpret_cast<uint32_t*>(ss4);              // reuses Xs once profiles exist
+    uint32_t* hist = reinterpret_cast<uint32_t*>(ss4);              // 2 x 2048 bins: reuses Xs once profiles exist
     uint32_t* vals = reinterpret_cast<uint32_t*>(Xs + kSampStride);  // [ns]
     float* tws = reinterpret_cast<float*>(vals + kSigmaCap);        // the level's C2 then S2 rows (TWS)
     const float* C2 = TWS ? tws : a.tw + L.tw_off;
@@ -1123,10 +1211,10 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 2) k_sigma(WaveArgs a, int
     const int half = ns >> 1;
     float med;
     if (ns & 1) {
-        med = __uint_as_float(radix_select(vals, ns, half, hist, sh, wtot));
+        med = __uint_as_float(radix_select_2buf(vals, ns, half, hist, sh2, wtot2));
     } else {
         // _median! (src/search.jl:295-305): mean of the two central order statistics.
-        const uint32_t lo = radix_select(vals, ns, half - 1, hist, sh, wtot);
+        const uint32_t lo = radix_select_2buf(vals, ns, half - 1, hist, sh2, wtot2);
         int le = 0;
         uint32_t above = 0xFFFFFFFFu;
         for (int i = threadIdx.x; i < ns; i += blockDim.x) {

@@ -360,10 +360,11 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
     __shared__ unsigned long long s_qm[kHG];       // ceil(2^64 / q): (n div q) = mulhi(n, s_qm) for n < 2^32
     __shared__ unsigned s_pm[kHG];                 // ceil(2^24 / P): (task div P) for task * P < 2^24
 
-    // blocks fastest: the CTAs resident on an SM share a group's weight tables in L1
-    const int hidx0 = blockIdx.y * kHG;
+    // harmonic groups fastest: the CTAs filling one block's A tiles (each a
+    // 128-byte piece of every 2 KB row group) run together
+    const int hidx0 = blockIdx.x * kHG;
     const int ng = min(kHG, a.nharms - hidx0);
-    const int blk = blockIdx.x;
+    const int blk = blockIdx.y;
     const int m = M > 0 ? M : a.m;
     const int m2 = m / 2;
     const int64_t t0 = blk_t0(a, blk);
@@ -499,7 +500,7 @@ __device__ __forceinline__ int i2_wstride(int win_max) { return (win_max + 3) & 
 __device__ void i2_prepare(const WaveArgs& a, int item, int ngroups, int win_max, float2* stage, HarmStage* st,
                            uint64_t* bar, int* err) {
     const int lane = threadIdx.x & 31;
-    const int grp = item / a.nblk, blk = item - grp * a.nblk;   // blocks fastest
+    const int blk = item / ngroups, grp = item - blk * ngroups;   // harmonic groups fastest
     const int hidx0 = grp * kHG;
     const int ng = min(kHG, a.nharms - hidx0);
     const int64_t t0 = blk_t0(a, blk);
@@ -585,7 +586,7 @@ __global__ void __launch_bounds__(kI2Threads, 2) k_interp2(WaveArgs a, int win_m
     if (!ok && threadIdx.x == 0) atomicExch(err, 4);
     for (int it = 0; item < nitems && ok; item += gridDim.x, ++it) {
         const HarmStage* S = st[it & 1];
-        const int grp = item / a.nblk, blk = item - grp * a.nblk;
+        const int blk = item / ngroups, grp = item - blk * ngroups;
         const int hidx0 = grp * kHG;
         const int ng = min(kHG, a.nharms - hidx0);
         const int64_t t0 = blk_t0(a, blk);
@@ -673,7 +674,7 @@ cudaError_t launch_amax(const float2* amps, int64_t n, uint32_t* out, cudaStream
 size_t interp_smem(int win_max, int Nprof) { return (size_t)(win_max + kHG * Nprof) * sizeof(float2); }
 
 cudaError_t launch_interp(const WaveArgs& a, cudaStream_t st, int win_max, int* err) {
-    dim3 grid(a.nblk, (a.nharms + kHG - 1) / kHG);
+    dim3 grid((a.nharms + kHG - 1) / kHG, a.nblk);
     const size_t smem = interp_smem(win_max, a.Nprof);
     const int Nst = a.Nprof;
     switch (a.m) {

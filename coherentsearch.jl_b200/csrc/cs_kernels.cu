@@ -130,10 +130,11 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
     }
     if (a.Atile) {
         // A tile (block, j/128), row r = j%128, K chunk hidx0/4 holds (Re, Im) of
-        // the 4 harmonics: SWIZZLE_NONE K-major core-matrix layout.  Split
+        // the 4 harmonics: SWIZZLE_NONE K-major core matrices, each K chunk's 16
+        // row groups contiguous (2 KB per chunk, chunks 2 KB apart).  Split
         // tiles: the tile of residuals x - hi follows each tile.
         const int tsz = a.asplit * kATileBytes;
-        uint8_t* base = a.Atile + (int64_t)blk * a.tiles_per_blk * tsz + (hidx0 >> 2) * 128;
+        uint8_t* base = a.Atile + (int64_t)blk * a.tiles_per_blk * tsz + (hidx0 >> 2) * 2048;
         const float2* x1 = xo + Nst;
         const float2* x2 = xo + 2 * Nst;
         const float2* x3 = xo + 3 * Nst;
@@ -145,7 +146,7 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
             const float2 v2 = ng > 2 ? x2[j] : z;
             const float2 v3 = ng > 3 ? x3[j] : z;
             uint4 pk;
-            const uint32_t off = (uint32_t)(j >> 7) * (uint32_t)tsz + ((uint32_t)(j & 127) >> 3) * 2048u +
+            const uint32_t off = (uint32_t)(j >> 7) * (uint32_t)tsz + ((uint32_t)(j & 127) >> 3) * 128u +
                                  (uint32_t)(j & 7) * 16u;
             if (a.asplit == 2) {
                 const float2 vv[4] = {v0, v1, v2, v3};

@@ -17,8 +17,9 @@
 // exact FP32 rescan, so the reported S/N never depends on the reduced precision.
 //
 // Layout: SWIZZLE_NONE K-major canonical UMMA layout -- 8-row x 16-byte core
-// matrices, K-adjacent core matrices 128 B apart (LBO), 8-row groups 2048 B
-// apart (SBO).  One persistent CTA per SM (it holds all 512 TMEM columns).
+// matrices.  B (twiddles): K-adjacent core matrices 128 B apart (LBO), 8-row
+// groups 2048 B apart (SBO).  A (amplitudes): the other way round, LBO 2048 B
+// and SBO 128 B, so that a tile's K chunk is contiguous.  One persistent CTA per SM (it holds all 512 TMEM columns).
 #include "cs_internal.h"
 
 #include <cuda_bf16.h>
@@ -38,14 +39,21 @@ constexpr int kK = 128;             // padded K: 2*nharms <= 128
 constexpr int kSBO = (kK / 8) * 128;  // bytes between 8-row groups
 constexpr int kABytes = kTM * kK * 2;
 
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo = 128, uint32_t sbo = kSBO) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);                 // start address
-    d |= (uint64_t)((128 >> 4) & 0x3FFF) << 16;             // LBO: K-adjacent core matrices
-    d |= (uint64_t)((kSBO >> 4) & 0x3FFF) << 32;            // SBO: 8-row groups
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;             // LBO: K-adjacent core matrices
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;             // SBO: 8-row groups
     d |= (uint64_t)1 << 46;                                 // descriptor version (sm_100)
     return d;                                               // base offset 0, SWIZZLE_NONE
 }
+
+// A tiles are laid out K-chunk by K-chunk: the 16 core matrices (8 trials x 8
+// K values, 128 bytes each) of one K chunk are adjacent (8-row groups 128 B
+// apart) and K-adjacent chunks 2 KB apart, so each chunk of a tile -- the
+// four harmonics one interpolation CTA computes -- is one contiguous 2 KB run.
+constexpr uint32_t kALBO = (kTM / 8) * 128;   // 2048
+constexpr uint32_t kASBO = 128;
 
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float v[8]) {
     uint32_t r[8];
@@ -373,7 +381,7 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
             // same twiddles, into one FP32 accumulator
             for (int kk = 0; kk < t.split * (kK / 16); ++kk) {
                 const int sp = kk / (kK / 16), ks = kk - sp * (kK / 16);
-                const uint64_t da = umma_desc(a_addr + sp * kABytes + ks * 256);
+                const uint64_t da = umma_desc(a_addr + sp * kABytes + ks * 2 * kALBO, kALBO, kASBO);
                 const uint64_t db = umma_desc(b_addr + (M.bcol / 8) * kSBO + ks * 256);
                 const uint32_t acc = kk > 0;
                 asm volatile(

@@ -225,13 +225,18 @@ class Engine:
 
     # -- spectrum ---------------------------------------------------------
     def set_spectrum(self, ft, force=False):
-        key = (id(ft), ft.N, len(ft.amps))
-        if key == self._spec_key and not force:
+        """Copy `ft`'s spectrum to the device, unless this very FFTFile (and
+        its amps array) was the last one attached.  The engine keeps both
+        objects referenced, so their identities cannot be reused by new ones;
+        after changing ft.amps in place, pass force=True."""
+        if not force and self._spec_key == ("file",) and self._spec_keep is not None and \
+                self._spec_keep[0] is ft and self._spec_keep[1] is ft.amps:
             return
         amps = np.ascontiguousarray(ft.amps, dtype=np.complex64)
         st = self.lib.cs_set_spectrum(self._h, amps.ctypes.data, len(amps), int(ft.N), float(ft.inf.dt))
         _lib.check(st, self._h, "cs_set_spectrum")
-        self._spec_key = key
+        self._spec_key = ("file",)
+        self._spec_keep = (ft, ft.amps)
 
     def set_spectrum_host(self, ptr: int, namps: int, N: int, dt: float):
         """Copy a spectrum from host memory at ``ptr`` (pinned for full speed)."""

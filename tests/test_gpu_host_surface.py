@@ -117,3 +117,19 @@ def test_batch_of_fft_files_from_disk(tmp_path):
     for ft, got in zip(fts, batch):
         want = cs.search(ft, params, lofreq=1.0, hifreq=60.0, threshold=7.0)
         assert want and [(c.r, c.metric, c.nharm) for c in got] == [(c.r, c.metric, c.nharm) for c in want]
+
+
+def test_each_new_spectrum_is_searched():
+    """Spectra of one length attached one after another as temporaries (whose
+    Python identities can be reused once freed): the engine must search each
+    new one, never a previous one."""
+    from oracle import cs_cpu as port
+    eng = cs.Engine(cs.SearchParams(nharms=16, m=16))
+    N, dt = 1 << 16, 1e-3
+    for seed in range(24):
+        amps = ((np.random.default_rng(seed).standard_normal(N // 2) +
+                 1j * np.random.default_rng(seed + 1000).standard_normal(N // 2)) * 0.7).astype(np.complex64)
+        eng.set_spectrum(cs.FFTFile.from_array(amps.copy(), N, dt))
+        got = eng.interp_chunk(2000.0, 0, 64)
+        want = port.interp_chunk(amps, N, 16, 16, 0.5, 2000.0, 0, 64)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), seed

@@ -186,14 +186,13 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
         }
     }
     if (!a.samp) return;
-    // The pooled columns j_c = (c*nv) div ncs (src/search.jl:528-537) of every
-    // (harmonic, level) pair whose level folds the harmonic, all pairs' columns
-    // dealt out over the whole CTA as one index space (consecutive threads on
-    // consecutive columns of a pair).  The division by ncs is a multiply-high
-    // by ceil(2^64/ncs), exact for every 32-bit dividend.
-    const int nthr = (int)blockDim.x;
-    int base = 0;
-    for (int e = 0; e < ng * a.nlev; ++e) {
+    // One warp per (harmonic, level) pair whose level folds this harmonic;
+    // lanes over its pooled columns j_c = (c*nv) div ncs (src/search.jl:528-537),
+    // the division by ncs done as a multiply-high by ceil(2^64/ncs), exact for
+    // every 32-bit dividend.
+    const int lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    for (int e = threadIdx.x >> 5; e < ng * a.nlev; e += nwarps) {
         const int g = e / a.nlev, l = e - g * a.nlev;
         const int h = hidx0 + g + 1;
         const DevLevel& L = a.levels[l];
@@ -204,19 +203,15 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
         const int ncs = all ? nv : min(nv, max(1, kSigmaCap / L.nbins));
         float2* dst = a.samp + ((int64_t)blk * a.nlev + l) * kSampStride + (int64_t)(h / L.k - 1) * ncs;
         const float2* src = xo + g * Nst;
-        // this thread's first column of the pair: (base + c) % nthr == threadIdx.x
-        int c = ((int)threadIdx.x - base) % nthr;
-        if (c < 0) c += nthr;
         if (all || ncs == 1) {
-            for (; c < ncs; c += nthr) dst[c] = src[all ? c : 0];
+            for (int c = lane; c < ncs; c += 32) dst[c] = src[all ? c : 0];
         } else {
             const uint64_t mg = 0xFFFFFFFFFFFFFFFFull / (uint64_t)ncs + 1ull;
-            for (; c < ncs; c += nthr) {
+            for (int c = lane; c < ncs; c += 32) {
                 const uint32_t x = (uint32_t)c * (uint32_t)nv;   // < 4096 * 65536
                 dst[c] = src[(int)__umul64hi((uint64_t)x, mg)];
             }
         }
-        base += ncs;
     }
 }
 

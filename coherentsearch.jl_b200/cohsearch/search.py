@@ -239,7 +239,9 @@ class Engine:
         self._spec_keep = (ft, ft.amps)
 
     def set_spectrum_host(self, ptr: int, namps: int, N: int, dt: float):
-        """Copy a spectrum from host memory at ``ptr`` (pinned for full speed)."""
+        """Copy a spectrum from host memory at ``ptr`` (cs_set_spectrum).  From
+        pinned memory the copy overlaps the next search, so the buffer must stay
+        unchanged until that search has returned."""
         st = self.lib.cs_set_spectrum(self._h, ctypes.c_void_p(ptr), int(namps), int(N), float(dt))
         _lib.check(st, self._h, "cs_set_spectrum")
         self._spec_key = ("host", ptr, namps, N)

@@ -245,6 +245,17 @@ struct cs_handle {
     double dt = 0.0;
     bool has_spec = false;
     int64_t spec_h2d_bytes = 0;   // bytes of the last host spectrum copy, charged to the next search
+    // A host spectrum (cs_set_spectrum) arrives in chunks on the copy stream:
+    // chunk c of amps_owned, and its maximum in d_amax_spec[c], are on the
+    // device once chunk_ev[c] has completed.  The first search after the copy
+    // starts interpolating each run of blocks as soon as the chunks it reads
+    // have landed; everything else that reads the spectrum waits for all.
+    const float2* chunked_amps = nullptr;   // amps_owned while chunk_ev describes it
+    bool chunks_pending = false;            // no search has overlapped with the copy yet
+    int spec_nchunk = 0;
+    cudaEvent_t chunk_ev[kMaxSpecChunks] = {};
+    cudaEvent_t spec_free_ev = nullptr;     // every earlier read of amps_owned, before an overwrite
+    DBuf d_amax_spec;
     // device buffers
     TcPlanHost tc;                      // tensor-core synthesis plan (synth != FP32)
     DBuf d_tcB;
@@ -344,6 +355,23 @@ cs_status cuda_fail(cs_handle* H, cudaError_t e, const char* where) {
         cudaError_t e_ = (call);                               \
         if (e_ != cudaSuccess) return cuda_fail(H, e_, where); \
     } while (0)
+
+// Chunks of a spectrum of namps bins: at least 64 Ki bins each, at most
+// kMaxSpecChunks of them.  Host and device spectra use the same layout, so a
+// block's FP16 tile scale does not depend on where its spectrum came from.
+static void spec_chunks(int64_t namps, int64_t* chunk, int* nchunk) {
+    const int64_t c = std::max<int64_t>((namps + kMaxSpecChunks - 1) / kMaxSpecChunks, (int64_t)1 << 16);
+    *chunk = c;
+    *nchunk = (int)std::max<int64_t>(1, (namps + c - 1) / c);
+}
+
+// Work on H->stream that reads the attached spectrum at once waits for the
+// whole of a chunked host copy.
+static cudaError_t spec_ready(cs_handle* H) {
+    if (H->amps && H->amps == H->chunked_amps)
+        return cudaStreamWaitEvent(H->stream, H->chunk_ev[H->spec_nchunk - 1], 0);
+    return cudaSuccess;
+}
 
 template <class T>
 cudaError_t upload(DBuf& b, const std::vector<T>& v, cudaStream_t st) {
@@ -475,7 +503,7 @@ struct RunSpec {
     // prefix go to these pinned slots, valid counts come from h_nvalid
     bool capture = false;
     int32_t* cap_io = nullptr;          // 64 bytes of counters, then kCandPrefix DevCands
-    int32_t* cap_nvalid = nullptr;      // pinned [nblocks][nlev], filled here
+    int32_t* cap_nvalid = nullptr;      // pinned [nblocks][nlev + 1], filled here
 };
 
 // _logedges (src/search.jl:1406-1411): nwin+1 log-spaced edges over [a, b].
@@ -608,10 +636,11 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         if ((want_x && small(H->d_X, (size_t)WB * p.nharms * Nprof * sizeof(float2))) ||
             (tensor && small(H->d_A, (size_t)WB * tiles_per_blk * kATileBytes * synth_split(p.synth))) ||
             small(H->d_samp, (size_t)WB * nlev * kSampStride * sizeof(float2)) ||
-            small(H->d_sigma, (size_t)WB * nlev * sizeof(float)) || small(H->d_nvalid, (size_t)WB * nlev * sizeof(int32_t)) ||
+            small(H->d_sigma, (size_t)WB * nlev * sizeof(float)) ||
+            small(H->d_nvalid, (size_t)WB * (nlev + 1) * sizeof(int32_t)) ||
             small(H->d_items, (size_t)WB * nlev * Nprof * sizeof(DevItem)) ||
             small(H->d_cands, (size_t)WB * nlev * Nprof * sizeof(DevCand)) || small(H->d_counts, 4 * sizeof(int32_t)) ||
-            (tensor && synth_fp16(p.synth) && small(H->d_amax, 16)))
+            (tensor && synth_fp16(p.synth) && small(H->d_amax, kMaxSpecChunks * sizeof(uint32_t))))
             return fail(H, CS_ERR_UNSUPPORTED, "a captured search needs buffers sized by an earlier run");
     }
 
@@ -629,7 +658,8 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         if (H->diag >= 2 && !R.exact_all)
             CS_CUDA(H->d_Q0.ensure((size_t)WB * nlev * Nprof * sizeof(float)), "alloc gate values");
         CS_CUDA(H->d_sigma.ensure((size_t)WB * nlev * sizeof(float)), "alloc sigma");
-        CS_CUDA(H->d_nvalid.ensure((size_t)WB * nlev * sizeof(int32_t)), "alloc nvalid");
+        // valid counts [nb][nlev], then each block's last spectrum chunk [nb]
+        CS_CUDA(H->d_nvalid.ensure((size_t)WB * (nlev + 1) * sizeof(int32_t)), "alloc nvalid");
         CS_CUDA(H->d_items.ensure((size_t)WB * nlev * Nprof * sizeof(DevItem)), "alloc items");
         CS_CUDA(H->d_cands.ensure((size_t)WB * nlev * Nprof * sizeof(DevCand)), "alloc cands");
         if (R.exact_all)
@@ -699,14 +729,30 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
     int32_t* counts = R.capture ? R.cap_io : H->h_io.as<int32_t>();
     DevCand* cand_pre = reinterpret_cast<DevCand*>(reinterpret_cast<uint8_t*>(counts) + 64);
 
-    // FP16 A tiles: the spectrum's largest component, for their range scale
+    // The spectrum's chunks: a host spectrum still being copied in chunks is
+    // interpolated run of blocks by run of blocks as its chunks land (first
+    // wave only; later work waits for the whole copy).
+    int64_t chunk = 0;
+    int nch = 0;
+    spec_chunks(H->namps, &chunk, &nch);
+    const bool host_spec = H->amps == H->chunked_amps;
+    if (host_spec && nch != H->spec_nchunk) return fail(H, CS_ERR_INVALID_ARGUMENT, "spectrum chunk layout changed");
+    bool overlap = host_spec && H->chunks_pending && !R.capture;
+    // FP16 A tiles: each spectrum chunk's largest component, for their range
+    // scale (a host spectrum's come with its copy)
     const bool fp16_scale = tensor && !R.interp_only && synth_fp16(p.synth);
-    if (fp16_scale) {
-        if (!R.capture) CS_CUDA(H->d_amax.ensure(16), "alloc spectrum maximum");
-        CS_CUDA(cudaMemsetAsync(H->d_amax.p, 0, sizeof(uint32_t), H->stream), "reset spectrum maximum");
-        CS_CUDA(launch_amax(H->amps, H->namps, H->d_amax.as<uint32_t>(), H->stream, H->num_sms), "maximum launch");
+    const uint32_t* amax = nullptr;
+    if (fp16_scale && host_spec) {
+        amax = H->d_amax_spec.as<uint32_t>();
+    } else if (fp16_scale) {
+        if (!R.capture) CS_CUDA(H->d_amax.ensure(kMaxSpecChunks * sizeof(uint32_t)), "alloc chunk maxima");
+        CS_CUDA(cudaMemsetAsync(H->d_amax.p, 0, kMaxSpecChunks * sizeof(uint32_t), H->stream), "reset chunk maxima");
+        CS_CUDA(launch_amax(H->amps, H->namps, chunk, nch, H->d_amax.as<uint32_t>(), H->stream, H->num_sms),
+                "maximum launch");
         S.launches += 1;
+        amax = H->d_amax.as<uint32_t>();
     }
+    if (host_spec && !overlap) CS_CUDA(spec_ready(H), "wait for the spectrum");
 
     for (int64_t c0 = 0; c0 < R.nblocks; c0 += WB) {
         const int nb = (int)std::min<int64_t>(WB, R.nblocks - c0);
@@ -734,7 +780,9 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         a.tiles_per_blk = tiles_per_blk;
         a.fp16 = synth_fp16(p.synth) ? 1 : 0;
         a.asplit = synth_split(p.synth);
-        a.amax_bits = fp16_scale ? H->d_amax.as<uint32_t>() : nullptr;
+        a.amax_bits = amax;
+        a.blk_cidx = nullptr;
+        a.blk_first = 0;
         a.samp = R.interp_only ? nullptr : H->d_samp.as<float2>();
         a.Q0 = (H->diag >= 2 && !R.exact_all) ? H->d_Q0.as<float>() : nullptr;   // gate values: diagnostics only
         a.sigma = H->d_sigma.as<float>();
@@ -788,14 +836,20 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         }
         int* d_err = H->d_counts.as<int32_t>() + 2;
 
-        if (!R.capture) CS_CUDA(H->h_nvalid.ensure((size_t)nb * nlev * sizeof(int32_t)), "pinned valid counts");
+        if (!R.capture) CS_CUDA(H->h_nvalid.ensure((size_t)nb * (nlev + 1) * sizeof(int32_t)), "pinned valid counts");
         int32_t* nvalid = R.capture ? R.cap_nvalid : H->h_nvalid.as<int32_t>();
+        int32_t* cidx = nvalid + (size_t)nb * nlev;   // each block's last spectrum chunk
         for (int b = 0; b < nb; ++b) {
             const int64_t c = c0 + b;
             // global trial of the block's first trial
             const int64_t tb = R.blist ? R.blist[c] * (int64_t)Nprof : R.t_base + c * (int64_t)Nprof;
             const int n = (int)std::min<int64_t>(Nprof, R.t_end - tb);
             const double rstart = R.r_lo + (double)tb * R.lodr;
+            // the highest bin any harmonic's window reaches: nharms * r of the
+            // block's last trial, m/2 taps past it, and a margin for rounding
+            const double top = std::floor((double)p.nharms * (rstart + (double)(n - 1) * R.lodr));
+            const int64_t bin_max = top < 0 ? 0 : (top > 4.0e18 ? INT64_MAX / 2 : (int64_t)top) + p.m / 2 + 4;
+            cidx[b] = (int32_t)std::min<int64_t>(nch - 1, bin_max / chunk);
             for (int l = 0; l < nlev; ++l) {
                 const int k = H->dlev[l].k;
                 nvalid[(size_t)b * nlev + l] = (k == 1) ? n : nvalid_decim(k, rstart, R.lodr, n, nyq);
@@ -825,19 +879,43 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         }
         CS_CUDA(cudaMemsetAsync(H->d_counts.p, 0, 4 * sizeof(int32_t), H->stream), "reset counters");
         if (!R.interp_only) {
-            CS_CUDA(cudaMemcpyAsync(H->d_nvalid.p, nvalid, (size_t)nb * nlev * sizeof(int32_t),
+            CS_CUDA(cudaMemcpyAsync(H->d_nvalid.p, nvalid, (size_t)nb * (nlev + 1) * sizeof(int32_t),
                                     cudaMemcpyHostToDevice, H->stream),
                     "upload nvalid");
-            S.h2d_bytes += (int64_t)nb * nlev * (int64_t)sizeof(int32_t);
+            S.h2d_bytes += (int64_t)nb * (nlev + 1) * (int64_t)sizeof(int32_t);
             a.nvalid = H->d_nvalid.as<int32_t>();
+            a.blk_cidx = H->d_nvalid.as<int32_t>() + (size_t)nb * nlev;
         }
         if (!R.capture) CS_CUDA(cudaEventRecord(H->ev[0], H->stream), "event");
-        if (interp2)
-            CS_CUDA(launch_interp2(a, H->stream, win_max, d_err, H->num_sms), "interp launch");
-        else
-            CS_CUDA(launch_interp(a, H->stream, win_max, d_err), "interp launch");
+        auto interp_launch = [&](const WaveArgs& w) {
+            return interp2 ? launch_interp2(w, H->stream, win_max, d_err, H->num_sms)
+                           : launch_interp(w, H->stream, win_max, d_err);
+        };
+        if (overlap) {
+            // runs of blocks by the last chunk they read (the running maximum
+            // of cidx): each run starts once that chunk has landed
+            int s = 0, need = cidx[0];
+            for (int b = 1; b <= nb; ++b) {
+                if (b < nb && cidx[b] <= need) continue;
+                WaveArgs w = a;
+                w.blk_first = s;
+                w.nblk = b - s;
+                CS_CUDA(cudaStreamWaitEvent(H->stream, H->chunk_ev[need], 0), "wait for a spectrum chunk");
+                CS_CUDA(interp_launch(w), "interp launch");
+                S.launches += 1;
+                if (b < nb) {
+                    s = b;
+                    need = cidx[b];
+                }
+            }
+            CS_CUDA(spec_ready(H), "wait for the spectrum");
+            H->chunks_pending = false;
+            overlap = false;
+        } else {
+            CS_CUDA(interp_launch(a), "interp launch");
+            S.launches += 1;
+        }
         if (!R.capture) CS_CUDA(cudaEventRecord(H->ev[1], H->stream), "event");
-        S.launches += 1;
         if (!R.interp_only) {
             // sigma needs only the samples, so it runs first and the synthesis
             // epilogue applies the medcut test itself (no gate pass over HBM);
@@ -1111,6 +1189,7 @@ cs_status cs_destroy(cs_handle* H) {
     cudaSetDevice(H->device);
     if (H->stream) cudaStreamSynchronize(H->stream);
     if (H->own_stream) cudaStreamSynchronize(H->own_stream);
+    if (H->copy_stream) cudaStreamSynchronize(H->copy_stream);   // chunk copies still in flight
     for (auto& e : H->plan_sets) e->release();
     H->plan_sets.clear();
     if (H->gexec) cudaGraphExecDestroy(H->gexec);
@@ -1133,6 +1212,10 @@ cs_status cs_destroy(cs_handle* H) {
     H->d_batch[1].release();
     for (auto& e : H->copy_ev)
         if (e) cudaEventDestroy(e);
+    for (auto& e : H->chunk_ev)
+        if (e) cudaEventDestroy(e);
+    if (H->spec_free_ev) cudaEventDestroy(H->spec_free_ev);
+    H->d_amax_spec.release();
     if (H->copy_stream) cudaStreamDestroy(H->copy_stream);
     DBuf* mbufs[] = {&H->d_mst, &H->d_mwin, &H->d_mhist, &H->d_muo, &H->d_norm, &H->d_bm_r, &H->d_bm_h,
                      &H->d_bm_st, &H->d_bm_prof, &H->d_bm_w, &H->d_bm_sig, &H->d_bm_out};
@@ -1155,12 +1238,38 @@ cs_status cs_set_spectrum(cs_handle* H, const float* amps, int64_t namps, int64_
     cs_status st = check_spec_args(H, amps, namps, N, dt);
     if (st != CS_OK) return st;
     CS_CUDA(cudaSetDevice(H->device), "set device");
+    H->has_spec = false;
+    H->chunked_amps = nullptr;
+    H->chunks_pending = false;
+    if (!H->copy_stream) CS_CUDA(cudaStreamCreateWithFlags(&H->copy_stream, cudaStreamNonBlocking), "copy stream");
+    if (!H->spec_free_ev) CS_CUDA(cudaEventCreateWithFlags(&H->spec_free_ev, cudaEventDisableTiming), "event");
+    for (auto& e : H->chunk_ev)
+        if (!e) CS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    // the copies overwrite amps_owned only after everything issued so far that reads it
+    CS_CUDA(cudaEventRecord(H->spec_free_ev, H->stream), "event");
+    CS_CUDA(cudaStreamWaitEvent(H->copy_stream, H->spec_free_ev, 0), "order the copy");
     CS_CUDA(H->amps_owned.ensure((size_t)namps * sizeof(float2)), "alloc spectrum");
-    CS_CUDA(cudaMemcpyAsync(H->amps_owned.p, amps, (size_t)namps * sizeof(float2), cudaMemcpyHostToDevice,
-                            H->stream),
-            "copy spectrum");
+    CS_CUDA(H->d_amax_spec.ensure(kMaxSpecChunks * sizeof(uint32_t)), "alloc chunk maxima");
+    CS_CUDA(cudaMemsetAsync(H->d_amax_spec.p, 0, kMaxSpecChunks * sizeof(uint32_t), H->copy_stream),
+            "reset chunk maxima");
+    int64_t chunk = 0;
+    int nch = 0;
+    spec_chunks(namps, &chunk, &nch);
+    float2* dst = H->amps_owned.as<float2>();
+    for (int c = 0; c < nch; ++c) {
+        const int64_t b0 = (int64_t)c * chunk, nb = std::min(chunk, namps - b0);
+        CS_CUDA(cudaMemcpyAsync(dst + b0, amps + 2 * b0, (size_t)nb * sizeof(float2), cudaMemcpyHostToDevice,
+                                H->copy_stream),
+                "copy spectrum");
+        CS_CUDA(launch_amax(dst + b0, nb, nb, 1, H->d_amax_spec.as<uint32_t>() + c, H->copy_stream, H->num_sms),
+                "chunk maximum launch");
+        CS_CUDA(cudaEventRecord(H->chunk_ev[c], H->copy_stream), "event");
+    }
+    H->spec_nchunk = nch;
+    H->chunked_amps = dst;
+    H->chunks_pending = true;
     H->spec_h2d_bytes = namps * (int64_t)sizeof(float2);
-    H->amps = H->amps_owned.as<float2>();
+    H->amps = dst;
     H->namps = namps;
     H->N = N;
     H->dt = dt;
@@ -1344,7 +1453,7 @@ void capture_batch(cs_handle* H, const cs_spectrum* files, int nfiles, double lo
         empty[i] = e ? 1 : 0;
         if (e) continue;
         if (H->gslots[i].io.ensure(64 + (size_t)kGraphPrefix * sizeof(DevCand)) != cudaSuccess ||
-            H->gslots[i].nvalid.ensure((size_t)specs[i].nblocks * nlev * sizeof(int32_t)) != cudaSuccess)
+            H->gslots[i].nvalid.ensure((size_t)specs[i].nblocks * (nlev + 1) * sizeof(int32_t)) != cudaSuccess)
             return;
     }
     if (cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) return;
@@ -1421,6 +1530,7 @@ cs_status cs_block_features(cs_handle* H, double lofreq, double hifreq, int64_t 
     *nblocks_out = nb;
     if (nb > cap_blocks) return fail(H, CS_ERR_CAPACITY, "feature array too small");
     if (nb == 0) return CS_OK;
+    CS_CUDA(spec_ready(H), "wait for the spectrum");
     const cudaError_t e = launch_features(H->amps, H->namps, r_lo, lodr, blocksize, total,
                                           H->d_levels.as<DevLevel>(), (int)H->dlev.size(), nfeat, d_out, H->stream);
     if (e == cudaErrorInvalidValue) return fail(H, CS_ERR_UNSUPPORTED, "more than 512 features per block");
@@ -1752,6 +1862,7 @@ cs_status cs_block_metrics(cs_handle* H, const double* rfund, int64_t L, int32_t
     CS_CUDA(cudaMemcpyAsync(H->d_bm_r.p, rfund, (size_t)L * sizeof(double), cudaMemcpyHostToDevice, H->stream),
             "copy trials");
     CS_CUDA(upload(H->d_bm_h, hm, H->stream), "copy harmonic grid");
+    CS_CUDA(spec_ready(H), "wait for the spectrum");
     CS_CUDA(upload(H->d_bm_w, ws, H->stream), "copy widths");
     CS_CUDA(run_block_metrics(H->d_bm_r.as<double>(), (int)L, H->d_bm_h.as<BmHarm>(), nh, m, nb, kernel, H->amps,
                               H->namps, H->d_bm_st.as<double2>(), H->d_bm_prof.as<double>(), H->d_bm_w.as<int>(),
@@ -1782,6 +1893,7 @@ cs_status cs_refold(cs_handle* H, const double* r, const int32_t* nharm, int64_t
     CS_CUDA(cudaMemcpyAsync(H->d_bm_r.p, r, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, H->stream), "copy r");
     CS_CUDA(cudaMemcpyAsync(d_nh, nharm, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, H->stream),
             "copy nharm");
+    CS_CUDA(spec_ready(H), "wait for the spectrum");
     CS_CUDA(run_refold(H->d_bm_r.as<double>(), d_nh, (int)n, m, H->p.boxcar_fsp, H->p.boxcar_maxfrac, H->amps,
                        H->namps, H->N / 2, maxh, profiles ? H->d_bm_prof.as<double>() : nullptr, d_H,
                        H->d_bm_out.as<double>(), H->stream),

@@ -14,6 +14,7 @@ namespace cs {
 constexpr int kMaxLevels = 16;     // decimation factors per search
 constexpr int kMaxWidths = 64;     // boxcar widths per level
 constexpr int kMaxBins = 256;      // profile bins (nharms <= 128)
+constexpr int kMaxSpecChunks = 16;  // a host spectrum arrives in up to this many chunks
 constexpr int kSigmaCap = 8192;    // _BOXCAR_SIGMA_SAMPLES, src/search.jl:462
 constexpr int kTileTrials = 64;    // trials per CTA in the FP32 synthesis kernel
 constexpr int kATileBytes = 128 * 128 * 2;  // one 16-bit A tile: 128 trials x 128 K
@@ -95,10 +96,14 @@ struct WaveArgs {
     int32_t fp16;           // A-tile format: 1 = FP16, 0 = BF16
     int32_t asplit;         // 1, or 2: each 128-trial A tile is followed by the tile of the
                             // amplitudes' rounding residuals (x - hi), in the same format
-    // FP16 A tiles: bits of the spectrum's largest |Re| or |Im| (k_amax), from
-    // which a power-of-two scale keeps the tiles inside FP16's range; nullptr:
-    // no scale (BF16 has FP32's range)
+    // FP16 A tiles: bits of the largest |Re| or |Im| of each spectrum chunk
+    // (k_amax, kMaxSpecChunks entries, unused ones 0).  A block's tiles take a
+    // power-of-two scale from the maximum over chunks 0..blk_cidx[blk], which
+    // holds every bin the block reads, so the scale is known as soon as those
+    // chunks are on the device.  nullptr: no scale (BF16 has FP32's range)
     const uint32_t* amax_bits;
+    const int32_t* blk_cidx;  // [nblk]: last spectrum chunk the block reads; nullptr: all chunks
+    int32_t blk_first;        // interpolation launches over part of a wave: its first block
     float2* samp;           // [nblk][nlev][kSampStride]: pooled columns' amplitudes, [jh-1][slot]
     float* Q0;              // [nblk][nlev][Nprof] zero-baseline gate (unscaled by 1/sigma); diagnostics only, may be null
     float* sigma;           // [nblk][nlev]
@@ -303,9 +308,11 @@ __device__ __forceinline__ float inv_sigma(float sig) { return sig > 0.0f ? 1.0f
 // 16 taps' |sinc| weights), so 16 leaves a further factor 4 of headroom for
 // the tiles.  The gate is linear in the amplitudes: it comes back exactly by
 // 2^s.
-__device__ __forceinline__ int ascale_exp(const uint32_t* amax_bits) {
+__device__ __forceinline__ int ascale_exp(const uint32_t* amax_bits, int cidx) {
     if (!amax_bits) return 0;
-    const float r = __uint_as_float(*amax_bits) * (16.0f / 65504.0f);
+    uint32_t mx = 0;   // non-negative floats order as their bits
+    for (int c = 0; c <= cidx; ++c) mx = max(mx, amax_bits[c]);
+    const float r = __uint_as_float(mx) * (16.0f / 65504.0f);
     if (!(r >= 1.0f)) return 0;
     if (!(r < 1e30f)) return 100;                 // inf or NaN in the spectrum
     int e;
@@ -313,6 +320,10 @@ __device__ __forceinline__ int ascale_exp(const uint32_t* amax_bits) {
     return min(e, 100);
 }
 __device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }   // |e| <= 126
+// The scale exponent of wave block blk's A tiles.
+__device__ __forceinline__ int ascale_exp_blk(const WaveArgs& a, int blk) {
+    return ascale_exp(a.amax_bits, a.blk_cidx ? a.blk_cidx[blk] : kMaxSpecChunks - 1);
+}
 
 // Gate value g (zero-baseline boxcar maximum, not yet divided by sigma) of
 // valid trial j: at or above medcut_gate it goes to the rescan list, else its
@@ -361,7 +372,10 @@ cudaError_t launch_mlp_backward(const cs_mlp& net, const float* x, const float* 
                                 const cs_mlp_grads& g, float* loss, cudaStream_t st);
 cudaError_t launch_adam(const cs_adam_param& p, float lr, float b1, float b2, float eps, int step, cudaStream_t st);
 cudaError_t launch_to_bf16(const float* p, uint16_t* pb, int64_t n, cudaStream_t st);
-cudaError_t launch_amax(const float2* amps, int64_t n, uint32_t* out, cudaStream_t st, int num_sms);
+// Largest |Re| or |Im| of each chunk [c*chunk, min(n, (c+1)*chunk)), c < nchunk,
+// atomically maxed into out[c] (zeroed by the caller).
+cudaError_t launch_amax(const float2* amps, int64_t n, int64_t chunk, int nchunk, uint32_t* out, cudaStream_t st,
+                        int num_sms);
 
 // block_metrics (reference path): per harmonic, the fine-grid origin, its
 // length (numbins * numbetween) and the reference's range guard.

@@ -139,7 +139,7 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
         const float2* x2 = xo + 2 * Nst;
         const float2* x3 = xo + 3 * Nst;
         const float2 z = make_float2(0.0f, 0.0f);
-        const float sc = a.fp16 ? pow2f(-ascale_exp(a.amax_bits)) : 1.0f;   // exact power of two
+        const float sc = a.fp16 ? pow2f(-ascale_exp_blk(a, blk)) : 1.0f;   // exact power of two
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
             const float2 v0 = xo[j];
             const float2 v1 = ng > 1 ? x1[j] : z;
@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
     // 128-byte piece of every 2 KB row group) run together
     const int hidx0 = blockIdx.x * kHG;
     const int ng = min(kHG, a.nharms - hidx0);
-    const int blk = blockIdx.y;
+    const int blk = a.blk_first + (int)blockIdx.y;
     const int m = M > 0 ? M : a.m;
     const int m2 = m / 2;
     const int64_t t0 = blk_t0(a, blk);
@@ -496,7 +496,8 @@ __device__ __forceinline__ int i2_wstride(int win_max) { return (win_max + 3) & 
 __device__ void i2_prepare(const WaveArgs& a, int item, int ngroups, int win_max, float2* stage, HarmStage* st,
                            uint64_t* bar, int* err) {
     const int lane = threadIdx.x & 31;
-    const int blk = item / ngroups, grp = item - blk * ngroups;   // harmonic groups fastest
+    const int bi = item / ngroups, grp = item - bi * ngroups;   // harmonic groups fastest
+    const int blk = a.blk_first + bi;
     const int hidx0 = grp * kHG;
     const int ng = min(kHG, a.nharms - hidx0);
     const int64_t t0 = blk_t0(a, blk);
@@ -582,7 +583,8 @@ __global__ void __launch_bounds__(kI2Threads, 2) k_interp2(WaveArgs a, int win_m
     if (!ok && threadIdx.x == 0) atomicExch(err, 4);
     for (int it = 0; item < nitems && ok; item += gridDim.x, ++it) {
         const HarmStage* S = st[it & 1];
-        const int blk = item / ngroups, grp = item - blk * ngroups;
+        const int bi = item / ngroups, grp = item - bi * ngroups;
+        const int blk = a.blk_first + bi;
         const int hidx0 = grp * kHG;
         const int ng = min(kHG, a.nharms - hidx0);
         const int64_t t0 = blk_t0(a, blk);
@@ -648,22 +650,30 @@ cudaError_t launch_interp2(const WaveArgs& a, cudaStream_t st, int win_max, int*
     return cudaGetLastError();
 }
 
-// The largest |Re| or |Im| of a spectrum (NaN ignored), for the FP16 A-tile
-// scale: grid-stride maximum, warp reduction, one atomicMax on the float bits
-// (non-negative floats order like their bits) per warp.
-__global__ void __launch_bounds__(256) k_amax(const float2* __restrict__ amps, int64_t n, uint32_t* out) {
+// The largest |Re| or |Im| of each chunk of a spectrum (NaN ignored), for the
+// FP16 A-tile scale: one chunk per grid row, grid-stride maximum, warp
+// reduction, one atomicMax on the float bits (non-negative floats order like
+// their bits) per warp into out[chunk].
+__global__ void __launch_bounds__(256) k_amax(const float2* __restrict__ amps, int64_t n, int64_t chunk,
+                                               uint32_t* out) {
+    const int64_t c0 = (int64_t)blockIdx.y * chunk;
+    const int64_t c1 = min(n, c0 + chunk);
     float mx = 0.0f;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t i = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < c1;
+         i += (int64_t)gridDim.x * blockDim.x) {
         const float2 x = amps[i];
         mx = fmaxf(mx, fmaxf(fabsf(x.x), fabsf(x.y)));
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(mx));
+    if ((threadIdx.x & 31) == 0) atomicMax(out + blockIdx.y, __float_as_uint(mx));
 }
 
-cudaError_t launch_amax(const float2* amps, int64_t n, uint32_t* out, cudaStream_t st, int num_sms) {
-    k_amax<<<num_sms * 4, 256, 0, st>>>(amps, n, out);
+cudaError_t launch_amax(const float2* amps, int64_t n, int64_t chunk, int nchunk, uint32_t* out, cudaStream_t st,
+                        int num_sms) {
+    if (nchunk < 1 || nchunk > kMaxSpecChunks || chunk < 1) return cudaErrorInvalidValue;
+    const int gx = std::max(1, num_sms * 4 / nchunk);
+    k_amax<<<dim3(gx, nchunk), 256, 0, st>>>(amps, n, chunk, out);
     return cudaGetLastError();
 }
 

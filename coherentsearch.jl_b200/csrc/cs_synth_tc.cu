@@ -311,11 +311,11 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     __shared__ float inv_sh[kMaxLevels];        // 1/sigma of the tile's block, per level
     __shared__ int nv_sh[kMaxLevels];           // valid trials of the tile's block, per level
     __shared__ float cut_sh[kMaxLevels];        // gate bound for skipping a warp's scan, per level
+    __shared__ float gup_sh;                    // 2^s: undoes the tile's block's FP16 scale
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const int tiles_per_blk = a.tiles_per_blk;
-    const float gup = a.fp16 ? pow2f(ascale_exp(a.amax_bits)) : 1.0f;   // undoes the FP16 tile scale
     const int ntiles = a.nblk * tiles_per_blk;
     const int my_ntiles = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
@@ -427,6 +427,8 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
         // (the previous tile's epilogue finished at the last barrier)
         if (tid < t.nlev) {
             // 1/sigma times the A tiles' scale 2^s (exact): the gate in true units
+            const float gup = a.fp16 ? pow2f(ascale_exp_blk(a, blk)) : 1.0f;
+            if (tid == 0) gup_sh = gup;
             const float inv = inv_sigma(sig_next) * gup;
             inv_sh[tid] = inv;
             nv_sh[tid] = nv_next;
@@ -491,7 +493,7 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
             if (j >= nv_sh[l]) continue;
             float g = -INFINITY;
             for (int i = lu_start[l]; i < lu_start[l + 1]; ++i) g = fmaxf(g, part_sh[lu_idx[i]][r]);
-            if (a.Q0) a.Q0[((int64_t)blk * a.nlev + l) * a.Nprof + j] = g * gup;
+            if (a.Q0) a.Q0[((int64_t)blk * a.nlev + l) * a.Nprof + j] = g * gup_sh;
             gate_flag(a, blk, l, j, g, inv_sh[l]);
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

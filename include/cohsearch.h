@@ -115,7 +115,12 @@ const char* cs_last_error(const cs_handle* h);
 /* Attach a spectrum from HOST memory: namps complex64 values, interleaved
  * (re, im), amps[0] = DC.re + i*Nyquist, as FFTFile maps it
  * (src/fileio.jl:64-78); N = time-series length, dt = sample time (s), so
- * T = N*dt.  The data are copied to the device. */
+ * T = N*dt.  The data are copied to the device in up to 16 chunks on a copy
+ * stream of the handle's.  From page-locked memory the copy is asynchronous
+ * and the next search overlaps it, interpolating each run of blocks as soon
+ * as the chunks that run reads have landed: keep the buffer unchanged until
+ * that search (or any other call that reads the spectrum) has returned.
+ * From pageable memory the call returns once the data are staged. */
 cs_status cs_set_spectrum(cs_handle* h, const float* amps, int64_t namps, int64_t N, double dt);
 
 /* As cs_set_spectrum, but `d_amps` is already a DEVICE pointer on the

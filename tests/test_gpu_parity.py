@@ -284,7 +284,8 @@ def test_tensor_bright_spectrum_scale_invariant(synth):
     """A spectrum scaled by 2^17 (noise amplitudes ~1e5, past FP16's 65504)
     reports exactly the unscaled spectrum's candidates: a power of two scales
     every FP32 value exactly, and the FP16 A tiles carry a power-of-two range
-    scale taken from the spectrum's largest component, undone in the gate."""
+    scale taken from the largest component of the spectrum chunks their block
+    reads, undone in the gate."""
     amps, N, dt = multi_spectrum()
     big = (amps * np.float32(2.0 ** 17)).astype(np.complex64)
     assert np.abs(big.real).max() > 65504.0

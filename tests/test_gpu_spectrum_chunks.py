@@ -1,0 +1,118 @@
+"""A host spectrum arrives in chunks (cs_set_spectrum): the first search
+interpolates each run of blocks as soon as the chunks it reads have landed,
+and each block's FP16 tile scale comes from the maxima of those chunks only.
+
+  * from page-locked memory (copy overlapped with the search) and from pageable
+    memory: every record, block sigma and gate value equal to the same search
+    of a device-resident copy, for FP16, BF16 and plain FP32 synthesis, on the
+    first search (overlapped) and a second one (copy complete);
+  * a bright bin in chunk 7: the blocks that read no bin of chunks 7 and up
+    keep the gate values of the spectrum without it (their scale ignores those
+    chunks), and the FP16 records still equal the plain FP32 form's;
+  * the other calls that read the spectrum (block features) wait for the copy.
+"""
+import numpy as np
+import pytest
+
+import cohsearch as cs
+from cohsearch import synth
+from oracle import cs_ref as o
+
+pytestmark = pytest.mark.gpu
+
+THR = 8.0
+BAND = (0.1, 125.0)
+
+
+def _params(mode, nharms=60):
+    return cs.SearchParams(nharms=nharms, m=16, decimations=cs.decimation_set(nharms, 6), synth=mode, threshold=THR)
+
+
+def _search(eng):
+    got = eng.search_raw(BAND[0], BAND[1], 100, 2048, THR)
+    sig, nv = eng.block_values()
+    return got, np.asarray(sig).copy(), np.asarray(nv).copy(), eng.gate_values().copy()
+
+
+@pytest.mark.parametrize("mode", ["fp16", "bf16", "fp32"])
+def test_chunked_host_copy_equals_device_resident(mode):
+    import torch
+    amps, N, dt = synth.survey_config(seed=5)        # 2^22 bins: 16 chunks
+    namps = len(amps)
+    d = torch.from_numpy(amps.view(np.float32).copy()).cuda()
+    pinned = torch.from_numpy(amps.view(np.float32).copy()).pin_memory()
+    dev = cs.Engine(_params(mode))
+    dev.set_diagnostics(2)
+    dev.set_spectrum_device(d.data_ptr(), namps, N, dt, keep=d)
+    want = _search(dev)
+    launches_dev = dev.stats()["launches"]
+    assert len(want[0]) > 0
+
+    eng = cs.Engine(_params(mode))
+    eng.set_diagnostics(2)
+    eng.set_spectrum_host(pinned.data_ptr(), namps, N, dt)
+    first = _search(eng)                              # overlapped with the copy
+    assert eng.stats()["launches"] > launches_dev     # interpolation ran run by run
+    second = _search(eng)                             # copy complete: one launch
+    pageable = cs.Engine(_params(mode))
+    pageable.set_diagnostics(2)
+    pageable.set_spectrum(cs.FFTFile.from_array(amps, N, dt))
+    third = _search(pageable)
+    for got in (first, second, third):
+        assert np.array_equal(got[0], want[0])
+        assert np.array_equal(got[1], want[1])
+        assert np.array_equal(got[2], want[2])
+        assert np.array_equal(got[3].view(np.uint32), want[3].view(np.uint32))
+
+
+def test_bright_bin_scales_only_the_blocks_past_its_chunk():
+    """2^21 samples (16 chunks of 65,536 bins; the band's harmonics reach
+    chunk 8); one bin of chunk 7 set to 2^17 times the spectrum's largest
+    component."""
+    import torch
+    N, dt = 1 << 21, 64e-6
+    amps = synth.make_spectrum(N, dt, [synth.Pulsar(7.3, 0.05, 30.0, 0.4), synth.Pulsar(91.1, 0.1, 25.0, 0.1)], 21)
+    namps = len(amps)
+    chunk = 65536
+    assert namps == 16 * chunk
+    spike = amps.copy()
+    spike[7 * chunk + 1000] = np.complex64(np.abs(amps.view(np.float32)).max() * 2.0 ** 17)
+    res = {}
+    for name, a in (("clean", amps), ("spike", spike)):
+        for mode in ("fp16", "fp32"):
+            eng = cs.Engine(_params(mode, nharms=32))
+            eng.set_diagnostics(2)
+            h = torch.from_numpy(a.view(np.float32).copy()).pin_memory()
+            eng.set_spectrum_host(h.data_ptr(), namps, N, dt)
+            res[name, mode] = _search(eng)
+    # the FP16 records equal the plain form's, with and without the bright bin
+    for name in ("clean", "spike"):
+        assert np.array_equal(res[name, "fp16"][0], res[name, "fp32"][0])
+    # blocks whose highest bin lies below chunk 7: same gates as without it
+    op = o.SearchParams(nharms=32, m=16)
+    T, lodr, r_lo, r_hi, total, _ = o.search_setup(N, dt, op, BAND[0], BAND[1], 100, 2048)
+    nblk = (total + 2047) // 2048
+    last_trial = np.minimum(np.arange(1, nblk + 1) * 2048, total) - 1
+    top = np.floor(32 * (r_lo + last_trial * lodr)) + 8 + 4
+    early = top < 7 * chunk
+    assert 0 < early.sum() < nblk
+    nlev = len(cs.decimation_set(32, 6))
+    g_clean = res["clean", "fp16"][3].reshape(nblk, nlev, 2048)
+    g_spike = res["spike", "fp16"][3].reshape(nblk, nlev, 2048)
+    assert np.array_equal(g_clean[early].view(np.uint32), g_spike[early].view(np.uint32))
+    assert not np.array_equal(g_clean[~early].view(np.uint32), g_spike[~early].view(np.uint32))
+
+
+def test_features_wait_for_the_chunked_copy():
+    import torch
+    amps, N, dt = synth.survey_config(seed=6)
+    namps = len(amps)
+    d = torch.from_numpy(amps.view(np.float32).copy()).cuda()
+    dev = cs.Engine(_params("fp16"))
+    dev.set_spectrum_device(d.data_ptr(), namps, N, dt, keep=d)
+    want = dev.block_features(BAND[0], BAND[1], 100, 2048)
+    pinned = torch.from_numpy(amps.view(np.float32).copy()).pin_memory()
+    eng = cs.Engine(_params("fp16"))
+    eng.set_spectrum_host(pinned.data_ptr(), namps, N, dt)
+    got = eng.block_features(BAND[0], BAND[1], 100, 2048)
+    assert np.array_equal(got.cpu().numpy(), want.cpu().numpy())

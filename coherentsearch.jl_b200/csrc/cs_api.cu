@@ -356,13 +356,27 @@ cs_status cuda_fail(cs_handle* H, cudaError_t e, const char* where) {
         if (e_ != cudaSuccess) return cuda_fail(H, e_, where); \
     } while (0)
 
-// Chunks of a spectrum of namps bins: at least 64 Ki bins each, at most
-// kMaxSpecChunks of them.  Host and device spectra use the same layout, so a
-// block's FP16 tile scale does not depend on where its spectrum came from.
-static void spec_chunks(int64_t namps, int64_t* chunk, int* nchunk) {
-    const int64_t c = std::max<int64_t>((namps + kMaxSpecChunks - 1) / kMaxSpecChunks, (int64_t)1 << 16);
-    *chunk = c;
-    *nchunk = (int)std::max<int64_t>(1, (namps + c - 1) / c);
+// Chunks of a spectrum of namps bins, doubling in size: chunk 0 holds bins
+// [0, u), chunk c >= 1 bins [u*2^(c-1), u*2^c), with u = max(namps/32, 64 Ki)
+// (rounded up), so at most 6 chunks (spec_chunk_lo/hi, shared with k_amax).
+// A block of trials near r reads bins up to about nharms*r, so the blocks in
+// frequency order need growing prefixes: each chunk lands before the search
+// has interpolated the blocks of the chunks below it.  Host and device spectra
+// use the same layout, so a block's FP16 tile scale does not depend on where
+// its spectrum came from.
+static void spec_chunks(int64_t namps, int64_t* unit, int* nchunk) {
+    const int64_t u = std::max<int64_t>((namps + 31) / 32, (int64_t)1 << 16);
+    int n = 1;
+    while (spec_chunk_hi(u, n - 1, namps) < namps) ++n;
+    *unit = u;
+    *nchunk = n;
+}
+
+// The chunk holding bin x (>= 0) of a spectrum of chunk unit u, at most last.
+static int spec_chunk_of(int64_t x, int64_t u, int last) {
+    int c = 0;
+    while (c < last && x >= spec_chunk_hi(u, c, INT64_MAX)) ++c;
+    return c;
 }
 
 // Work on H->stream that reads the attached spectrum at once waits for the
@@ -732,9 +746,9 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
     // The spectrum's chunks: a host spectrum still being copied in chunks is
     // interpolated run of blocks by run of blocks as its chunks land (first
     // wave only; later work waits for the whole copy).
-    int64_t chunk = 0;
+    int64_t unit = 0;
     int nch = 0;
-    spec_chunks(H->namps, &chunk, &nch);
+    spec_chunks(H->namps, &unit, &nch);
     const bool host_spec = H->amps == H->chunked_amps;
     if (host_spec && nch != H->spec_nchunk) return fail(H, CS_ERR_INVALID_ARGUMENT, "spectrum chunk layout changed");
     bool overlap = host_spec && H->chunks_pending && !R.capture;
@@ -747,7 +761,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
     } else if (fp16_scale) {
         if (!R.capture) CS_CUDA(H->d_amax.ensure(kMaxSpecChunks * sizeof(uint32_t)), "alloc chunk maxima");
         CS_CUDA(cudaMemsetAsync(H->d_amax.p, 0, kMaxSpecChunks * sizeof(uint32_t), H->stream), "reset chunk maxima");
-        CS_CUDA(launch_amax(H->amps, H->namps, chunk, nch, H->d_amax.as<uint32_t>(), H->stream, H->num_sms),
+        CS_CUDA(launch_amax(H->amps, H->namps, unit, nch, H->d_amax.as<uint32_t>(), H->stream, H->num_sms),
                 "maximum launch");
         S.launches += 1;
         amax = H->d_amax.as<uint32_t>();
@@ -849,7 +863,7 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             // block's last trial, m/2 taps past it, and a margin for rounding
             const double top = std::floor((double)p.nharms * (rstart + (double)(n - 1) * R.lodr));
             const int64_t bin_max = top < 0 ? 0 : (top > 4.0e18 ? INT64_MAX / 2 : (int64_t)top) + p.m / 2 + 4;
-            cidx[b] = (int32_t)std::min<int64_t>(nch - 1, bin_max / chunk);
+            cidx[b] = spec_chunk_of(bin_max, unit, nch - 1);
             for (int l = 0; l < nlev; ++l) {
                 const int k = H->dlev[l].k;
                 nvalid[(size_t)b * nlev + l] = (k == 1) ? n : nvalid_decim(k, rstart, R.lodr, n, nyq);
@@ -1252,15 +1266,16 @@ cs_status cs_set_spectrum(cs_handle* H, const float* amps, int64_t namps, int64_
     CS_CUDA(H->d_amax_spec.ensure(kMaxSpecChunks * sizeof(uint32_t)), "alloc chunk maxima");
     CS_CUDA(cudaMemsetAsync(H->d_amax_spec.p, 0, kMaxSpecChunks * sizeof(uint32_t), H->copy_stream),
             "reset chunk maxima");
-    int64_t chunk = 0;
+    int64_t unit = 0;
     int nch = 0;
-    spec_chunks(namps, &chunk, &nch);
+    spec_chunks(namps, &unit, &nch);
     float2* dst = H->amps_owned.as<float2>();
     for (int c = 0; c < nch; ++c) {
-        const int64_t b0 = (int64_t)c * chunk, nb = std::min(chunk, namps - b0);
+        const int64_t b0 = spec_chunk_lo(unit, c), nb = spec_chunk_hi(unit, c, namps) - b0;
         CS_CUDA(cudaMemcpyAsync(dst + b0, amps + 2 * b0, (size_t)nb * sizeof(float2), cudaMemcpyHostToDevice,
                                 H->copy_stream),
                 "copy spectrum");
+        // a one-chunk layout of the chunk alone: its maximum into slot c
         CS_CUDA(launch_amax(dst + b0, nb, nb, 1, H->d_amax_spec.as<uint32_t>() + c, H->copy_stream, H->num_sms),
                 "chunk maximum launch");
         CS_CUDA(cudaEventRecord(H->chunk_ev[c], H->copy_stream), "event");

@@ -14,7 +14,7 @@ namespace cs {
 constexpr int kMaxLevels = 16;     // decimation factors per search
 constexpr int kMaxWidths = 64;     // boxcar widths per level
 constexpr int kMaxBins = 256;      // profile bins (nharms <= 128)
-constexpr int kMaxSpecChunks = 16;  // a host spectrum arrives in up to this many chunks
+constexpr int kMaxSpecChunks = 16;  // room for a spectrum's chunk maxima (it has at most 6 chunks)
 constexpr int kSigmaCap = 8192;    // _BOXCAR_SIGMA_SAMPLES, src/search.jl:462
 constexpr int kTileTrials = 64;    // trials per CTA in the FP32 synthesis kernel
 constexpr int kATileBytes = 128 * 128 * 2;  // one 16-bit A tile: 128 trials x 128 K
@@ -372,9 +372,15 @@ cudaError_t launch_mlp_backward(const cs_mlp& net, const float* x, const float* 
                                 const cs_mlp_grads& g, float* loss, cudaStream_t st);
 cudaError_t launch_adam(const cs_adam_param& p, float lr, float b1, float b2, float eps, int step, cudaStream_t st);
 cudaError_t launch_to_bf16(const float* p, uint16_t* pb, int64_t n, cudaStream_t st);
-// Largest |Re| or |Im| of each chunk [c*chunk, min(n, (c+1)*chunk)), c < nchunk,
-// atomically maxed into out[c] (zeroed by the caller).
-cudaError_t launch_amax(const float2* amps, int64_t n, int64_t chunk, int nchunk, uint32_t* out, cudaStream_t st,
+// Bins of chunk c of a spectrum of n bins and chunk unit u: [lo, hi), chunk
+// sizes doubling after the first (chunk 0: [0, u); chunk c: [u*2^(c-1), u*2^c)).
+__host__ __device__ inline int64_t spec_chunk_lo(int64_t u, int c) { return c == 0 ? 0 : u << (c - 1); }
+__host__ __device__ inline int64_t spec_chunk_hi(int64_t u, int c, int64_t n) {
+    return (u << c) < n ? (u << c) : n;
+}
+// Largest |Re| or |Im| of each chunk c < nchunk of a spectrum of n bins and
+// chunk unit u, atomically maxed into out[c] (zeroed by the caller).
+cudaError_t launch_amax(const float2* amps, int64_t n, int64_t unit, int nchunk, uint32_t* out, cudaStream_t st,
                         int num_sms);
 
 // block_metrics (reference path): per harmonic, the fine-grid origin, its

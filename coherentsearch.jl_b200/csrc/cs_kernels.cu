@@ -121,7 +121,7 @@ constexpr int kHG = 4;   // harmonics per interpolation CTA: one 16-byte K chunk
 // (tensor synthesis), and the exact FP32 amplitudes of the columns each
 // level's block sigma pools.
 __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, int Nst, int blk, int hidx0,
-                                          int ng, int n) {
+                                          int ng, int n, float sc) {
     if (a.X) {
         for (int g = 0; g < ng; ++g) {
             float2* xrow = a.X + ((int64_t)blk * a.nharms + hidx0 + g) * a.Nprof;
@@ -139,7 +139,6 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
         const float2* x2 = xo + 2 * Nst;
         const float2* x3 = xo + 3 * Nst;
         const float2 z = make_float2(0.0f, 0.0f);
-        const float sc = a.fp16 ? pow2f(-ascale_exp_blk(a, blk)) : 1.0f;   // exact power of two
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
             const float2 v0 = xo[j];
             const float2 v1 = ng > 1 ? x1[j] : z;
@@ -355,6 +354,7 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
     __shared__ long long s_lo[kHG], s_base[kHG];   // s_base = rfloor0 + qint0 - lo + 1 - m2
     __shared__ unsigned long long s_qm[kHG];       // ceil(2^64 / q): (n div q) = mulhi(n, s_qm) for n < 2^32
     __shared__ unsigned s_pm[kHG];                 // ceil(2^24 / P): (task div P) for task * P < 2^24
+    __shared__ float s_sc;                         // FP16 A tiles: the block's scale 2^-s (exact)
 
     // harmonic groups fastest: the CTAs filling one block's A tiles (each a
     // 128-byte piece of every 2 KB row group) run together
@@ -367,6 +367,7 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
     const int n = (int)min((int64_t)a.Nprof, a.total - t0);
     if (n <= 0) return;
 
+    if (threadIdx.x == 0) s_sc = a.fp16 && a.Atile ? pow2f(-ascale_exp_blk(a, blk)) : 1.0f;
     if (threadIdx.x < ng) {
         // Range guard on the TRUE trial range (src/directinterp.jl:490-496),
         // with the Julia 1-based bounds translated to 0-based windows.
@@ -463,7 +464,7 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
         }
     }
     __syncthreads();
-    emit_rows(a, xo, Nst, blk, hidx0, ng, n);
+    emit_rows(a, xo, Nst, blk, hidx0, ng, n, s_sc);
 }
 
 // ---------------------------------------------------------------------------
@@ -485,6 +486,7 @@ struct HarmStage {
     int head;           // window element 0 sits at stage + head (1 when its address is not 16-byte aligned)
     int p0, res0, Ub, Tc, chunk, small, Hs;
     unsigned pm;        // ceil(2^24 / P)
+    float sc;           // FP16 A tiles: the block's scale 2^-s (exact), the same in every slot
     long long base;     // rfloor0 + qint0 - lo + 1 - m2
     unsigned long long qm;   // ceil(2^64 / q), q > 1
 };
@@ -543,6 +545,7 @@ __device__ void i2_prepare(const WaveArgs& a, int item, int ngroups, int win_max
         h.Tc = Tc;
         h.chunk = (Ub + 1 + Tc - 1) / Tc;
         h.small = ((uint64_t)hp.q + (uint64_t)P * (uint64_t)hpn) < 0xFFFFFFFFull && hp.q > 1;
+        h.sc = a.fp16 && a.Atile ? pow2f(-ascale_exp_blk(a, blk)) : 1.0f;
         h.Hs = (int)(((int64_t)P * hpn) / hp.q);   // bins between trials t and t+P
         h.qm = hp.q > 1 ? 0xFFFFFFFFFFFFFFFFull / (uint64_t)hp.q + 1ull : 0ull;
         h.pm = (unsigned)((((uint64_t)1 << 24) + (uint64_t)P - 1) / (uint64_t)P);
@@ -628,7 +631,7 @@ __global__ void __launch_bounds__(kI2Threads, 2) k_interp2(WaveArgs a, int win_m
         const int nxt = item + (int)gridDim.x;
         if (nxt < nitems && warp == 0) i2_prepare(a, nxt, ngroups, win_max, stage, st[(it + 1) & 1], &wbar, err);
         if (nxt < nitems) pend = (uint32_t)((it + 1) & 1);
-        emit_rows(a, xo, Nst, blk, hidx0, ng, n);
+        emit_rows(a, xo, Nst, blk, hidx0, ng, n, S[0].sc);
         // rows emitted; the next item's windows have landed (bounded wait)
         ok = __syncthreads_or(nxt < nitems && !mbar_wait(&wbar, (uint32_t)((it + 1) & 1))) == 0;
         if (!ok && threadIdx.x == 0) atomicExch(err, 4);
@@ -654,10 +657,10 @@ cudaError_t launch_interp2(const WaveArgs& a, cudaStream_t st, int win_max, int*
 // FP16 A-tile scale: one chunk per grid row, grid-stride maximum, warp
 // reduction, one atomicMax on the float bits (non-negative floats order like
 // their bits) per warp into out[chunk].
-__global__ void __launch_bounds__(256) k_amax(const float2* __restrict__ amps, int64_t n, int64_t chunk,
+__global__ void __launch_bounds__(256) k_amax(const float2* __restrict__ amps, int64_t n, int64_t unit,
                                                uint32_t* out) {
-    const int64_t c0 = (int64_t)blockIdx.y * chunk;
-    const int64_t c1 = min(n, c0 + chunk);
+    const int64_t c0 = spec_chunk_lo(unit, (int)blockIdx.y);
+    const int64_t c1 = spec_chunk_hi(unit, (int)blockIdx.y, n);
     float mx = 0.0f;
     for (int64_t i = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < c1;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -669,11 +672,11 @@ __global__ void __launch_bounds__(256) k_amax(const float2* __restrict__ amps, i
     if ((threadIdx.x & 31) == 0) atomicMax(out + blockIdx.y, __float_as_uint(mx));
 }
 
-cudaError_t launch_amax(const float2* amps, int64_t n, int64_t chunk, int nchunk, uint32_t* out, cudaStream_t st,
+cudaError_t launch_amax(const float2* amps, int64_t n, int64_t unit, int nchunk, uint32_t* out, cudaStream_t st,
                         int num_sms) {
-    if (nchunk < 1 || nchunk > kMaxSpecChunks || chunk < 1) return cudaErrorInvalidValue;
+    if (nchunk < 1 || nchunk > kMaxSpecChunks || unit < 1) return cudaErrorInvalidValue;
     const int gx = std::max(1, num_sms * 4 / nchunk);
-    k_amax<<<dim3(gx, nchunk), 256, 0, st>>>(amps, n, chunk, out);
+    k_amax<<<dim3(gx, nchunk), 256, 0, st>>>(amps, n, unit, out);
     return cudaGetLastError();
 }
 

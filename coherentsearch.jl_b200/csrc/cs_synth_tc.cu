@@ -405,12 +405,13 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     }
     // The per-level sigma and valid counts of the first tile's block; each
     // iteration then loads the next tile's while its own epilogue runs.
-    float sig_next = 0.0f;
+    float sig_next = 0.0f, gup_next = 1.0f;   // gup: 2^s, undoes the block's FP16 tile scale
     int nv_next = 0;
     if (tid < t.nlev && my_ntiles > 0) {
         const int b0 = (int)blockIdx.x / tiles_per_blk;
         sig_next = a.sigma[b0 * a.nlev + tid];
         nv_next = a.nvalid[b0 * a.nlev + tid];
+        if (a.fp16) gup_next = pow2f(ascale_exp_blk(a, b0));
     }
     ok = __syncthreads_and(mma_ok_sh != 0) != 0;
     if (!ok && tid == 0) atomicExch(err, 2);
@@ -427,7 +428,7 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
         // (the previous tile's epilogue finished at the last barrier)
         if (tid < t.nlev) {
             // 1/sigma times the A tiles' scale 2^s (exact): the gate in true units
-            const float gup = a.fp16 ? pow2f(ascale_exp_blk(a, blk)) : 1.0f;
+            const float gup = gup_next;
             if (tid == 0) gup_sh = gup;
             const float inv = inv_sigma(sig_next) * gup;
             inv_sh[tid] = inv;
@@ -442,6 +443,7 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
                 const int bn = (tile + (int)gridDim.x) / tiles_per_blk;
                 sig_next = a.sigma[bn * a.nlev + tid];
                 nv_next = a.nvalid[bn * a.nlev + tid];
+                if (a.fp16) gup_next = pow2f(ascale_exp_blk(a, bn));
             }
         }
         // this tile's product has completed: its accumulators are readable and

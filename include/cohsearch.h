@@ -115,8 +115,8 @@ const char* cs_last_error(const cs_handle* h);
 /* Attach a spectrum from HOST memory: namps complex64 values, interleaved
  * (re, im), amps[0] = DC.re + i*Nyquist, as FFTFile maps it
  * (src/fileio.jl:64-78); N = time-series length, dt = sample time (s), so
- * T = N*dt.  The data are copied to the device in up to 16 chunks on a copy
- * stream of the handle's.  From page-locked memory the copy is asynchronous
+ * T = N*dt.  The data are copied to the device in chunks of doubling size
+ * (at most 6) on a copy stream of the handle's.  From page-locked memory the copy is asynchronous
  * and the next search overlaps it, interpolating each run of blocks as soon
  * as the chunks that run reads have landed: keep the buffer unchanged until
  * that search (or any other call that reads the spectrum) has returned.

@@ -1,12 +1,13 @@
-"""A host spectrum arrives in chunks (cs_set_spectrum): the first search
-interpolates each run of blocks as soon as the chunks it reads have landed,
-and each block's FP16 tile scale comes from the maxima of those chunks only.
+"""A host spectrum arrives in chunks of doubling size (cs_set_spectrum): the
+first search interpolates each run of blocks as soon as the chunks it reads
+have landed, and each block's FP16 tile scale comes from the maxima of those
+chunks only.
 
   * from page-locked memory (copy overlapped with the search) and from pageable
     memory: every record, block sigma and gate value equal to the same search
     of a device-resident copy, for FP16, BF16 and plain FP32 synthesis, on the
     first search (overlapped) and a second one (copy complete);
-  * a bright bin in chunk 7: the blocks that read no bin of chunks 7 and up
+  * a bright bin in chunk 3: the blocks that read no bin of chunks 3 and up
     keep the gate values of the spectrum without it (their scale ignores those
     chunks), and the FP16 records still equal the plain FP32 form's;
   * the other calls that read the spectrum (block features) wait for the copy.
@@ -28,6 +29,16 @@ def _params(mode, nharms=60):
     return cs.SearchParams(nharms=nharms, m=16, decimations=cs.decimation_set(nharms, 6), synth=mode, threshold=THR)
 
 
+def chunk_of(x, namps):
+    """The chunk holding bin x: chunk 0 is [0, u), chunk c >= 1 is
+    [u*2^(c-1), u*2^c), u = max(ceil(namps/32), 65536)."""
+    u = max(-(-namps // 32), 1 << 16)
+    c = 0
+    while min(u << c, namps) <= x and (u << c) < namps:
+        c += 1
+    return c
+
+
 def _search(eng):
     got = eng.search_raw(BAND[0], BAND[1], 100, 2048, THR)
     sig, nv = eng.block_values()
@@ -37,7 +48,7 @@ def _search(eng):
 @pytest.mark.parametrize("mode", ["fp16", "bf16", "fp32"])
 def test_chunked_host_copy_equals_device_resident(mode):
     import torch
-    amps, N, dt = synth.survey_config(seed=5)        # 2^22 bins: 16 chunks
+    amps, N, dt = synth.survey_config(seed=5)        # 2^22 bins: 6 chunks
     namps = len(amps)
     d = torch.from_numpy(amps.view(np.float32).copy()).cuda()
     pinned = torch.from_numpy(amps.view(np.float32).copy()).pin_memory()
@@ -66,17 +77,18 @@ def test_chunked_host_copy_equals_device_resident(mode):
 
 
 def test_bright_bin_scales_only_the_blocks_past_its_chunk():
-    """2^21 samples (16 chunks of 65,536 bins; the band's harmonics reach
-    chunk 8); one bin of chunk 7 set to 2^17 times the spectrum's largest
-    component."""
+    """2^21 samples (chunks [0, 64Ki), [64Ki, 128Ki), ..., [512Ki, 1Mi); the
+    band's harmonics reach bin 537 Ki); one bin of chunk 3 set to 2^17 times
+    the spectrum's largest component."""
     import torch
     N, dt = 1 << 21, 64e-6
     amps = synth.make_spectrum(N, dt, [synth.Pulsar(7.3, 0.05, 30.0, 0.4), synth.Pulsar(91.1, 0.1, 25.0, 0.1)], 21)
     namps = len(amps)
-    chunk = 65536
-    assert namps == 16 * chunk
+    assert namps == 1 << 20
+    bright = 300_000
+    assert chunk_of(bright, namps) == 3 and chunk_of(262_143, namps) == 2
     spike = amps.copy()
-    spike[7 * chunk + 1000] = np.complex64(np.abs(amps.view(np.float32)).max() * 2.0 ** 17)
+    spike[bright] = np.complex64(np.abs(amps.view(np.float32)).max() * 2.0 ** 17)
     res = {}
     for name, a in (("clean", amps), ("spike", spike)):
         for mode in ("fp16", "fp32"):
@@ -88,13 +100,13 @@ def test_bright_bin_scales_only_the_blocks_past_its_chunk():
     # the FP16 records equal the plain form's, with and without the bright bin
     for name in ("clean", "spike"):
         assert np.array_equal(res[name, "fp16"][0], res[name, "fp32"][0])
-    # blocks whose highest bin lies below chunk 7: same gates as without it
+    # blocks whose highest bin lies below chunk 3: same gates as without it
     op = o.SearchParams(nharms=32, m=16)
     T, lodr, r_lo, r_hi, total, _ = o.search_setup(N, dt, op, BAND[0], BAND[1], 100, 2048)
     nblk = (total + 2047) // 2048
     last_trial = np.minimum(np.arange(1, nblk + 1) * 2048, total) - 1
     top = np.floor(32 * (r_lo + last_trial * lodr)) + 8 + 4
-    early = top < 7 * chunk
+    early = np.array([chunk_of(int(x), namps) < 3 for x in top])
     assert 0 < early.sum() < nblk
     nlev = len(cs.decimation_set(32, 6))
     g_clean = res["clean", "fp16"][3].reshape(nblk, nlev, 2048)

@@ -354,7 +354,8 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
     __shared__ long long s_lo[kHG], s_base[kHG];   // s_base = rfloor0 + qint0 - lo + 1 - m2
     __shared__ unsigned long long s_qm[kHG];       // ceil(2^64 / q): (n div q) = mulhi(n, s_qm) for n < 2^32
     __shared__ unsigned s_pm[kHG];                 // ceil(2^24 / P): (task div P) for task * P < 2^24
-    __shared__ float s_sc;                         // FP16 A tiles: the block's scale 2^-s (exact)
+    __shared__ uint32_t s_am[kMaxSpecChunks];      // FP16 A tiles: the spectrum chunks' maxima
+    __shared__ int s_cidx;                         // and the block's last chunk: its scale 2^-s
 
     // harmonic groups fastest: the CTAs filling one block's A tiles (each a
     // 128-byte piece of every 2 KB row group) run together
@@ -367,7 +368,10 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
     const int n = (int)min((int64_t)a.Nprof, a.total - t0);
     if (n <= 0) return;
 
-    if (threadIdx.x == 0) s_sc = a.fp16 && a.Atile ? pow2f(-ascale_exp_blk(a, blk)) : 1.0f;
+    // (loaded by warps 1-2 beside warp 0's per-harmonic set-up, not after it)
+    if (threadIdx.x >= 32 && threadIdx.x < 32 + kMaxSpecChunks)
+        s_am[threadIdx.x - 32] = a.amax_bits ? a.amax_bits[threadIdx.x - 32] : 0u;
+    if (threadIdx.x == 32 + kMaxSpecChunks) s_cidx = a.blk_cidx ? a.blk_cidx[blk] : kMaxSpecChunks - 1;
     if (threadIdx.x < ng) {
         // Range guard on the TRUE trial range (src/directinterp.jl:490-496),
         // with the Julia 1-based bounds translated to 0-based windows.
@@ -464,7 +468,8 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
         }
     }
     __syncthreads();
-    emit_rows(a, xo, Nst, blk, hidx0, ng, n, s_sc);
+    const float sc = a.fp16 && a.Atile ? pow2f(-ascale_exp(s_am, s_cidx)) : 1.0f;   // exact power of two
+    emit_rows(a, xo, Nst, blk, hidx0, ng, n, sc);
 }
 
 // ---------------------------------------------------------------------------

@@ -312,6 +312,7 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     __shared__ int nv_sh[kMaxLevels];           // valid trials of the tile's block, per level
     __shared__ float cut_sh[kMaxLevels];        // gate bound for skipping a warp's scan, per level
     __shared__ float gup_sh;                    // 2^s: undoes the tile's block's FP16 scale
+    __shared__ float gup_chunk_sh[kMaxSpecChunks];   // 2^s of a block whose last spectrum chunk is c
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
@@ -325,6 +326,10 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     if (tid < t.nlev) lev_sh[tid] = t.lev[tid];
     if (tid < t.nunit) unit_sh[tid] = t.unit[tid];
     if (tid < t.nmma) mma_sh[tid] = t.mma[tid];
+    // the chunk maxima are the search's constants: each chunk index's scale,
+    // once per CTA, so that a tile needs only its block's chunk index
+    if (tid >= 32 && tid < 32 + kMaxSpecChunks)
+        gup_chunk_sh[tid - 32] = a.fp16 ? pow2f(ascale_exp(a.amax_bits, tid - 32)) : 1.0f;
     if (tid == 0) {
         // each level's units, listed contiguously, for the per-level gate maximum
         int c = 0;
@@ -405,13 +410,13 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     }
     // The per-level sigma and valid counts of the first tile's block; each
     // iteration then loads the next tile's while its own epilogue runs.
-    float sig_next = 0.0f, gup_next = 1.0f;   // gup: 2^s, undoes the block's FP16 tile scale
-    int nv_next = 0;
+    float sig_next = 0.0f;
+    int nv_next = 0, cidx_next = kMaxSpecChunks - 1;   // the block's last spectrum chunk: its FP16 scale
     if (tid < t.nlev && my_ntiles > 0) {
         const int b0 = (int)blockIdx.x / tiles_per_blk;
         sig_next = a.sigma[b0 * a.nlev + tid];
         nv_next = a.nvalid[b0 * a.nlev + tid];
-        if (a.fp16) gup_next = pow2f(ascale_exp_blk(a, b0));
+        if (a.blk_cidx) cidx_next = a.blk_cidx[b0];
     }
     ok = __syncthreads_and(mma_ok_sh != 0) != 0;
     if (!ok && tid == 0) atomicExch(err, 2);
@@ -428,7 +433,7 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
         // (the previous tile's epilogue finished at the last barrier)
         if (tid < t.nlev) {
             // 1/sigma times the A tiles' scale 2^s (exact): the gate in true units
-            const float gup = gup_next;
+            const float gup = gup_chunk_sh[cidx_next];
             if (tid == 0) gup_sh = gup;
             const float inv = inv_sigma(sig_next) * gup;
             inv_sh[tid] = inv;
@@ -443,7 +448,7 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
                 const int bn = (tile + (int)gridDim.x) / tiles_per_blk;
                 sig_next = a.sigma[bn * a.nlev + tid];
                 nv_next = a.nvalid[bn * a.nlev + tid];
-                if (a.fp16) gup_next = pow2f(ascale_exp_blk(a, bn));
+                if (a.blk_cidx) cidx_next = a.blk_cidx[bn];
             }
         }
         // this tile's product has completed: its accumulators are readable and

@@ -332,7 +332,11 @@ def run_ours(args, rank, world, local_rank):
 
     lof, hif = args.band if args.band else (LOF, HIF)
     # launch shapes from the autotuner (setup, outside the timed region)
-    tune = None if args.no_tune else eng.autotune(lof, hif, 100, BLOCK, nsample=256)
+    if args.shapes:
+        # fixed launch shapes (reproducible profiling runs): no tuner launches
+        i_k, s_k, d0, d1, db = args.shapes
+        eng.set_launch_shapes(interp_kernel=i_k, sigma_kernel=s_k, tc_double_buffer=db, tc_div=(d0, d1))
+    tune = None if (args.no_tune or args.shapes) else eng.autotune(lof, hif, 100, BLOCK, nsample=1024)
 
     # Device-resident step: the search of the resident spectrum through the
     # batch entry point with its captured graph (cs_set_batch_graph): the
@@ -402,7 +406,7 @@ def run_ours(args, rank, world, local_rank):
         eng32.set_stream(stream.cuda_stream)
         eng32.set_spectrum_device(d_amps.data_ptr(), namps, N, dt, keep=d_amps)
         if not args.no_tune:
-            eng32.autotune(lof, hif, 100, BLOCK, nsample=256)
+            eng32.autotune(lof, hif, 100, BLOCK, nsample=1024)
         eng32.set_batch_graph(not args.no_graph)
         for _ in range(2):
             c32 = eng32.search_batch_raw(dev_batch, lof, hif, 100, BLOCK, THR, on_device=True)[0]
@@ -490,6 +494,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison run")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuner)")
+    ap.add_argument("--shapes", type=int, nargs=5, default=None, metavar=("INTERP", "SIGMA", "DIV0", "DIV1", "DBUF"),
+                    help="fixed launch shapes instead of the autotuner (cs_set_launch_shapes): interpolation kernel "
+                         "(0 per item, 1 persistent), sigma kernel (0 or 1), epilogue divisors, TMEM double buffer")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 

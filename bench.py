@@ -336,7 +336,7 @@ def run_ours(args, rank, world, local_rank):
         # fixed launch shapes (reproducible profiling runs): no tuner launches
         i_k, s_k, d0, d1, db = args.shapes
         eng.set_launch_shapes(interp_kernel=i_k, sigma_kernel=s_k, tc_double_buffer=db, tc_div=(d0, d1))
-    tune = None if (args.no_tune or args.shapes) else eng.autotune(lof, hif, 100, BLOCK, nsample=1024)
+    tune = None if (args.no_tune or args.shapes) else eng.autotune(lof, hif, 100, BLOCK, nsample=4096)
 
     # Device-resident step: the search of the resident spectrum through the
     # batch entry point with its captured graph (cs_set_batch_graph): the
@@ -406,7 +406,7 @@ def run_ours(args, rank, world, local_rank):
         eng32.set_stream(stream.cuda_stream)
         eng32.set_spectrum_device(d_amps.data_ptr(), namps, N, dt, keep=d_amps)
         if not args.no_tune:
-            eng32.autotune(lof, hif, 100, BLOCK, nsample=1024)
+            eng32.autotune(lof, hif, 100, BLOCK, nsample=4096)
         eng32.set_batch_graph(not args.no_graph)
         for _ in range(2):
             c32 = eng32.search_batch_raw(dev_batch, lof, hif, 100, BLOCK, THR, on_device=True)[0]

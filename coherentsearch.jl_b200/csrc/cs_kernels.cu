@@ -120,8 +120,12 @@ constexpr int kHG = 4;   // harmonics per interpolation CTA: one 16-byte K chunk
 // (plain synthesis) or one 16-byte K chunk per trial of the block's A tiles
 // (tensor synthesis), and the exact FP32 amplitudes of the columns each
 // level's block sigma pools.
+// pair_jh[g*nlev + l]: the index jh of harmonic hidx0+g+1 among level l's
+// harmonics (h/k - 1), or -1 when the level does not fold it; pair_ncap[l] =
+// max(1, kSigmaCap/nbins).  Both optional (nullptr: computed per pair here).
 __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, int Nst, int blk, int hidx0,
-                                          int ng, int n, float sc) {
+                                          int ng, int n, float sc, const short* pair_jh = nullptr,
+                                          const int* pair_ncap = nullptr) {
     if (a.X) {
         for (int g = 0; g < ng; ++g) {
             float2* xrow = a.X + ((int64_t)blk * a.nharms + hidx0 + g) * a.Nprof;
@@ -186,28 +190,53 @@ __device__ __forceinline__ void emit_rows(const WaveArgs& a, const float2* xo, i
     }
     if (!a.samp) return;
     // One warp per (harmonic, level) pair whose level folds this harmonic;
-    // lanes over its pooled columns j_c = (c*nv) div ncs (src/search.jl:528-537),
-    // the division by ncs done as a multiply-high by ceil(2^64/ncs), exact for
-    // every 32-bit dividend.
+    // lanes over its pooled columns j_c = (c*nv) div ncs (src/search.jl:528-537).
     const int lane = threadIdx.x & 31;
     const int nwarps = blockDim.x >> 5;
-    for (int e = threadIdx.x >> 5; e < ng * a.nlev; e += nwarps) {
-        const int g = e / a.nlev, l = e - g * a.nlev;
-        const int h = hidx0 + g + 1;
+    const int npair = ng * a.nlev;
+    for (int e = threadIdx.x >> 5; e < npair; e += nwarps) {
+        int g = 0, l = e;
+        while (l >= a.nlev) {
+            l -= a.nlev;
+            ++g;
+        }
         const DevLevel& L = a.levels[l];
-        if (h % L.k != 0 || h / L.k > L.Hk) continue;
+        int jh;
+        if (pair_jh) {
+            jh = pair_jh[e];
+        } else {
+            const int h = hidx0 + g + 1;
+            jh = (h % L.k == 0 && h / L.k <= L.Hk) ? h / L.k - 1 : -1;
+        }
+        if (jh < 0) continue;
         const int nv = a.nvalid[blk * a.nlev + l];
         if (nv <= 0) continue;
         const bool all = (int64_t)L.nbins * nv <= kSigmaCap;
-        const int ncs = all ? nv : min(nv, max(1, kSigmaCap / L.nbins));
-        float2* dst = a.samp + ((int64_t)blk * a.nlev + l) * kSampStride + (int64_t)(h / L.k - 1) * ncs;
+        const int ncap = pair_ncap ? pair_ncap[l] : max(1, kSigmaCap / L.nbins);
+        const int ncs = all ? nv : min(nv, ncap);
+        float2* dst = a.samp + ((int64_t)blk * a.nlev + l) * kSampStride + (int64_t)jh * ncs;
         const float2* src = xo + g * Nst;
         if (all || ncs == 1) {
             for (int c = lane; c < ncs; c += 32) dst[c] = src[all ? c : 0];
+        } else if ((int64_t)ncs * nv < (1 << 24) && nv < (1 << 22)) {
+            // c*nv < 2^24 is exact in FP32, and c*nv/ncs < 2^22 carries an
+            // error below 1 through the rounded reciprocal and the truncating
+            // product, so one correction step either way gives the quotient.
+            const uint32_t un = (uint32_t)ncs;
+            const float inv = __frcp_rn((float)ncs);
+            for (int c = lane; c < ncs; c += 32) {
+                const uint32_t x = (uint32_t)c * (uint32_t)nv;
+                uint32_t q = __float2uint_rz(__fmul_rz((float)x, inv));
+                if (q * un > x) --q;
+                else if ((q + 1u) * un <= x) ++q;
+                dst[c] = src[q];
+            }
         } else {
+            // the division by ncs as a multiply-high by ceil(2^64/ncs), exact
+            // for every 32-bit dividend
             const uint64_t mg = 0xFFFFFFFFFFFFFFFFull / (uint64_t)ncs + 1ull;
             for (int c = lane; c < ncs; c += 32) {
-                const uint32_t x = (uint32_t)c * (uint32_t)nv;   // < 4096 * 65536
+                const uint32_t x = (uint32_t)c * (uint32_t)nv;
                 dst[c] = src[(int)__umul64hi((uint64_t)x, mg)];
             }
         }
@@ -356,6 +385,8 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
     __shared__ unsigned s_pm[kHG];                 // ceil(2^24 / P): (task div P) for task * P < 2^24
     __shared__ uint32_t s_am[kMaxSpecChunks];      // FP16 A tiles: the spectrum chunks' maxima
     __shared__ int s_cidx;                         // and the block's last chunk: its scale 2^-s
+    __shared__ short s_jh[kHG * kMaxLevels];       // per (harmonic, level) pair: emit_rows' pair_jh
+    __shared__ int s_ncap[kMaxLevels];             // per level: emit_rows' pair_ncap
 
     // harmonic groups fastest: the CTAs filling one block's A tiles (each a
     // 128-byte piece of every 2 KB row group) run together
@@ -372,6 +403,20 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
     if (threadIdx.x >= 32 && threadIdx.x < 32 + kMaxSpecChunks)
         s_am[threadIdx.x - 32] = a.amax_bits ? a.amax_bits[threadIdx.x - 32] : 0u;
     if (threadIdx.x == 32 + kMaxSpecChunks) s_cidx = a.blk_cidx ? a.blk_cidx[blk] : kMaxSpecChunks - 1;
+    // the sigma samples' per-pair bookkeeping, once per CTA by warps 2-3 (its
+    // integer divisions off the emission's path)
+    if (threadIdx.x >= 64 && threadIdx.x < 64 + ng * a.nlev) {
+        const int e = (int)threadIdx.x - 64;
+        int g = 0, l = e;
+        while (l >= a.nlev) {
+            l -= a.nlev;
+            ++g;
+        }
+        const int h = hidx0 + g + 1, k = a.levels[l].k;
+        s_jh[e] = (short)((h % k == 0 && h / k <= a.levels[l].Hk) ? h / k - 1 : -1);
+    }
+    if (threadIdx.x >= 160 && threadIdx.x < 160 + a.nlev)
+        s_ncap[threadIdx.x - 160] = max(1, kSigmaCap / a.levels[threadIdx.x - 160].nbins);
     if (threadIdx.x < ng) {
         // Range guard on the TRUE trial range (src/directinterp.jl:490-496),
         // with the Julia 1-based bounds translated to 0-based windows.
@@ -469,7 +514,7 @@ __global__ void __launch_bounds__(256, 3) k_interp(WaveArgs a, int win_max, int 
     }
     __syncthreads();
     const float sc = a.fp16 && a.Atile ? pow2f(-ascale_exp(s_am, s_cidx)) : 1.0f;   // exact power of two
-    emit_rows(a, xo, Nst, blk, hidx0, ng, n, sc);
+    emit_rows(a, xo, Nst, blk, hidx0, ng, n, sc, s_jh, s_ncap);
 }
 
 // ---------------------------------------------------------------------------
@@ -1037,7 +1082,12 @@ __device__ uint32_t radix_select(const uint32_t* vals, int ns, int kth, uint32_t
 // for the scan's warp totals and the pass result, so that nothing written in
 // one pass is overwritten before every thread has read it.  Four barriers per
 // pass.  hist2 holds 2 x 2048 bins; wtot2 2 x 32 ints; sh2 2 x 4 ints.
-__device__ uint32_t radix_select_2buf(const uint32_t* vals, int ns, int kth, uint32_t* hist2, int* sh2, int* wtot2) {
+// With `next`, also the (kth+1)-th smallest value into *next (written by
+// thread 0 before the last barrier) when the last pass's histogram holds it,
+// that is when it shares the kth's top 22 bits; else 0xFFFFFFFF, and the
+// caller finds it itself.
+__device__ uint32_t radix_select_2buf(const uint32_t* vals, int ns, int kth, uint32_t* hist2, int* sh2, int* wtot2,
+                                      uint32_t* next = nullptr) {
     uint32_t prefix = 0, mask = 0;
     int kk = kth;
     const int shifts[3] = {21, 10, 0};
@@ -1052,6 +1102,7 @@ __device__ uint32_t radix_select_2buf(const uint32_t* vals, int ns, int kth, uin
         uint32_t* hnext = hist2 + ((pass + 1) & 1) * 2048;
         int* wtot = wtot2 + (pass & 1) * 32;
         int* sh = sh2 + (pass & 1) * 4;
+        if (next && pass == 2 && threadIdx.x == 0) sh[2] = -1;   // read only after the barriers below
         for (int i = threadIdx.x; i < ns; i += nthr) {
             const uint32_t v = vals[i];
             if ((v & mask) == prefix) atomicAdd(&hist[(v >> shift) & (uint32_t)(nb - 1)], 1u);
@@ -1096,7 +1147,21 @@ __device__ uint32_t radix_select_2buf(const uint32_t* vals, int ns, int kth, uin
                 c += hb;
             }
         }
+        // last pass: the bin of rank kk+1 as well
+        if (next && pass == 2 && excl <= kk + 1 && kk + 1 < excl + local) {
+            int c = excl;
+            for (int b = b0; b < b1; ++b) {
+                const int hb = (int)hist[b];
+                if (c + hb > kk + 1) {
+                    sh[2] = b;
+                    break;
+                }
+                c += hb;
+            }
+        }
         __syncthreads();
+        if (next && pass == 2 && threadIdx.x == 0)
+            *next = sh[2] >= 0 ? (prefix | (uint32_t)sh[2]) : 0xFFFFFFFFu;
         prefix |= (uint32_t)sh[0] << shift;
         mask |= (uint32_t)(nb - 1) << shift;
         kk = sh[1];
@@ -1229,7 +1294,15 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 2) k_sigma(WaveArgs a, int
         med = __uint_as_float(radix_select_2buf(vals, ns, half, hist, sh2, wtot2));
     } else {
         // _median! (src/search.jl:295-305): mean of the two central order statistics.
-        const uint32_t lo = radix_select_2buf(vals, ns, half - 1, hist, sh2, wtot2);
+        __shared__ uint32_t hi_sh;
+        const uint32_t lo = radix_select_2buf(vals, ns, half - 1, hist, sh2, wtot2, &hi_sh);
+        __syncthreads();
+        const uint32_t hi = hi_sh;
+        if (hi != 0xFFFFFFFFu) {
+            med = 0.5f * (__uint_as_float(lo) + __uint_as_float(hi));
+            if (threadIdx.x == 0) a.sigma[bl] = 1.4826f * med;
+            return;
+        }
         int le = 0;
         uint32_t above = 0xFFFFFFFFu;
         for (int i = threadIdx.x; i < ns; i += blockDim.x) {

@@ -128,3 +128,59 @@ def test_features_wait_for_the_chunked_copy():
     eng.set_spectrum_host(pinned.data_ptr(), namps, N, dt)
     got = eng.block_features(BAND[0], BAND[1], 100, 2048)
     assert np.array_equal(got.cpu().numpy(), want.cpu().numpy())
+
+
+def _pair(seed, nsamp=1 << 22, dt=64e-6):
+    """A spectrum with one pulsar, on the device and in pinned host memory."""
+    import torch
+    amps = synth.make_spectrum(nsamp, dt, [synth.Pulsar(11.0 + seed, 0.05, 25.0, 0.3)], seed)
+    d = torch.from_numpy(amps.view(np.float32).copy()).cuda()
+    h = torch.from_numpy(amps.view(np.float32).copy()).pin_memory()
+    return amps, d, h, nsamp, dt
+
+
+def test_overlapped_copy_with_waves_block_lists_and_a_new_stream():
+    """The first search after a chunked copy splits only its first wave's
+    interpolation; later waves, block-list searches, a second spectrum copied
+    before any search, and a search on another stream all see the whole copy."""
+    import torch
+    amps, d, h, N, dt = _pair(1)
+    band = (1.0, 60.0)
+    dev = cs.Engine(_params("fp16"))
+    dev.set_spectrum_device(d.data_ptr(), len(amps), N, dt, keep=d)
+    want = dev.search_raw(band[0], band[1], 100, 2048, THR)
+    nblk = dev.stats()["blocks"]
+    blist = np.arange(3, nblk, 7)
+    want_blocks = dev.search_blocks_raw(blist, band[0], band[1], 100, 2048, THR)
+    assert len(want) > 0 and len(want_blocks) > 0
+
+    # several waves under a memory cap: the spectrum (16 MiB) and a few blocks
+    eng = cs.Engine(_params("fp16"))
+    eng.set_memory_limit(len(amps) * 8 + (24 << 20))
+    eng.set_spectrum_host(h.data_ptr(), len(amps), N, dt)
+    got = eng.search_raw(band[0], band[1], 100, 2048, THR)
+    assert eng.stats()["waves"] > 1
+    assert np.array_equal(got, want)
+
+    # a block list as the first search after the copy
+    eng = cs.Engine(_params("fp16"))
+    eng.set_spectrum_host(h.data_ptr(), len(amps), N, dt)
+    assert np.array_equal(eng.search_blocks_raw(blist, band[0], band[1], 100, 2048, THR), want_blocks)
+
+    # two copies before any search: the second spectrum is the one searched
+    amps2, d2, h2, _, _ = _pair(2)
+    dev.set_spectrum_device(d2.data_ptr(), len(amps2), N, dt, keep=d2)
+    want2 = dev.search_raw(band[0], band[1], 100, 2048, THR)
+    assert not np.array_equal(want2, want)
+    eng = cs.Engine(_params("fp16"))
+    eng.set_spectrum_host(h.data_ptr(), len(amps), N, dt)
+    eng.set_spectrum_host(h2.data_ptr(), len(amps2), N, dt)
+    assert np.array_equal(eng.search_raw(band[0], band[1], 100, 2048, THR), want2)
+
+    # the copy issued while the handle used its own stream, the search on another
+    side = torch.cuda.Stream()
+    eng = cs.Engine(_params("fp16"))
+    eng.set_spectrum_host(h.data_ptr(), len(amps), N, dt)
+    eng.set_stream(side.cuda_stream)
+    assert np.array_equal(eng.search_raw(band[0], band[1], 100, 2048, THR), want)
+    side.synchronize()

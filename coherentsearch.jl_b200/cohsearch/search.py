@@ -373,7 +373,7 @@ class Engine:
         return {"interp_kernel": "persistent" if r.interp_kernel else "per-item",
                 "sigma_kernel": "256 threads, twiddles via L1" if r.sigma_kernel else "384 threads, twiddles in smem",
                 "ms_sigma": list(r.ms_sigma),
-                "tc_double_buffer": bool(r.tc_double_buffer), "tc_div": list(r.tc_div),
+                "tc_double_buffer": int(r.tc_double_buffer), "tc_div": list(r.tc_div),
                 "units_per_level": {int(r.nbins[i]): int(r.units[i]) for i in range(n)},
                 "ms_interp": {"per-item": r.ms_interp[0], "persistent": r.ms_interp[1]},
                 "ms_synth_model": r.ms_synth_model, "ms_synth_tuned": r.ms_synth_tuned,

@@ -2016,11 +2016,13 @@ cs_status cs_autotune(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
         rep.ms_sigma[v] = H->stats_sigma_min;
     }
     if (st == CS_OK) H->tune_sigma = rep.ms_sigma[1] < rep.ms_sigma[0] ? 1 : 0;
-    // 3. tensor epilogue: segment divisor of each phase, then one or two base-level slots
+    // 3. tensor epilogue: the form (one slot, phased double buffer, split) and
+    // each phase's segment divisor
     if (st == CS_OK && tensor) {
         int best[3] = {0, 0, 1};   // div0, div1, dbuf
         double best_ms = ms_model;
-        auto trial = [&](int d0, int d1, int db) -> cs_status {
+        auto trial = [&](int d0, int d1, int db, double* ms) -> cs_status {
+            if (ms) *ms = 1e300;
             H->tune_div[0] = d0;
             H->tune_div[1] = d1;
             H->tune_dbuf = db;
@@ -2028,6 +2030,7 @@ cs_status cs_autotune(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
             double a = 0.0, b = 0.0;
             const cs_status e = timed(&a, &b);
             if (e != CS_OK) return e;
+            if (ms) *ms = b;
             if (b < best_ms) {
                 best_ms = b;
                 best[0] = d0;
@@ -2036,13 +2039,28 @@ cs_status cs_autotune(cs_handle* H, double lofreq, double hifreq, int64_t lobin,
             }
             return CS_OK;
         };
+        // Per epilogue form (one slot; base level double-buffered and scanned
+        // after the decimated levels; split between warpgroup pairs): the
+        // divisor of phase 0 first, then, with the base level in a phase of
+        // its own, the divisor of phase 1 (each form weighs its segments
+        // differently, so none borrows another's).
         const int divs[] = {2, 3, 4, 5, 6, 8, 10, 12, 16};
-        if (H->dlev.size() > 1)
-            for (int d : divs)
-                if (st == CS_OK) st = trial(d, best[1], best[2]);
-        for (int d : divs)
-            if (st == CS_OK) st = trial(best[0], d, best[2]);
-        if (st == CS_OK) st = trial(best[0], best[1], 0);
+        for (int db = 0; db < 3 && st == CS_OK; ++db) {
+            int bd0 = 2;
+            double bms = 1e300;
+            if (db == 0 || H->dlev.size() > 1)
+                for (int d : divs) {
+                    double ms = 0.0;
+                    if (st == CS_OK) st = trial(d, 2, db, &ms);
+                    if (ms < bms) {
+                        bms = ms;
+                        bd0 = d;
+                    }
+                }
+            if (db > 0)
+                for (int d : divs)
+                    if (st == CS_OK) st = trial(bd0, d, db, nullptr);
+        }
         H->tune_div[0] = best[0];
         H->tune_div[1] = best[1];
         H->tune_dbuf = best[2];
@@ -2077,7 +2095,7 @@ cs_status cs_set_launch_shapes(cs_handle* H, const cs_tune_report* sh) {
     auto div_ok = [](int d) { return d == 0 || d == 2 || d == 3 || d == 4 || d == 5 || d == 6 || d == 8 || d == 10 ||
                                      d == 12 || d == 16; };
     if ((sh->interp_kernel != 0 && sh->interp_kernel != 1) || (sh->sigma_kernel != 0 && sh->sigma_kernel != 1) ||
-        (sh->tc_double_buffer != 0 && sh->tc_double_buffer != 1) || !div_ok(sh->tc_div[0]) || !div_ok(sh->tc_div[1]))
+        sh->tc_double_buffer < 0 || sh->tc_double_buffer > 2 || !div_ok(sh->tc_div[0]) || !div_ok(sh->tc_div[1]))
         return fail(H, CS_ERR_INVALID_ARGUMENT, "launch shapes out of range");
     CS_CUDA(cudaSetDevice(H->device), "set device");
     H->tune_interp = sh->interp_kernel;

@@ -165,16 +165,20 @@ struct TcUnit {
     int16_t col;
     int16_t col1;
     int16_t phase;     // 0: scanned first (decimated levels); 1: after the next tile's product is issued
+                       // (split epilogue: 1 = warpgroups 0-1's levels, 0 = warpgroups 2-3's)
     int16_t pad;
 };
 
 // One tcgen05.mma column range: B columns [bcol, bcol + n) into TMEM columns
-// from tcol (even tiles) or tcol1 (odd tiles).
+// from tcol (even tiles) or tcol1 (odd tiles).  phase: the split epilogue's
+// group that issues it (1: warpgroups 0-1, 0: warpgroups 2-3).
 struct TcMma {
     int16_t bcol;
     int16_t n;
     int16_t tcol;
     int16_t tcol1;
+    int16_t phase;
+    int16_t pad;
 };
 
 constexpr int kMaxUnits = 32;
@@ -190,7 +194,9 @@ struct TcArgs {
     int32_t hm;            // prefix-sum ring size: 8 or 32 (>= widest boxcar)
     int32_t ncols_total;   // B columns of the product (multiple of 16)
     int32_t dbuf;          // 1: the base level has two TMEM slots, so the next tile's product
-                           // runs while this tile's base level is scanned
+                           // runs while this tile's base level is scanned; 2: besides, the
+                           // levels are split between two pairs of warpgroups that scan side
+                           // by side, each pair issuing the products of its own levels
     int32_t fp16;          // operand format: 1 = FP16, 0 = BF16
     int32_t split;         // A tiles per 128 trials: 1, or 2 (hi and lo: K runs over both)
 };

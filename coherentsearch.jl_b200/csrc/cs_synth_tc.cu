@@ -284,6 +284,37 @@ __device__ __forceinline__ float gate_dispatch(uint32_t tcol, int nbins, int pw,
 
 constexpr int kEpiThreads = 512;   // 4 warpgroups share the epilogue
 
+// Named barriers of 256 threads (two warpgroups), for the split epilogue
+// (t.dbuf == 2): id 1 for warpgroups 0-1, id 2 for warpgroups 2-3 (id 0 is
+// __syncthreads).  The reductions return the same value to every thread.
+__device__ __forceinline__ void group_sync(int id) {
+    asm volatile("barrier.cta.sync %0, 256;" ::"r"(id) : "memory");
+}
+__device__ __forceinline__ bool group_and(bool v, int id) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "barrier.cta.red.and.pred p, %2, 256, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id)
+        : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ bool group_or(bool v, int id) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "barrier.cta.red.or.pred p, %2, 256, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id)
+        : "memory");
+    return r != 0;
+}
+
 // One persistent CTA per SM walks the tiles blockIdx.x, +gridDim.x, ...
 // Thread 0 issues each tile's product (one commit per tile) as soon as its A
 // tile has landed and the TMEM columns it writes are free: with two base-level
@@ -313,6 +344,16 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     __shared__ float cut_sh[kMaxLevels];        // gate bound for skipping a warp's scan, per level
     __shared__ float gup_sh;                    // 2^s: undoes the tile's block's FP16 scale
     __shared__ float gup_chunk_sh[kMaxSpecChunks];   // 2^s of a block whose last spectrum chunk is c
+    // split epilogue (t.dbuf == 2): base-level products per slot, A buffers
+    // released by both groups, and the counts the final drain waits for
+    __shared__ uint64_t mbar_b2[2];             // base-level product of the slot's tiles
+    __shared__ int afree_sh[2];                 // arrivals of the two groups at an A buffer
+    __shared__ int nload_sh[2];                 // A loads issued into each buffer
+    __shared__ int ncommit_sh[3];               // products committed: decimated, base slot 0, base slot 1
+    __shared__ uint8_t grp_lev[2][kMaxLevels];  // each group's levels (group 0: warpgroups 0-1)
+    __shared__ int grp_nlev[2];
+    __shared__ int grp_ok_sh[2];                // 0 once a group's product could not be issued
+    __shared__ float gup2_sh[2];                // each group's tile scale 2^s
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
@@ -343,6 +384,21 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
         mbar_init(&mbar, 1);
         mbar_init(&lbar[0], 1);
         mbar_init(&lbar[1], 1);
+        mbar_init(&mbar_b2[0], 1);
+        mbar_init(&mbar_b2[1], 1);
+        afree_sh[0] = afree_sh[1] = 0;
+        nload_sh[0] = nload_sh[1] = 0;
+        ncommit_sh[0] = ncommit_sh[1] = ncommit_sh[2] = 0;
+        // the split epilogue's level lists: a level belongs to the group of its units
+        grp_nlev[0] = grp_nlev[1] = 0;
+        for (int l = 0; l < t.nlev; ++l) {
+            int g = 1;
+            for (int u = 0; u < t.nunit; ++u)
+                if (t.unit[u].lev == l && t.unit[u].phase == 1) g = 0;
+            if (l == 0) g = 0;
+            grp_lev[g][grp_nlev[g]++] = (uint8_t)l;
+        }
+        grp_ok_sh[0] = grp_ok_sh[1] = 1;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -403,19 +459,29 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     };
 
     bool ok = true;
-    if (tid == 0 && my_ntiles > 0) {
+    if (t.dbuf != 2 && tid == 0 && my_ntiles > 0) {
         load_a(0);
         if (nbuf == 2 && my_ntiles > 1) load_a(1);
         if (!issue_mma(0)) mma_ok_sh = 0;
     }
     // The per-level sigma and valid counts of the first tile's block; each
     // iteration then loads the next tile's while its own epilogue runs.
+    // (the split epilogue: thread 0 keeps the base level's, threads 256+l the
+    // decimated level l's)
+    int plev = tid < t.nlev ? tid : -1;
+    if (t.dbuf == 2) {
+        // the split epilogue: warpgroups 0-1's levels to threads l, 2-3's to 256+l
+        plev = -1;
+        const int g = tid < 256 ? 0 : 1;
+        for (int i = 0; i < grp_nlev[g]; ++i)
+            if (grp_lev[g][i] == (tid & 255)) plev = tid & 255;
+    }
     float sig_next = 0.0f;
     int nv_next = 0, cidx_next = kMaxSpecChunks - 1;   // the block's last spectrum chunk: its FP16 scale
-    if (tid < t.nlev && my_ntiles > 0) {
+    if (plev >= 0 && my_ntiles > 0) {
         const int b0 = (int)blockIdx.x / tiles_per_blk;
-        sig_next = a.sigma[b0 * a.nlev + tid];
-        nv_next = a.nvalid[b0 * a.nlev + tid];
+        sig_next = a.sigma[b0 * a.nlev + plev];
+        nv_next = a.nvalid[b0 * a.nlev + plev];
         if (a.blk_cidx) cidx_next = a.blk_cidx[b0];
     }
     ok = __syncthreads_and(mma_ok_sh != 0) != 0;
@@ -425,6 +491,146 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
     const int row = (warp & 3) * 32 + (tid & 31);
     const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
 
+    if (t.dbuf == 2) {
+        // Split epilogue.  Warpgroups 0-1 (group A, named barrier 1) scan the
+        // base level from the slot of the tile's parity; warpgroups 2-3
+        // (group B, barrier 2) scan the decimated levels.  Each group's first
+        // thread issues its own products: A the base level of tile it+2 into
+        // the slot it just read, B the decimated levels of tile it+1, so
+        // neither group waits for the other's scan.  Tile it's A buffer is
+        // refilled with tile it+2 by whichever group is done with it second.
+        const bool grpA = tid < 256;
+        const int gid = grpA ? 0 : 1;
+        const int bar_id = grpA ? 1 : 2;
+        const int gtid = tid & 255;
+        auto load2 = [&](int it) {
+            const int b = it & 1;
+            bulk_load(smem_u32(As0 + b * abytes),
+                      a.Atile + (int64_t)((int)blockIdx.x + it * (int)gridDim.x) * abytes, abytes, &lbar[b]);
+            atomicAdd(&nload_sh[b], 1);
+        };
+        // This group's products of tile it (its A tile waited for, bounded):
+        // warpgroups 0-1 the base level's ranges (phase 1) into the slot of
+        // the tile's parity, 2-3 the decimated levels' (phase 0).
+        auto issue2 = [&](int it) -> bool {
+            const int b = it & 1;
+            if (!mbar_wait(&lbar[b], (uint32_t)((it >> 1) & 1))) return false;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a_addr = smem_u32(As0 + b * abytes);
+            for (int q = 0; q < t.nmma; ++q) {
+                const TcMma M = mma_sh[q];
+                if ((M.phase == 1) != grpA) continue;
+                const uint32_t idesc = idesc_base | ((uint32_t)(M.n >> 3) << 17);
+                const uint32_t dcol = (uint32_t)((it & 1) ? M.tcol1 : M.tcol);
+                for (int ks = 0; ks < kK / 16; ++ks) {
+                    const uint64_t da = umma_desc(a_addr + ks * 2 * kALBO, kALBO, kASBO);
+                    const uint64_t db = umma_desc(b_addr + (M.bcol / 8) * kSBO + ks * 256);
+                    const uint32_t acc = ks > 0;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                        ::"r"(tmem + dcol), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+                }
+            }
+            uint64_t* done = grpA ? &mbar_b2[it & 1] : &mbar;
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(smem_u32(done)) : "memory");
+            atomicAdd(&ncommit_sh[grpA ? 1 + (it & 1) : 0], 1);
+            return true;
+        };
+        if (gtid == 0 && my_ntiles > 0 && ok) {
+            bool good = true;
+            if (grpA) {
+                load2(0);
+                if (my_ntiles > 1) load2(1);
+                good = issue2(0) && (my_ntiles < 2 || issue2(1));
+            } else {
+                good = issue2(0);
+            }
+            if (!good) grp_ok_sh[gid] = 0;
+        }
+        ok = group_and(ok, bar_id);
+        for (int it = 0; it < my_ntiles && ok; ++it) {
+            const int tile = (int)blockIdx.x + it * (int)gridDim.x;
+            const int blk = tile / tiles_per_blk;
+            const int j0 = (tile % tiles_per_blk) * kTM;
+            if (plev >= 0) {
+                // this group's level(s): 1/sigma times the tile scale, valid count, skip bound
+                const float gup = gup_chunk_sh[cidx_next];
+                gup2_sh[gid] = gup;   // (every owner of the group writes the same value)
+                const float inv = inv_sigma(sig_next) * gup;
+                inv_sh[plev] = inv;
+                nv_sh[plev] = nv_next;
+                float cut = -INFINITY;
+                const float c = fminf(a.medcut_gate, a.threshold);
+                if (!a.Q0 && inv > 0.0f && c > 0.0f) cut = (c / inv) * (1.0f - 0x1p-16f);
+                cut_sh[plev] = cut;
+                if (it + 1 < my_ntiles) {
+                    const int bn = (tile + (int)gridDim.x) / tiles_per_blk;
+                    sig_next = a.sigma[bn * a.nlev + plev];
+                    nv_next = a.nvalid[bn * a.nlev + plev];
+                    if (a.blk_cidx) cidx_next = a.blk_cidx[bn];
+                }
+            }
+            // this tile's product for the group has landed (bounded)
+            const bool landed = grpA ? mbar_wait(&mbar_b2[it & 1], (uint32_t)((it >> 1) & 1))
+                                     : mbar_wait(&mbar, (uint32_t)(it & 1));
+            ok = group_and(landed && grp_ok_sh[gid] != 0, bar_id);
+            if (!ok) {
+                if (gtid == 0) atomicExch(err, 2);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            // both groups' products of tile it are done with its A buffer
+            if (gtid == 0 && it + 2 < my_ntiles) {
+                __threadfence_block();
+                if (atomicAdd(&afree_sh[it & 1], 1) & 1) {
+                    __threadfence_block();
+                    load2(it + 2);
+                }
+            }
+            const int par = it & 1;
+            bool need = false;
+            for (int u = 0; u < t.nunit; ++u) {
+                const TcUnit& U = unit_sh[u];
+                if (U.phase != (grpA ? 1 : 0) || U.wg != wg) continue;           // warp-uniform
+                if (j0 >= nv_sh[U.lev]) continue;                                // warp-uniform
+                const TcLevel& L = lev_sh[U.lev];
+                const float cut = cut_sh[U.lev];
+                const uint32_t col = (uint32_t)(par ? U.col1 : U.col);
+                const float v = gate_dispatch<HM>(lane_base + col, U.nstart, U.pw, L.wmask, L.rsq, cut,
+                                                  j0 + row < nv_sh[U.lev]);
+                part_sh[u][row] = v;
+                need |= !(cut > 0.0f) || v != -INFINITY;
+            }
+            // the group's columns are read: its next product may land in them
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            need = group_or(need, bar_id);
+            if (gtid == 0) {
+                // the base level two tiles on into the slot just read; the
+                // decimated levels of the next tile into their one slot
+                const int nxt = grpA ? it + 2 : it + 1;
+                if (nxt < my_ntiles && !issue2(nxt)) grp_ok_sh[gid] = 0;
+            }
+            if (need) {
+                // gate = max over the level's units, then the medcut test
+                const int nl = grp_nlev[gid];
+                for (int idx = gtid; idx < nl * kTM; idx += 256) {
+                    const int l = grp_lev[gid][idx / kTM], r = idx % kTM;
+                    const int j = j0 + r;
+                    if (j >= nv_sh[l]) continue;
+                    float g = -INFINITY;
+                    for (int i = lu_start[l]; i < lu_start[l + 1]; ++i) g = fmaxf(g, part_sh[lu_idx[i]][r]);
+                    if (a.Q0) a.Q0[((int64_t)blk * a.nlev + l) * a.Nprof + j] = g * gup2_sh[gid];
+                    gate_flag(a, blk, l, j, g, inv_sh[l]);
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            ok = group_and(grp_ok_sh[gid] != 0, bar_id);
+            if (!ok && gtid == 0) atomicExch(err, 2);
+        }
+    } else
     for (int it = 0; it < my_ntiles && ok; ++it) {
         const int tile = (int)blockIdx.x + it * (int)gridDim.x;
         const int blk = tile / tiles_per_blk;
@@ -507,12 +713,21 @@ __global__ void __launch_bounds__(kEpiThreads, 1) k_synth_tc(WaveArgs a, TcArgs 
         ok = __syncthreads_and(mma_ok_sh != 0) != 0;
         if (!ok && tid == 0) atomicExch(err, 2);
     }
+    if (t.dbuf == 2) __syncthreads();   // both groups are out of their loops: the counts are final
     if (tid == 0) {
         // bounded: let every product and A-tile copy this CTA issued land
         // before its TMEM and shared memory go away (all have on the normal path)
-        if (nmma_issued > 0) mbar_wait(&mbar, (uint32_t)((nmma_issued - 1) & 1));
-        for (int b = 0; b < 2; ++b)
-            if (nload[b] > 0) mbar_wait(&lbar[b], (uint32_t)((nload[b] - 1) & 1));
+        if (t.dbuf == 2) {
+            if (ncommit_sh[0] > 0) mbar_wait(&mbar, (uint32_t)((ncommit_sh[0] - 1) & 1));
+            for (int sl = 0; sl < 2; ++sl)
+                if (ncommit_sh[1 + sl] > 0) mbar_wait(&mbar_b2[sl], (uint32_t)((ncommit_sh[1 + sl] - 1) & 1));
+            for (int b = 0; b < 2; ++b)
+                if (nload_sh[b] > 0) mbar_wait(&lbar[b], (uint32_t)((nload_sh[b] - 1) & 1));
+        } else {
+            if (nmma_issued > 0) mbar_wait(&mbar, (uint32_t)((nmma_issued - 1) & 1));
+            for (int b = 0; b < 2; ++b)
+                if (nload[b] > 0) mbar_wait(&lbar[b], (uint32_t)((nload[b] - 1) & 1));
+        }
     }
     __syncthreads();
     if (warp == 0) {
@@ -570,12 +785,16 @@ int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, Tc
     const int g1 = pad16(rcol);          // decimated levels
     if (g1 + pad16(t.lev[0].pw) > 512) return -3;
     int try_dbuf = 1;
+    int mode = 0;
     auto phase_of = [&](int l) { return (try_dbuf && l == 0) ? 1 : 0; };
     struct UC { int lev, p0, nst; double c; };
     auto seg_cost = [&](int l, int nst) { return (double)(nst + dl[l].wmax) * (1 + 2 * dl[l].nw); };
     // The units of one phase for a segment target of (phase cost / div), and
     // their longest-processing-time placement on the 4 warpgroups.
+    // (mode 2: the base level's units on warpgroups 0-1, the decimated levels'
+    // on 2-3, the two groups scanning side by side)
     auto build_phase = [&](int ph, int div, UC* uc, int* wg_of, double* maxload) -> int {
+        const int wg0 = mode == 2 ? (ph == 1 ? 0 : 2) : 0, nwg = mode == 2 ? 2 : 4;
         double ph_cost = 0.0;
         for (int l = 0; l < nlev; ++l)
             if (phase_of(l) == ph) ph_cost += seg_cost(l, dl[l].nbins);
@@ -601,8 +820,8 @@ int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, Tc
             for (int i = 0; i < nu; ++i)
                 if (!used[i] && (best < 0 || uc[i].c > uc[best].c)) best = i;
             used[best] = true;
-            int g = 0;
-            for (int q = 1; q < 4; ++q) if (load[q] < load[g]) g = q;
+            int g = wg0;
+            for (int q = wg0 + 1; q < wg0 + nwg; ++q) if (load[q] < load[g]) g = q;
             load[g] += uc[best].c;
             wg_of[best] = g;
         }
@@ -622,7 +841,8 @@ int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, Tc
     int all_wg[kMaxUnits], all_ph[kMaxUnits];
     int nall = 0;
     int slot_w = t.lev[0].pw;
-    for (try_dbuf = allow_dbuf ? 1 : 0; try_dbuf >= 0; --try_dbuf) {
+    for (mode = allow_dbuf >= 2 && split == 1 && nlev >= 2 ? 2 : (allow_dbuf ? 1 : 0); mode >= 0; --mode) {
+        try_dbuf = mode > 0 ? 1 : 0;
         nall = 0;
         bool okp = true;
         for (int ph = 0; ph < 2 && okp; ++ph) {
@@ -662,8 +882,8 @@ int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, Tc
         slot_w = pad16(slot_w);
         if (!try_dbuf || pad32(g1) + pad32(slot_w) + slot_w <= 512) break;
     }
-    if (try_dbuf < 0) return -4;
-    t.dbuf = try_dbuf;
+    if (mode < 0) return -4;
+    t.dbuf = mode;
     // B columns: the base level's slot width (its bins, its wrapped tail and
     // zero columns up to the reach of its scans, so that every column a scan
     // reads is written by the product), then the decimated levels.
@@ -679,12 +899,13 @@ int prepare_tc(const DevLevel* dl, int nlev, int nharms, int fp16, int split, Tc
     t.nmma = 0;
     for (int c = 0; c < g0; c += 256) {
         const int n = g0 - c < 256 ? g0 - c : 256;
-        t.mma[t.nmma++] = {(int16_t)c, (int16_t)n, (int16_t)(slot0 + c), (int16_t)(slot1 + c)};
+        t.mma[t.nmma++] = {(int16_t)c, (int16_t)n, (int16_t)(slot0 + c), (int16_t)(slot1 + c), 1, 0};
     }
+    // the decimated levels (issued by warpgroups 2-3 in the split epilogue)
     for (int c = 0; c < g1; c += 256) {
         const int n = g1 - c < 256 ? g1 - c : 256;
         if (t.nmma >= kMaxMma) return -4;
-        t.mma[t.nmma++] = {(int16_t)(g0 + c), (int16_t)n, (int16_t)c, (int16_t)c};
+        t.mma[t.nmma++] = {(int16_t)(g0 + c), (int16_t)n, (int16_t)c, (int16_t)c, 0, 0};
     }
     t.nunit = nall;
     for (int l = 0; l < nlev; ++l) t.lev[l].nunits = 0;

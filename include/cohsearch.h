@@ -405,7 +405,10 @@ cs_status cs_search_trial_metrics(const cs_handle* h, float* out, int64_t cap, i
 typedef struct cs_tune_report {
     int32_t interp_kernel;        /* 1: persistent kernel with bulk-copied windows; 0: one CTA per item */
     int32_t sigma_kernel;         /* block sigma: 0 = 384 threads, twiddles in shared memory; 1 = 256, via L1 */
-    int32_t tc_double_buffer;     /* tensor modes: 1 = base level in two TMEM slots */
+    int32_t tc_double_buffer;     /* tensor modes: 0 = one TMEM slot; 1 = base level in two slots,
+                                     scanned after the decimated levels; 2 = base level in two
+                                     slots, scanned by warpgroups 0-1 beside warpgroups 2-3 on the
+                                     decimated levels, each pair issuing its own products */
     int32_t tc_div[2];            /* epilogue segment divisor of each phase (0: FP32 synthesis) */
     int32_t nlev;                 /* decimation levels */
     int32_t nbins[CS_MAX_DECIM];  /* profile bins of each level, in level order */
@@ -420,8 +423,10 @@ typedef struct cs_tune_report {
 /* Autotune the handle's launch shapes on its attached spectrum: a sample of
  * nsample blocks from the middle of the band [lofreq, hifreq] (arguments as
  * cs_search) is searched with each candidate -- the interpolation kernel, the
- * block-sigma kernel, and in the tensor modes the epilogue segment size of each phase per profile bin
- * count and the base level's TMEM double buffer -- timed with CUDA events
+ * block-sigma kernel, and in the tensor modes the epilogue form (one TMEM
+ * slot, the base level double-buffered and scanned after the decimated
+ * levels, or split between two warpgroup pairs) with, per form, the segment
+ * size of each phase per profile bin count -- timed with CUDA events
  * (the least of 3 runs after a warm-up), and the fastest kept on the handle.
  * Every candidate computes the same values, so candidates are unchanged.  The
  * choice is also cached for the device and these parameters: handles created
@@ -432,7 +437,9 @@ cs_status cs_autotune(cs_handle* h, double lofreq, double hifreq, int64_t lobin,
 
 /* Apply launch shapes chosen earlier (a cs_autotune report, e.g. stored by a
  * pipeline at its first run): interp_kernel, sigma_kernel, tc_double_buffer
- * and tc_div are read; the other fields are ignored.  tc_div entries are 0
+ * and tc_div are read; the other fields are ignored.  tc_double_buffer is 0,
+ * 1 or 2 (2 needs unsplit tiles and decimation levels; otherwise the plan
+ * falls back to 1, then 0).  tc_div entries are 0
  * (the cost model's choice) or one of 2, 3, 4, 5, 6, 8, 10, 12, 16.  Every
  * shape computes the same values.  No counterpart in the reference. */
 cs_status cs_set_launch_shapes(cs_handle* h, const cs_tune_report* shapes);

@@ -1,7 +1,8 @@
 """The launch-shape autotuner (cs_autotune): it times the interpolation
 kernels and, in the tensor modes, the epilogue's segment size per profile bin
-count and the base level's TMEM double buffer on a sample of the band, keeps
-the fastest, and every shape it may choose computes the same values.
+count, the base level's TMEM double buffer and the split epilogue on a sample
+of the band, keeps the fastest, and every shape it may choose computes the
+same values.
 
 Checked: the tuned search returns exactly the untuned search's records and
 agrees with the C port of the reference search (tolerances of
@@ -64,7 +65,8 @@ def test_every_launch_shape_gives_the_same_records(synth):
     want = ref.search_raw(band[0], band[1], 100, 2048, 8.0)
     wsig, wnv = ref.block_values()
     assert len(want) > 0
-    shapes = [(1, 0, 1, (0, 0)), (0, 1, 1, (4, 4)), (1, 1, 0, (2, 0)), (0, 0, 1, (16, 3)), (1, 1, 1, (8, 12))]
+    shapes = [(1, 0, 1, (0, 0)), (0, 1, 1, (4, 4)), (1, 1, 0, (2, 0)), (0, 0, 1, (16, 3)), (1, 1, 1, (8, 12)),
+              (0, 0, 2, (2, 2)), (1, 1, 2, (3, 4)), (0, 0, 2, (0, 0))]
     for sh in shapes:
         eng, _, _, _ = _engine(synth)
         eng.set_launch_shapes(*sh)
@@ -75,3 +77,23 @@ def test_every_launch_shape_gives_the_same_records(synth):
     import cohsearch as cs
     with pytest.raises(ValueError):
         ref.set_launch_shapes(0, 0, 1, (7, 0))
+
+
+@pytest.mark.parametrize("synth", ["fp16", "bf16"])
+def test_split_epilogue_gates_equal_the_phased_form(synth):
+    """The split epilogue (warpgroups 0-1 on the base level's two TMEM slots,
+    2-3 on the decimated levels, each pair issuing its own products) and the
+    phased one (all warpgroups on the decimated levels, then the base level)
+    read the same accumulators through the same segments: every gate value
+    and record bit for bit."""
+    band = (0.2, 120.0)
+    out = []
+    for db in (1, 2):
+        eng, _, _, _ = _engine(synth)
+        eng.set_diagnostics(2)
+        eng.set_launch_shapes(0, 0, db, (2, 2))
+        got = eng.search_raw(band[0], band[1], 100, 2048, 8.0)
+        out.append((got, eng.gate_values().copy()))
+    assert len(out[0][0]) > 0
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1].view(np.uint32), out[1][1].view(np.uint32))

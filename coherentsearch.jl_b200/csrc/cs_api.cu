@@ -261,6 +261,16 @@ struct cs_handle {
     DBuf d_tcB;
     DBuf d_A, d_samp;
     HBuf h_nvalid, h_io;                // pinned: valid counts up; counters + candidate prefix down
+    // What h_nvalid holds after a single-wave search of a band: a repeat of
+    // the same band on a spectrum of the same size reuses it as it stands.
+    struct NvKey {
+        double r_lo, lodr, nyq;
+        int64_t t_base, t_end, nblocks, namps;
+        int32_t Nprof, nlev, nharms, m;
+        int64_t profiles;   // its valid-count total (the stats' profile count)
+    };
+    NvKey nv_key{};
+    bool nv_key_ok = false;
     HBuf h_bmap;                        // pinned: a wave's block map (block-list search)
     DBuf d_levels, d_tw, d_nvalid, d_X, d_Q0, d_sigma,
         d_tmetric, d_items, d_counts, d_cands, d_amax, d_bmap;
@@ -610,8 +620,25 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
     // Working set of one wave: up to 16 GiB, and at most half of the free
     // device memory (a full survey band of a 2^24-sample spectrum, ~9 GB, is
     // one wave on a 180 GB part).
+    // When the wave buffers the handle holds already cover every block of this
+    // run (a repeated search), it is one wave with no query of the free memory
+    // (a driver call that costs more host time than the rest of the set-up).
+    const int64_t NB = R.nblocks;
+    auto holds = [](const DBuf& d, size_t n) { return d.bytes >= n; };
+    const bool held_all =
+        !H->mem_limit && !R.stats && (!want_x || holds(H->d_X, (size_t)NB * p.nharms * Nprof * sizeof(float2))) &&
+        (!(tensor && !R.interp_only) ||
+         holds(H->d_A, (size_t)NB * tiles_per_blk * kATileBytes * synth_split(p.synth))) &&
+        (R.interp_only ||
+         (holds(H->d_samp, (size_t)NB * nlev * kSampStride * sizeof(float2)) &&
+          (!(H->diag >= 2 && !R.exact_all) || holds(H->d_Q0, (size_t)NB * nlev * Nprof * sizeof(float))) &&
+          holds(H->d_sigma, (size_t)NB * nlev * sizeof(float)) &&
+          holds(H->d_nvalid, (size_t)NB * (nlev + 1) * sizeof(int32_t)) &&
+          holds(H->d_items, (size_t)NB * nlev * Nprof * sizeof(DevItem)) &&
+          holds(H->d_cands, (size_t)NB * nlev * Nprof * sizeof(DevCand)) &&
+          (!R.exact_all || holds(H->d_tmetric, (size_t)NB * nlev * Nprof * sizeof(float)))));
     size_t budget = (size_t)16 << 30;
-    {
+    if (!held_all) {
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
             // memory this handle already holds for waves counts as free
@@ -639,7 +666,8 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
                             std::to_string(per_blk) + " B more");
         budget = std::min(budget, room);
     }
-    const int64_t WB = std::max<int64_t>(1, std::min<int64_t>(R.nblocks, (int64_t)(budget / per_blk)));
+    const int64_t WB =
+        held_all ? NB : std::max<int64_t>(1, std::min<int64_t>(R.nblocks, (int64_t)(budget / per_blk)));
     if (R.capture) {
         // a captured search runs as one wave on buffers an earlier run sized,
         // without statistics, diagnostics or host round trips
@@ -850,10 +878,25 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
         }
         int* d_err = H->d_counts.as<int32_t>() + 2;
 
-        if (!R.capture) CS_CUDA(H->h_nvalid.ensure((size_t)nb * (nlev + 1) * sizeof(int32_t)), "pinned valid counts");
+        if (!R.capture) {
+            const size_t had = H->h_nvalid.bytes;
+            CS_CUDA(H->h_nvalid.ensure((size_t)nb * (nlev + 1) * sizeof(int32_t)), "pinned valid counts");
+            if (H->h_nvalid.bytes != had) H->nv_key_ok = false;
+        }
         int32_t* nvalid = R.capture ? R.cap_nvalid : H->h_nvalid.as<int32_t>();
         int32_t* cidx = nvalid + (size_t)nb * nlev;   // each block's last spectrum chunk
-        for (int b = 0; b < nb; ++b) {
+        const bool cacheable = !R.capture && !R.blist && !mwin && c0 == 0 && nb == R.nblocks;
+        const cs_handle::NvKey key{R.r_lo, R.lodr, nyq, R.t_base, R.t_end, R.nblocks, H->namps,
+                                   Nprof, nlev, p.nharms, p.m, 0};
+        const cs_handle::NvKey& kk = H->nv_key;
+        const bool reuse = cacheable && H->nv_key_ok && kk.r_lo == key.r_lo && kk.lodr == key.lodr &&
+                           kk.nyq == key.nyq && kk.t_base == key.t_base && kk.t_end == key.t_end &&
+                           kk.nblocks == key.nblocks && kk.namps == key.namps && kk.Nprof == key.Nprof &&
+                           kk.nlev == key.nlev && kk.nharms == key.nharms && kk.m == key.m;
+        if (!R.capture && !reuse) H->nv_key_ok = false;   // h_nvalid is rewritten below
+        const int64_t profiles0 = S.profiles;
+        if (reuse) S.profiles += kk.profiles;
+        for (int b = 0; b < nb && !reuse; ++b) {
             const int64_t c = c0 + b;
             // global trial of the block's first trial
             const int64_t tb = R.blist ? R.blist[c] * (int64_t)Nprof : R.t_base + c * (int64_t)Nprof;
@@ -877,6 +920,11 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
                         window_index(&H->ms_edges[(size_t)l * (mnw + 1)], mnw, f);
                 }
             }
+        }
+        if (cacheable && !reuse) {
+            H->nv_key = key;
+            H->nv_key.profiles = S.profiles - profiles0;
+            H->nv_key_ok = true;
         }
         if (mwin)
             CS_CUDA(cudaMemcpyAsync(H->d_mwin.p, mwin, (size_t)nb * nlev * sizeof(int32_t), cudaMemcpyHostToDevice,

@@ -336,10 +336,12 @@ struct cs_handle {
     size_t mem_limit = 0;   // cs_set_memory_limit: device bytes the handle may hold (0: no cap)
     // launch shapes (cs_autotune): interpolation kernel (-1: by applicability,
     // 0: one CTA per item, 1: persistent), the tensor epilogue's segment
-    // divisors per phase (0: cost model) and its base-level double buffer
-    int tune_interp = -1;
-    int tune_div[2] = {0, 0};
-    int tune_dbuf = 1;
+    // divisors per phase (0: cost model) and its form (0 one slot, 1 phased
+    // double buffer, 2 split).  The defaults are the shapes the tuner picks on
+    // the survey workload (nharms 60, six levels), measured fastest there.
+    int tune_interp = 0;
+    int tune_div[2] = {3, 2};
+    int tune_dbuf = 0;
     int tune_sigma = 0;
     double stats_sigma_min = 0.0;   // cs_autotune: least sigma-stage time of its last timed configuration     // block-sigma kernel: 0 = 384 threads, twiddles in shared memory; 1 = 256, through L1
     bool interp2_used = false, interp2_ok = false;   // the last search's interpolation kernel / its applicability

@@ -430,8 +430,10 @@ typedef struct cs_tune_report {
  * (the least of 3 runs after a warm-up), and the fastest kept on the handle.
  * Every candidate computes the same values, so candidates are unchanged.  The
  * choice is also cached for the device and these parameters: handles created
- * later with the same cs_params on the same device start with it.  No
- * counterpart in the reference. */
+ * later with the same cs_params on the same device start with it.  An
+ * untuned handle runs one CTA per interpolation item, 384-thread sigma and
+ * the one-slot epilogue with segment divisors 3 and 2 (the tuner's choice on
+ * the nharms-60 survey workload).  No counterpart in the reference. */
 cs_status cs_autotune(cs_handle* h, double lofreq, double hifreq, int64_t lobin, int64_t blocksize, int64_t nsample,
                       cs_tune_report* out);
 

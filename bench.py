@@ -156,7 +156,7 @@ def sigma_flops_per_block():
 # DRAM bytes (read + write) per trial of one launch, from the ncu captures
 # summarised under profiles/ (small survey case, 1,282,048 trials; the traffic
 # of these kernels grows in proportion to the trial count).
-NCU_BYTES_PER_TRIAL = {"k_interp": 295.0, "k_synth_tc": 260.0, "k_sigma": 98.8, "k_rescue": 0.44}
+NCU_BYTES_PER_TRIAL = {"k_interp": 294.9, "k_synth_tc": 260.1, "k_sigma": 100.9, "k_rescue": 0.44}
 
 
 def load_peaks():

@@ -671,6 +671,11 @@ def main():
         cpu = {"value": r["trials"] / secs[1], "unit": "trials/s", "cores": r["threads"], "kind": "port",
                "sample": f"{what} ({r['blocks']} blocks, {r['trials']} trials), median of 3 runs; "
                          + CPU_PORT_NOTE}
+        # and one thread alone, on 32 mid-band blocks (the per-core rate)
+        one = [cpu_band_run(1, nblocks=32) for _ in range(3)]
+        s1 = sorted(o["seconds"] for o in one)
+        cpu["value_1thread"] = one[0]["trials"] / s1[1]
+        cpu["sample_1thread"] = f"{one[0]['blocks']} mid-band blocks, {one[0]['trials']} trials, median of 3 runs"
     except Exception as e:  # the baseline is reported, never required
         cpu = {"value": None, "unit": "trials/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
     cfg = workload_config(args.synth)

@@ -725,8 +725,10 @@ __global__ void __launch_bounds__(256) k_amax(const float2* __restrict__ amps, i
 cudaError_t launch_amax(const float2* amps, int64_t n, int64_t unit, int nchunk, uint32_t* out, cudaStream_t st,
                         int num_sms) {
     if (nchunk < 1 || nchunk > kMaxSpecChunks || unit < 1) return cudaErrorInvalidValue;
-    const int gx = std::max(1, num_sms * 4 / nchunk);
-    k_amax<<<dim3(gx, nchunk), 256, 0, st>>>(amps, n, unit, out);
+    // every chunk gets the full grid row (the last holds half the bins; the
+    // small ones leave most of theirs idle), so the largest chunk has enough
+    // loads in flight
+    k_amax<<<dim3(num_sms * 4, nchunk), 256, 0, st>>>(amps, n, unit, out);
     return cudaGetLastError();
 }
 

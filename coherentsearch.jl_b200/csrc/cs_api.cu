@@ -323,6 +323,10 @@ struct cs_handle {
     DBuf d_bm_r, d_bm_h, d_bm_st, d_bm_prof, d_bm_w, d_bm_sig, d_bm_out;   // block_metrics
     // batch: spectra copied on a second stream into two alternating buffers
     cudaStream_t copy_stream = nullptr;
+    // a second compute stream: the overlapped search's interpolation runs
+    // alternate between it and the handle's stream (fork and join events)
+    cudaStream_t run_stream = nullptr;
+    cudaEvent_t run_fork_ev = nullptr, run_join_ev = nullptr;
     cudaEvent_t copy_ev[2] = {nullptr, nullptr};
     DBuf d_batch[2];
     HBuf h_mwin, h_mst;
@@ -951,32 +955,45 @@ cs_status run_blocks(cs_handle* H, const RunSpec& R, std::vector<DevCand>* cands
             a.blk_cidx = H->d_nvalid.as<int32_t>() + (size_t)nb * nlev;
         }
         if (!R.capture) CS_CUDA(cudaEventRecord(H->ev[0], H->stream), "event");
-        auto interp_launch = [&](const WaveArgs& w) {
-            return interp2 ? launch_interp2(w, H->stream, win_max, d_err, H->num_sms)
-                           : launch_interp(w, H->stream, win_max, d_err);
+        auto interp_launch = [&](const WaveArgs& w, cudaStream_t st) {
+            return interp2 ? launch_interp2(w, st, win_max, d_err, H->num_sms) : launch_interp(w, st, win_max, d_err);
         };
         if (overlap) {
-            // runs of blocks by the last chunk they read (the running maximum
-            // of cidx): each run starts once that chunk has landed
-            int s = 0, need = cidx[0];
+            // Runs of blocks by the last chunk they read (the running maximum
+            // of cidx): each run starts once that chunk has landed.  The runs
+            // write disjoint blocks, so they alternate between the handle's
+            // stream and a second one, each run's start overlapping the
+            // previous run's tail; the handle's stream joins the second after
+            // the last run.
+            if (!H->run_stream)
+                CS_CUDA(cudaStreamCreateWithFlags(&H->run_stream, cudaStreamNonBlocking), "run stream");
+            if (!H->run_fork_ev) CS_CUDA(cudaEventCreateWithFlags(&H->run_fork_ev, cudaEventDisableTiming), "event");
+            if (!H->run_join_ev) CS_CUDA(cudaEventCreateWithFlags(&H->run_join_ev, cudaEventDisableTiming), "event");
+            CS_CUDA(cudaEventRecord(H->run_fork_ev, H->stream), "event");   // after the uploads above
+            CS_CUDA(cudaStreamWaitEvent(H->run_stream, H->run_fork_ev, 0), "fork");
+            int s = 0, need = cidx[0], run = 0;
             for (int b = 1; b <= nb; ++b) {
                 if (b < nb && cidx[b] <= need) continue;
                 WaveArgs w = a;
                 w.blk_first = s;
                 w.nblk = b - s;
-                CS_CUDA(cudaStreamWaitEvent(H->stream, H->chunk_ev[need], 0), "wait for a spectrum chunk");
-                CS_CUDA(interp_launch(w), "interp launch");
+                cudaStream_t st = (run & 1) ? H->run_stream : H->stream;
+                CS_CUDA(cudaStreamWaitEvent(st, H->chunk_ev[need], 0), "wait for a spectrum chunk");
+                CS_CUDA(interp_launch(w, st), "interp launch");
                 S.launches += 1;
+                ++run;
                 if (b < nb) {
                     s = b;
                     need = cidx[b];
                 }
             }
+            CS_CUDA(cudaEventRecord(H->run_join_ev, H->run_stream), "event");
+            CS_CUDA(cudaStreamWaitEvent(H->stream, H->run_join_ev, 0), "join");
             CS_CUDA(spec_ready(H), "wait for the spectrum");
             H->chunks_pending = false;
             overlap = false;
         } else {
-            CS_CUDA(interp_launch(a), "interp launch");
+            CS_CUDA(interp_launch(a, H->stream), "interp launch");
             S.launches += 1;
         }
         if (!R.capture) CS_CUDA(cudaEventRecord(H->ev[1], H->stream), "event");
@@ -1279,6 +1296,12 @@ cs_status cs_destroy(cs_handle* H) {
     for (auto& e : H->chunk_ev)
         if (e) cudaEventDestroy(e);
     if (H->spec_free_ev) cudaEventDestroy(H->spec_free_ev);
+    if (H->run_fork_ev) cudaEventDestroy(H->run_fork_ev);
+    if (H->run_join_ev) cudaEventDestroy(H->run_join_ev);
+    if (H->run_stream) {
+        cudaStreamSynchronize(H->run_stream);
+        cudaStreamDestroy(H->run_stream);
+    }
     H->d_amax_spec.release();
     if (H->copy_stream) cudaStreamDestroy(H->copy_stream);
     DBuf* mbufs[] = {&H->d_mst, &H->d_mwin, &H->d_mhist, &H->d_muo, &H->d_norm, &H->d_bm_r, &H->d_bm_h,

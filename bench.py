@@ -222,6 +222,7 @@ def run_dmsweep(args, rank, local_rank):
     with ClockSampler(local_rank) as clk:
         ms, launches, trials, ncand, _ = timed(on_dev, True, args.steps)
         torch.cuda.synchronize()
+    timed(on_host, False, 1)   # (pinned host spectra: the ordinary run and the graph capture)
     ms_e2e, _, _, _, d2h = timed(on_host, False, args.steps)
     gc.enable()
     h2d = sum(a.nbytes for a, _, _ in files)

@@ -305,7 +305,10 @@ struct cs_handle {
     std::vector<GraphSlot> gslots;
     std::vector<cs_spectrum> gkey;
     double gkey_d[3] = {0, 0, 0};
-    int64_t gkey_i[2] = {0, 0};
+    int64_t gkey_i[3] = {0, 0, 0};     // lobin, blocksize, spectra on the device
+    // a graph of page-locked host spectra: each file's copy into the batch
+    // buffer of its parity, on the copy stream forked into the capture
+    cudaEvent_t bg_copied_ev[2] = {nullptr, nullptr}, bg_done_ev[2] = {nullptr, nullptr};
     int64_t plan_bytes = 0;
     // metric statistics (MetricStats) and normalisation (MetricNorm)
     bool ms_on = false;
@@ -1507,8 +1510,8 @@ constexpr int kGraphPrefix = 4096;   // candidates a captured search reads back 
 // own pinned slot, the search's launches and the readback of its counters
 // and candidate prefix into that slot.  Not an error when a spectrum cannot
 // be captured (more than one wave): the batch then stays ordinary.
-void capture_batch(cs_handle* H, const cs_spectrum* files, int nfiles, double lofreq, double hifreq, int64_t lobin,
-                   int64_t blocksize, double threshold) {
+void capture_batch(cs_handle* H, const cs_spectrum* files, int nfiles, int on_device, double lofreq, double hifreq,
+                   int64_t lobin, int64_t blocksize, double threshold) {
     if (H->gexec) cudaGraphExecDestroy(H->gexec);
     H->gexec = nullptr;
     H->graph_valid = false;
@@ -1519,6 +1522,7 @@ void capture_batch(cs_handle* H, const cs_spectrum* files, int nfiles, double lo
     H->gkey_d[2] = threshold;
     H->gkey_i[0] = lobin;
     H->gkey_i[1] = blocksize;
+    H->gkey_i[2] = on_device;
     const cs_stats keep = H->stats;   // the batch's own statistics survive the capture
     struct Restore {
         cs_handle* H;
@@ -1531,7 +1535,7 @@ void capture_batch(cs_handle* H, const cs_spectrum* files, int nfiles, double lo
     std::vector<RunSpec> specs(nfiles);
     std::vector<char> empty(nfiles, 1);
     for (int i = 0; i < nfiles; ++i) {
-        H->amps = reinterpret_cast<const float2*>(files[i].amps);
+        H->amps = on_device ? reinterpret_cast<const float2*>(files[i].amps) : H->d_batch[i & 1].as<float2>();
         H->namps = files[i].namps;
         H->N = files[i].N;
         H->dt = files[i].dt;
@@ -1544,11 +1548,47 @@ void capture_batch(cs_handle* H, const cs_spectrum* files, int nfiles, double lo
             H->gslots[i].nvalid.ensure((size_t)specs[i].nblocks * (nlev + 1) * sizeof(int32_t)) != cudaSuccess)
             return;
     }
+    if (!on_device) {
+        if (!H->copy_stream || !H->copy_ev[0]) return;   // the ordinary run before made them
+        for (int b = 0; b < 2; ++b) {
+            if (!H->bg_copied_ev[b] && cudaEventCreateWithFlags(&H->bg_copied_ev[b], cudaEventDisableTiming)) return;
+            if (!H->bg_done_ev[b] && cudaEventCreateWithFlags(&H->bg_done_ev[b], cudaEventDisableTiming)) return;
+        }
+    }
     if (cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) return;
     bool ok = true;
+    // Host spectra: file i lands in batch buffer i&1 by a copy on the copy
+    // stream, issued before file i-1's search so that the two overlap; the
+    // copy into a buffer waits for the search two files back that read it.
+    auto copy_file = [&](int i) -> bool {
+        const int b = i & 1;
+        if (i >= 2 && cudaStreamWaitEvent(H->copy_stream, H->bg_done_ev[b], 0) != cudaSuccess) return false;
+        if (cudaMemcpyAsync(H->d_batch[b].p, files[i].amps, (size_t)files[i].namps * sizeof(float2),
+                            cudaMemcpyHostToDevice, H->copy_stream) != cudaSuccess)
+            return false;
+        return cudaEventRecord(H->bg_copied_ev[b], H->copy_stream) == cudaSuccess;
+    };
+    if (!on_device && nfiles > 0) {
+        // fork the copy stream into the capture
+        ok = cudaEventRecord(H->copy_ev[0], H->stream) == cudaSuccess &&
+             cudaStreamWaitEvent(H->copy_stream, H->copy_ev[0], 0) == cudaSuccess && copy_file(0);
+    }
     for (int i = 0; i < nfiles && ok; ++i) {
-        if (empty[i]) continue;
-        H->amps = reinterpret_cast<const float2*>(files[i].amps);
+        if (!on_device) {
+            if (i + 1 < nfiles && !copy_file(i + 1)) {
+                ok = false;
+                break;
+            }
+            if (cudaStreamWaitEvent(H->stream, H->bg_copied_ev[i & 1], 0) != cudaSuccess) {
+                ok = false;
+                break;
+            }
+        }
+        if (empty[i]) {
+            if (!on_device) ok = cudaEventRecord(H->bg_done_ev[i & 1], H->stream) == cudaSuccess;
+            continue;
+        }
+        H->amps = on_device ? reinterpret_cast<const float2*>(files[i].amps) : H->d_batch[i & 1].as<float2>();
         H->namps = files[i].namps;
         H->N = files[i].N;
         H->dt = files[i].dt;
@@ -1560,6 +1600,7 @@ void capture_batch(cs_handle* H, const cs_spectrum* files, int nfiles, double lo
         std::vector<DevCand> unused;   // (the candidates come back through the slot)
         ok = run_blocks(H, R, &unused, nullptr) == CS_OK;
         H->gslots[i].launches = H->stats.launches;
+        if (ok && !on_device) ok = cudaEventRecord(H->bg_done_ev[i & 1], H->stream) == cudaSuccess;
     }
     cudaGraph_t g = nullptr;
     const cudaError_t ec = cudaStreamEndCapture(H->stream, &g);
@@ -1681,11 +1722,19 @@ cs_status cs_search_batch(cs_handle* H, const cs_spectrum* files, int32_t nfiles
     std::vector<cs_candidate> all;
     std::vector<int32_t> owner;
     cs_stats tot{};
-    const bool want_graph = on_device && H->batch_graph && nfiles > 0;
+    // a replayable graph: device spectra, or host spectra that are all page-locked
+    // (the graph's copies read them in place at every replay)
+    bool host_pinned = !on_device && nfiles > 0;
+    for (int i = 0; i < nfiles && host_pinned; ++i) {
+        cudaPointerAttributes at{};
+        host_pinned = cudaPointerGetAttributes(&at, files[i].amps) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    }
+    cudaGetLastError();   // (an unregistered pointer is an answer, not an error)
+    const bool want_graph = (on_device || host_pinned) && H->batch_graph && nfiles > 0;
     auto same_key = [&]() {
         if ((int)H->gkey.size() != nfiles) return false;
         if (H->gkey_d[0] != lofreq || H->gkey_d[1] != hifreq || H->gkey_d[2] != threshold ||
-            H->gkey_i[0] != lobin || H->gkey_i[1] != blocksize)
+            H->gkey_i[0] != lobin || H->gkey_i[1] != blocksize || H->gkey_i[2] != on_device)
             return false;
         for (int i = 0; i < nfiles; ++i)
             if (H->gkey[i].amps != files[i].amps || H->gkey[i].namps != files[i].namps || H->gkey[i].N != files[i].N ||
@@ -1700,7 +1749,7 @@ cs_status cs_search_batch(cs_handle* H, const cs_spectrum* files, int32_t nfiles
         CS_CUDA(cudaStreamSynchronize(H->stream), "batch graph");
         for (int i = 0; i < nfiles; ++i) {
             const cs_spectrum& f = files[i];
-            H->amps = reinterpret_cast<const float2*>(f.amps);
+            H->amps = on_device ? reinterpret_cast<const float2*>(f.amps) : H->d_batch[i & 1].as<float2>();
             H->namps = f.namps;
             H->N = f.N;
             H->dt = f.dt;
@@ -1716,7 +1765,14 @@ cs_status cs_search_batch(cs_handle* H, const cs_spectrum* files, int32_t nfiles
                 const int n_c = counts[1];
                 if (n_c > kGraphPrefix) {
                     // more candidates than the captured prefix: search this one
-                    // again the ordinary way (the graph is dropped and rebuilt)
+                    // again the ordinary way (the graph is dropped and rebuilt);
+                    // a host spectrum is copied to the batch buffer first
+                    if (!on_device) {
+                        CS_CUDA(cudaMemcpyAsync(H->d_batch[0].p, f.amps, (size_t)f.namps * sizeof(float2),
+                                                cudaMemcpyHostToDevice, H->stream),
+                                "copy spectrum");
+                        H->amps = H->d_batch[0].as<float2>();
+                    }
                     st = search_core(H, lofreq, hifreq, lobin, blocksize, threshold, 0, 0, -1, &all);
                     if (st != CS_OK) return st;
                     // the re-search's own launches and copies count too
@@ -1735,6 +1791,7 @@ cs_status cs_search_batch(cs_handle* H, const cs_spectrum* files, int32_t nfiles
                 tot.waves += 1;
                 tot.launches += H->gslots[i].launches;
                 tot.d2h_bytes += 64 + (int64_t)std::min(n_c, kGraphPrefix) * (int64_t)sizeof(DevCand);
+                if (!on_device) tot.h2d_bytes += f.namps * (int64_t)sizeof(float2);
             }
             owner.insert(owner.end(), all.size() - before, i);
         }
@@ -1782,7 +1839,7 @@ cs_status cs_search_batch(cs_handle* H, const cs_spectrum* files, int32_t nfiles
     }
     H->stats = tot;
     if (want_graph && !(key_match && H->graph_failed))
-        capture_batch(H, files, nfiles, lofreq, hifreq, lobin, blocksize, threshold);
+        capture_batch(H, files, nfiles, on_device, lofreq, hifreq, lobin, blocksize, threshold);
     H->has_spec = false;   // the batch buffers are not a spectrum of the handle's
     const int64_t n = (int64_t)all.size();
     std::copy_n(all.begin(), std::min(n, cap), out);

@@ -416,3 +416,48 @@ def test_batch_graph_replays_the_ordinary_batch():
     eng.search_raw(1.0, 60.0, 100, 2048, 8.0)
     got3, own3 = eng.search_batch_raw(files, 1.0, 60.0, 100, 2048, 8.0, on_device=True)
     assert np.array_equal(got3, want2) and np.array_equal(own3, wown2)
+
+
+def test_batch_graph_of_pinned_host_spectra():
+    """cs_set_batch_graph with page-locked host spectra: each file's copy into
+    the batch buffer of its parity is captured with the searches (the copy of
+    file i+1 under file i's search) and replayed -- the same records as the
+    ordinary batch of pageable copies, also after the pinned buffers are
+    refilled in place, with every file's bytes counted as copied."""
+    import torch
+    from cohsearch import synth
+    cs = _cs()
+    lens = [1 << 20, 1 << 21, 1 << 20, 1 << 19]
+
+    def spectra(seed):
+        out = []
+        for i, n in enumerate(lens):
+            ps = synth.random_pulsars(np.random.default_rng(seed + i), 6, 0.5, 200.0, 0.02, 0.2, 8.0, 20.0)
+            out.append(synth.make_spectrum_fd(n, 64e-6, ps, seed + i))
+        return out
+    first = spectra(700)
+    pinned = [torch.from_numpy(a.view(np.float32).copy()).pin_memory() for a in first]
+    files = [(p.numpy().view(np.complex64), n, 64e-6) for p, n in zip(pinned, lens)]
+    params = cs.SearchParams(nharms=32, m=16, decimations=cs.decimation_set(32, 4), synth="fp16")
+    ref = cs.Engine(params)
+    want, wown = ref.search_batch_raw([(a, n, 64e-6) for a, n in zip(first, lens)], 1.0, 60.0, 100, 2048, 8.0)
+    assert len(want) > 0
+    side = torch.cuda.Stream()
+    eng = cs.Engine(params)
+    eng.set_stream(side.cuda_stream)
+    eng.set_batch_graph(True)
+    for it in range(3):                      # ordinary run and capture, then replays
+        got, own = eng.search_batch_raw(files, 1.0, 60.0, 100, 2048, 8.0)
+        side.synchronize()
+        assert np.array_equal(got, want) and np.array_equal(own, wown)
+        st = eng.stats()
+        assert st["h2d_bytes"] >= sum(n // 2 * 8 for n in lens)
+        # a replay times no stage (its kernels run inside one graph launch)
+        assert (st["ms_interp"] == 0.0) == (it > 0), (it, st["ms_interp"])
+    second = spectra(1100)
+    for p, a in zip(pinned, second):
+        p.copy_(torch.from_numpy(a.view(np.float32).copy()))
+    want2, wown2 = ref.search_batch_raw([(a, n, 64e-6) for a, n in zip(second, lens)], 1.0, 60.0, 100, 2048, 8.0)
+    got2, own2 = eng.search_batch_raw(files, 1.0, 60.0, 100, 2048, 8.0)
+    side.synchronize()
+    assert np.array_equal(got2, want2) and np.array_equal(own2, wown2)

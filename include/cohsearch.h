@@ -154,9 +154,11 @@ cs_status cs_search_range(cs_handle* h, double lofreq, double hifreq, int64_t lo
                           double threshold, int32_t exact_all, int64_t block_begin, int64_t block_end,
                           cs_candidate* out, int64_t cap, int64_t* n_out);
 
-/* enable != 0: cs_search_batch over device spectra (on_device = 1) runs the
- * batch the ordinary way once, captures it into one CUDA graph -- per
- * spectrum its uploads, launches and readback, no host round trip between
+/* enable != 0: cs_search_batch over device spectra (on_device = 1), or over
+ * host spectra that are all page-locked, runs the batch the ordinary way
+ * once, captures it into one CUDA graph -- per spectrum its uploads (for host
+ * spectra the copy into a batch buffer, overlapped with the previous
+ * spectrum's search), launches and readback, no host round trip between
  * spectra -- and replays that graph while later calls repeat the same batch
  * (same spectrum addresses, lengths, band and threshold; refill the spectra
  * in place between calls).  Any other search on the handle drops the graph.

@@ -447,8 +447,8 @@ def cpu_band_run(nthreads, nblocks=None, seed=2, first_block=None):
     """Time the C port of the reference search (oracle/cs_cpu.c, all given
     threads, blocks dealt round-robin as the reference's tasks take chunks) on
     the survey workload: the whole band by default, else `nblocks` blocks from
-    `first_block` (mid-band when not given).  The port's c2r transform is a
-    direct FP64 DFT where the reference calls FFTW."""
+    `first_block` (mid-band when not given).  The port's c2r transform is its
+    own mixed-radix FP64 FFT where the reference calls FFTW."""
     from oracle import cs_cpu
     if seed not in _CPU_SPECTRUM:
         from cohsearch import synth
@@ -468,8 +468,8 @@ def cpu_band_run(nthreads, nblocks=None, seed=2, first_block=None):
 
 
 CPU_PORT_NOTE = ("C restatement of the reference's production search (Float32-weight interpolation, FP64 "
-                 "profiles, block sigma, batched FP32 gate, exact rescan); its c2r transform is a direct FP64 "
-                 "DFT where the reference calls FFTW")
+                 "profiles, block sigma, batched FP32 gate, exact rescan); its c2r transform is its own "
+                 "mixed-radix FP64 FFT where the reference calls FFTW")
 
 
 def main():

@@ -9,10 +9,12 @@
  *   - build_direct_plans with Float32 weights (src/directinterp.jl:342-405):
  *     FP64 tables rounded once;
  *   - fill_harmonic_row_direct! (src/directinterp.jl:470-572): residue state
- *     by exact 128-bit divrem (direct_chunk_state, :414-418), phase row lookup,
+ *     by exact 128-bit divrem at the row's first trial (direct_chunk_state,
+ *     :414-418) and exact integer steps after it, phase row lookup,
  *     range guard on the true trial range, sequential FP32 fmaf over the m taps,
  *     unfused Complex{Float32} product;
- *   - _fill_row_direct_slow! (:623-661) for a non-rational trial step.
+ *   - _fill_row_direct_slow! (:623-661) for a non-rational trial step;
+ *   - the profile stage's brfft as a mixed-radix FFT (ft_c2r).
  * Built with -ffp-contract=off so only the explicit fma calls fuse.
  */
 #include <math.h>
@@ -171,21 +173,41 @@ static void fill_row(const plan_t* d, const float* amps, int64_t namps, int64_t 
     int64_t lo_trial = d->rfloor0 + qint + d->carry[d->row[res]] + 2 - m2;          /* 1-based */
     int64_t hi_trial = d->rfloor0 + qintl + d->carry[d->row[resl]] + 1 + m2;
     if (!(lo_trial >= 1 && hi_trial <= namps && (d->rfloor0 + qintl) < Nhalf)) return;
-    for (int64_t k = 0; k < n; ++k) {
-        int64_t r_, qi;
-        chunk_state(d, t0 + k, &r_, &qi);
-        int p = d->row[r_];
-        int64_t base = d->rfloor0 + qi + d->carry[p] + 1 - m2;  /* 0-based first tap */
-        const float* w = d->W + (size_t)p * m;
-        float sre = 0.0f, sim = 0.0f;
-        for (int i = 0; i < m; ++i) {
-            sre = fmaf(w[i], amps[2 * (base + i)], sre);
-            sim = fmaf(w[i], amps[2 * (base + i) + 1], sim);
+    /* Trials in groups of FR_V.  The state steps exactly from trial to trial,
+     * as the reference advances it (src/directinterp.jl:563-567): one trial
+     * adds base_adv to qint and s to res, with a carry of one bin when res
+     * passes q.  Each trial keeps its own sequential fmaf chain over the taps;
+     * the group's FR_V chains are independent, so they overlap. */
+    enum { FR_V = 8 };
+    int64_t r_ = res, qi = qint;
+    for (int64_t k0 = 0; k0 < n; k0 += FR_V) {
+        const int nv = (n - k0) < FR_V ? (int)(n - k0) : FR_V;
+        int64_t ao[FR_V];
+        int pv[FR_V];
+        for (int v = 0; v < FR_V; ++v) {
+            if (v >= nv) { pv[v] = pv[0]; ao[v] = ao[0]; continue; }   /* padding lanes, discarded */
+            const int p = d->row[r_];
+            pv[v] = p;
+            ao[v] = 2 * (d->rfloor0 + qi + d->carry[p] + 1 - m2);      /* 0-based first tap */
+            qi += d->base_adv;
+            r_ += d->s;
+            if (r_ >= d->q) { r_ -= d->q; ++qi; }
         }
-        float ar = d->A[2 * p], ai = d->A[2 * p + 1];
-        float pr0 = ar * sre, pr1 = ai * sim, pi0 = ar * sim, pi1 = ai * sre;
-        out[2 * k] = pr0 - pr1;
-        out[2 * k + 1] = pi0 + pi1;
+        float sre[FR_V], sim[FR_V];
+        for (int v = 0; v < FR_V; ++v) { sre[v] = 0.0f; sim[v] = 0.0f; }
+        for (int i = 0; i < m; ++i)
+            for (int v = 0; v < FR_V; ++v) {
+                const float w = d->W[(size_t)pv[v] * m + i];
+                sre[v] = fmaf(w, amps[ao[v] + 2 * i], sre[v]);
+                sim[v] = fmaf(w, amps[ao[v] + 2 * i + 1], sim[v]);
+            }
+        for (int v = 0; v < nv; ++v) {
+            const int p = pv[v];
+            float ar = d->A[2 * p], ai = d->A[2 * p + 1];
+            float pr0 = ar * sre[v], pr1 = ai * sim[v], pi0 = ar * sim[v], pi1 = ai * sre[v];
+            out[2 * (k0 + v)] = pr0 - pr1;
+            out[2 * (k0 + v) + 1] = pi0 + pi1;
+        }
     }
 }
 
@@ -219,11 +241,273 @@ int csref_plan_tables(int nharms, int m, double hidr, double r_lo, int h, float*
 }
 
 /* ------------------------------------------------------------------------
+ * The profile stage's c2r transform in FP64, vectorised across trials: the
+ * unnormalised brfft the reference applies to each trial's stacked harmonics
+ * (src/search.jl:1291, :1675),
+ *     prof[t] = X[H] (-1)^t + 2 sum_{j=1}^{H-1} Re(X[j] e^{+2 pi i j t / 2H}),
+ * t = 0 .. 2H-1 (the DC term is zero on this path, and brfft drops the
+ * imaginary parts of DC and Nyquist).
+ *
+ * Computed as one complex FFT of length H: with the even/odd split of a real
+ * sequence, z[n] = prof[2n] + i prof[2n+1] is the inverse DFT of
+ *     Z[j] = E[j] + i O[j],  E[j] = X[j] + conj(X[H-j]),
+ *                            O[j] = (X[j] - conj(X[H-j])) e^{+i pi j / H}
+ * (Z[0] = X[H] (1 - i)).  The length-H transform is a mixed-radix
+ * (4, 2, 3, 5) self-sorting Stockham decimation in frequency: a stage of
+ * radix p over sequences of length n = p m at stride s maps
+ *     y[q + s (p u + j)] = w_n^{j u} sum_k x[q + s (u + k m)] w_p^{j k}
+ * (w_r = e^{+2 pi i / r}), then the next stage takes length m at stride p s;
+ * after the last the output is in natural order.  Each element is a vector of
+ * up to FT_LANES trials, so every loop runs over contiguous lanes.  Lengths
+ * with another prime factor keep the direct symmetric DFT.
+ * ------------------------------------------------------------------------ */
+#define FT_LANES 64
+#define FT_MAXST 24
+
+typedef struct {
+    int H, nst, rad[FT_MAXST];
+    double* tw[FT_MAXST];   /* stage s: m x (p-1) complex w_n^{j u}, [u][j-1] */
+    double* pre;            /* H complex e^{+i pi j / H} */
+    double* C2;             /* direct DFT (other lengths): (H) x (H+1) 2 cos(2 pi j t / 2H) */
+    double* S2;             /* and -2 sin */
+} ft_plan_t;
+
+static void ft_free(ft_plan_t* P) {
+    for (int s = 0; s < P->nst; ++s) free(P->tw[s]);
+    free(P->pre);
+    free(P->C2);
+    free(P->S2);
+    memset(P, 0, sizeof(*P));
+}
+
+static void ft_init(ft_plan_t* P, int H) {
+    memset(P, 0, sizeof(*P));
+    P->H = H;
+    const int nb = 2 * H;
+    int n = H, ok = 1;
+    while (n > 1 && ok) {
+        const int p = n % 4 == 0 ? 4 : n % 2 == 0 ? 2 : n % 3 == 0 ? 3 : n % 5 == 0 ? 5 : 0;
+        if (!p || P->nst == FT_MAXST) ok = 0;
+        else { P->rad[P->nst++] = p; n /= p; }
+    }
+    if (!ok) {
+        P->nst = 0;
+        P->C2 = (double*)calloc((size_t)H * (H + 1), sizeof(double));
+        P->S2 = (double*)calloc((size_t)H * (H + 1), sizeof(double));
+        for (int j = 1; j < H; ++j)
+            for (int q = 0; q <= H; ++q) {
+                double ang = 2.0 * M_PI * (double)(((int64_t)j * q) % nb) / (double)nb;
+                P->C2[(size_t)j * (H + 1) + q] = 2.0 * cos(ang);
+                P->S2[(size_t)j * (H + 1) + q] = -2.0 * sin(ang);
+            }
+        return;
+    }
+    n = H;
+    for (int s = 0; s < P->nst; ++s) {
+        const int p = P->rad[s], m = n / p;
+        P->tw[s] = (double*)malloc(sizeof(double) * 2 * (size_t)m * (p - 1));
+        for (int u = 0; u < m; ++u)
+            for (int j = 1; j < p; ++j) {
+                double ang = 2.0 * M_PI * (double)(((int64_t)j * u) % n) / (double)n;
+                P->tw[s][2 * ((size_t)u * (p - 1) + j - 1)] = cos(ang);
+                P->tw[s][2 * ((size_t)u * (p - 1) + j - 1) + 1] = sin(ang);
+            }
+        n = m;
+    }
+    P->pre = (double*)malloc(sizeof(double) * 2 * (size_t)H);
+    for (int j = 0; j < H; ++j) {
+        P->pre[2 * j] = cos(M_PI * (double)j / (double)H);
+        P->pre[2 * j + 1] = sin(M_PI * (double)j / (double)H);
+    }
+}
+
+/* The butterflies of one (u, q) of a stage: inputs a_k at x + k istep,
+ * outputs y_j = w_j * (sum_k a_k w_p^{jk}) at y + j ostep (w_0 = 1), for L
+ * lanes.  One function per radix, restrict-qualified, so each lane loop
+ * vectorises. */
+#define FT_ROT(r, i, wr, wi, outr, outi)  do { (outr) = (r) * (wr) - (i) * (wi); (outi) = (r) * (wi) + (i) * (wr); } while (0)
+
+static void ft_bf2(const double* __restrict xr, const double* __restrict xi, size_t is, double* __restrict yr,
+                   double* __restrict yi, size_t os, const double* w, int L) {
+    const double w1r = w[0], w1i = w[1];
+#pragma omp simd
+    for (int b = 0; b < L; ++b) {
+        const double ar = xr[b], ai = xi[b], br = xr[is + b], bi = xi[is + b];
+        yr[b] = ar + br; yi[b] = ai + bi;
+        FT_ROT(ar - br, ai - bi, w1r, w1i, yr[os + b], yi[os + b]);
+    }
+}
+
+static void ft_bf3(const double* __restrict xr, const double* __restrict xi, size_t is, double* __restrict yr,
+                   double* __restrict yi, size_t os, const double* w, int L) {
+    const double S3 = 0.86602540378443864676;   /* sin(2 pi / 3) */
+    const double w1r = w[0], w1i = w[1], w2r = w[2], w2i = w[3];
+#pragma omp simd
+    for (int b = 0; b < L; ++b) {
+        const double a0r = xr[b], a0i = xi[b], a1r = xr[is + b], a1i = xi[is + b];
+        const double a2r = xr[2 * is + b], a2i = xi[2 * is + b];
+        const double t1r = a1r + a2r, t1i = a1i + a2i;
+        const double t2r = a0r - 0.5 * t1r, t2i = a0i - 0.5 * t1i;
+        const double t3r = S3 * (a1r - a2r), t3i = S3 * (a1i - a2i);
+        yr[b] = a0r + t1r; yi[b] = a0i + t1i;
+        FT_ROT(t2r - t3i, t2i + t3r, w1r, w1i, yr[os + b], yi[os + b]);
+        FT_ROT(t2r + t3i, t2i - t3r, w2r, w2i, yr[2 * os + b], yi[2 * os + b]);
+    }
+}
+
+static void ft_bf4(const double* __restrict xr, const double* __restrict xi, size_t is, double* __restrict yr,
+                   double* __restrict yi, size_t os, const double* w, int L) {
+    const double w1r = w[0], w1i = w[1], w2r = w[2], w2i = w[3], w3r = w[4], w3i = w[5];
+#pragma omp simd
+    for (int b = 0; b < L; ++b) {
+        const double a0r = xr[b], a0i = xi[b], a1r = xr[is + b], a1i = xi[is + b];
+        const double a2r = xr[2 * is + b], a2i = xi[2 * is + b], a3r = xr[3 * is + b], a3i = xi[3 * is + b];
+        const double t0r = a0r + a2r, t0i = a0i + a2i;
+        const double t1r = a0r - a2r, t1i = a0i - a2i;
+        const double t2r = a1r + a3r, t2i = a1i + a3i;
+        const double t3r = -(a1i - a3i), t3i = a1r - a3r;   /* i (a1 - a3) */
+        yr[b] = t0r + t2r; yi[b] = t0i + t2i;
+        FT_ROT(t1r + t3r, t1i + t3i, w1r, w1i, yr[os + b], yi[os + b]);
+        FT_ROT(t0r - t2r, t0i - t2i, w2r, w2i, yr[2 * os + b], yi[2 * os + b]);
+        FT_ROT(t1r - t3r, t1i - t3i, w3r, w3i, yr[3 * os + b], yi[3 * os + b]);
+    }
+}
+
+static void ft_bf5(const double* __restrict xr, const double* __restrict xi, size_t is, double* __restrict yr,
+                   double* __restrict yi, size_t os, const double* w, int L) {
+    const double C51 = 0.30901699437494742410, C52 = -0.80901699437494742410;   /* cos(2 pi/5), cos(4 pi/5) */
+    const double S51 = 0.95105651629515357212, S52 = 0.58778525229247312917;    /* sin(2 pi/5), sin(4 pi/5) */
+    const double w1r = w[0], w1i = w[1], w2r = w[2], w2i = w[3], w3r = w[4], w3i = w[5], w4r = w[6], w4i = w[7];
+#pragma omp simd
+    for (int b = 0; b < L; ++b) {
+        const double a0r = xr[b], a0i = xi[b];
+        const double a1r = xr[is + b], a1i = xi[is + b], a2r = xr[2 * is + b], a2i = xi[2 * is + b];
+        const double a3r = xr[3 * is + b], a3i = xi[3 * is + b], a4r = xr[4 * is + b], a4i = xi[4 * is + b];
+        const double s1r = a1r + a4r, s1i = a1i + a4i, d1r = a1r - a4r, d1i = a1i - a4i;
+        const double s2r = a2r + a3r, s2i = a2i + a3i, d2r = a2r - a3r, d2i = a2i - a3i;
+        const double c1r = a0r + C51 * s1r + C52 * s2r, c1i = a0i + C51 * s1i + C52 * s2i;
+        const double c2r = a0r + C52 * s1r + C51 * s2r, c2i = a0i + C52 * s1i + C51 * s2i;
+        const double e1r = S51 * d1r + S52 * d2r, e1i = S51 * d1i + S52 * d2i;
+        const double e2r = S52 * d1r - S51 * d2r, e2i = S52 * d1i - S51 * d2i;
+        yr[b] = a0r + s1r + s2r; yi[b] = a0i + s1i + s2i;
+        FT_ROT(c1r - e1i, c1i + e1r, w1r, w1i, yr[os + b], yi[os + b]);           /* c1 + i e1 */
+        FT_ROT(c2r - e2i, c2i + e2r, w2r, w2i, yr[2 * os + b], yi[2 * os + b]);   /* c2 + i e2 */
+        FT_ROT(c2r + e2i, c2i - e2r, w3r, w3i, yr[3 * os + b], yi[3 * os + b]);   /* c2 - i e2 */
+        FT_ROT(c1r + e1i, c1i - e1r, w4r, w4i, yr[4 * os + b], yi[4 * os + b]);   /* c1 - i e1 */
+    }
+}
+
+/* One stage of radix p over sequences of length n at stride s (L lanes per
+ * element): y[q + s (p u + j)] = w_n^{j u} sum_k x[q + s (u + k m)] w_p^{jk}. */
+static void ft_stage(int p, int n, int s, const double* tw, const double* xr, const double* xi, double* yr,
+                     double* yi, int L) {
+    const int m = n / p;
+    const size_t istep = (size_t)s * m * L, ostep = (size_t)s * L;
+    for (int u = 0; u < m; ++u) {
+        const double* w = tw + 2 * (size_t)u * (p - 1);
+        for (int q = 0; q < s; ++q) {
+            const size_t i0 = (size_t)(q + s * u) * L, o0 = (size_t)(q + s * p * u) * L;
+            switch (p) {
+            case 2: ft_bf2(xr + i0, xi + i0, istep, yr + o0, yi + o0, ostep, w, L); break;
+            case 3: ft_bf3(xr + i0, xi + i0, istep, yr + o0, yi + o0, ostep, w, L); break;
+            case 4: ft_bf4(xr + i0, xi + i0, istep, yr + o0, yi + o0, ostep, w, L); break;
+            default: ft_bf5(xr + i0, xi + i0, istep, yr + o0, yi + o0, ostep, w, L); break;
+            }
+        }
+    }
+}
+
+/* prof[t * pstride + b] for t < 2H, b < n, from the harmonics
+ * X[j] = (re, im)[j * rstride + b], j = 1..H (row 0 is not read).  scratch:
+ * 4 H FT_LANES doubles (FFT) or 2 n doubles (direct DFT). */
+static void ft_c2r(const ft_plan_t* P, const double* re, const double* im, size_t rstride, double* prof,
+                   size_t pstride, int n, double* scratch) {
+    const int H = P->H, nb = 2 * H;
+    if (P->C2) {
+        double* E = scratch;
+        double* O = scratch + n;
+        const double* ny = re + (size_t)H * rstride;
+        for (int q = 0; q <= H; ++q) {
+            double sgn = (q & 1) ? -1.0 : 1.0;
+            for (int b = 0; b < n; ++b) { E[b] = sgn * ny[b]; O[b] = 0.0; }
+            for (int jh = 1; jh < H; ++jh) {
+                const double c2 = P->C2[(size_t)jh * (H + 1) + q], s2 = P->S2[(size_t)jh * (H + 1) + q];
+                const double* rr = re + (size_t)jh * rstride;
+                const double* ii = im + (size_t)jh * rstride;
+                for (int b = 0; b < n; ++b) { E[b] += rr[b] * c2; O[b] += ii[b] * s2; }
+            }
+            double* p0 = prof + (size_t)q * pstride;
+            for (int b = 0; b < n; ++b) p0[b] = E[b] + O[b];
+            if (q >= 1 && q < H) {
+                double* p1 = prof + (size_t)(nb - q) * pstride;
+                for (int b = 0; b < n; ++b) p1[b] = E[b] - O[b];
+            }
+        }
+        return;
+    }
+    const size_t V = (size_t)H * FT_LANES;
+    for (int b0 = 0; b0 < n; b0 += FT_LANES) {
+        const int L = n - b0 < FT_LANES ? n - b0 : FT_LANES;
+        double *xr = scratch, *xi = scratch + V, *yr = scratch + 2 * V, *yi = scratch + 3 * V;
+        const double* nr = re + (size_t)H * rstride + b0;
+        for (int b = 0; b < L; ++b) { xr[b] = nr[b]; xi[b] = -nr[b]; }
+        for (int j = 1; j < H; ++j) {
+            const double *ar = re + (size_t)j * rstride + b0, *ai = im + (size_t)j * rstride + b0;
+            const double *br = re + (size_t)(H - j) * rstride + b0, *bi = im + (size_t)(H - j) * rstride + b0;
+            const double c = P->pre[2 * j], s = P->pre[2 * j + 1];
+            double *zr = xr + (size_t)j * L, *zi = xi + (size_t)j * L;
+            for (int b = 0; b < L; ++b) {
+                const double er = ar[b] + br[b], ei = ai[b] - bi[b];   /* X[j] + conj(X[H-j]) */
+                const double dr = ar[b] - br[b], di = ai[b] + bi[b];   /* X[j] - conj(X[H-j]) */
+                const double orr = dr * c - di * s, oi = dr * s + di * c;
+                zr[b] = er - oi;
+                zi[b] = ei + orr;
+            }
+        }
+        int len = H, st = 1;
+        for (int k = 0; k < P->nst; ++k) {
+            ft_stage(P->rad[k], len, st, P->tw[k], xr, xi, yr, yi, L);
+            double* t = xr; xr = yr; yr = t;
+            t = xi; xi = yi; yi = t;
+            len /= P->rad[k];
+            st *= P->rad[k];
+        }
+        for (int t = 0; t < H; ++t) {
+            double* pe = prof + (size_t)(2 * t) * pstride + b0;
+            double* po = pe + pstride;
+            const double *zr = xr + (size_t)t * L, *zi = xi + (size_t)t * L;
+            for (int b = 0; b < L; ++b) { pe[b] = zr[b]; po[b] = zi[b]; }
+        }
+    }
+}
+
+static size_t ft_scratch(int Hmax, int n) {
+    size_t a = 4 * (size_t)Hmax * FT_LANES, b = 2 * (size_t)n;
+    return a > b ? a : b;
+}
+
+/* The profile stage's transform on n profiles, for the tests: X = (re, im)
+ * [H+1][n] (harmonic j's lanes at j * n; row 0 ignored), prof [2H][n].
+ * Returns the number of FFT stages (0 for the direct DFT of lengths with a
+ * prime factor above 5, or for H = 1), or -1 for bad arguments. */
+int csref_c2r(const double* re, const double* im, int H, int n, double* prof) {
+    if (H < 1 || n < 1 || !re || !im || !prof) return -1;
+    ft_plan_t P;
+    ft_init(&P, H);
+    double* scratch = (double*)malloc(sizeof(double) * ft_scratch(H, n));
+    ft_c2r(&P, re, im, (size_t)n, prof, (size_t)n, n, scratch);
+    const int nst = P.C2 ? 0 : P.nst;
+    free(scratch);
+    ft_free(&P);
+    return nst;
+}
+
+/* ------------------------------------------------------------------------
  * Full production search over a range of blocks, multithreaded: the timed
  * CPU restatement of `_search_region!` (src/search.jl:1768-1894) with the
  * default profile precision :f64.  Per block: Float32-weight interpolation
- * (fill_row above), the FP64 c2r transform of every level (direct symmetric
- * DFT, vectorised across the block's profiles), the block sigma
+ * (fill_row above), the FP64 c2r transform of every level (ft_c2r above: a
+ * mixed-radix FFT across the block's profiles), the block sigma
  * (src/search.jl:490-566), the batched Float32 zero-baseline gate over
  * 128-profile tiles and the FP64 scalar gate for the tail (:784-807), the
  * exact median rescan of trials reaching medcut (:893-904), and candidate
@@ -246,8 +530,7 @@ typedef struct {
     int nharms, m;
     double hidr, lodr, r_lo;
     int nlev, ks[CS_MAXLEV], Hk[CS_MAXLEV], nw[CS_MAXLEV], widths[CS_MAXLEV][CS_MAXW];
-    double* C2[CS_MAXLEV];   /* (Hk) x (Hk+1): 2cos(2 pi j n / N) */
-    double* S2[CS_MAXLEV];   /* -2 sin */
+    ft_plan_t ft[CS_MAXLEV]; /* each level's c2r transform (length Hk) */
     int64_t total;
     int Nprof;
     int64_t first_block, nblocks;
@@ -327,8 +610,9 @@ static void* worker(void* arg) {
     double* im = (double*)calloc((size_t)(nh + 1) * Np, sizeof(double));
     float* row = (float*)malloc(sizeof(float) * 2 * (size_t)Np);
     double* prof = (double*)malloc(sizeof(double) * (size_t)maxbins * Np);   /* [bin][b] */
-    double* E = (double*)malloc(sizeof(double) * (size_t)Np);
-    double* O = (double*)malloc(sizeof(double) * (size_t)Np);
+    int maxH = 1;
+    for (int l = 0; l < J->nlev; ++l) if (J->Hk[l] > maxH) maxH = J->Hk[l];
+    double* fts = (double*)malloc(sizeof(double) * ft_scratch(maxH, Np));
     double* sig = (double*)malloc(sizeof(double) * CS_SIGCAP);
     double* mv = (double*)malloc(sizeof(double) * (size_t)Np);
     float* psT = (float*)malloc(sizeof(float) * (size_t)CS_BATCH * (2 * maxbins + 2));
@@ -357,26 +641,8 @@ static void* worker(void* arg) {
                 nvalid = 0;
                 while (nvalid < n && (double)k * (rstart + (double)nvalid * J->lodr) < nyq) ++nvalid;
             }
-            /* c2r of the stride-k stack: prof[n] = E + O, prof[N-n] = E - O */
-            const double* C2 = J->C2[l];
-            const double* S2 = J->S2[l];
-            const double* ny = re + (size_t)(Hk * k) * Np;
-            for (int q = 0; q <= Hk; ++q) {
-                double sgn = (q & 1) ? -1.0 : 1.0;
-                for (int b = 0; b < n; ++b) { E[b] = sgn * ny[b]; O[b] = 0.0; }
-                for (int jh = 1; jh < Hk; ++jh) {
-                    const double c2 = C2[(size_t)jh * (Hk + 1) + q], s2 = S2[(size_t)jh * (Hk + 1) + q];
-                    const double* rr = re + (size_t)(jh * k) * Np;
-                    const double* ii = im + (size_t)(jh * k) * Np;
-                    for (int b = 0; b < n; ++b) { E[b] += rr[b] * c2; O[b] += ii[b] * s2; }
-                }
-                double* p0 = prof + (size_t)q * Np;
-                for (int b = 0; b < n; ++b) p0[b] = E[b] + O[b];
-                if (q >= 1 && q < Hk) {
-                    double* p1 = prof + (size_t)(nb - q) * Np;
-                    for (int b = 0; b < n; ++b) p1[b] = E[b] - O[b];
-                }
-            }
+            /* c2r of the stride-k stack (harmonics k, 2k, .., Hk k) */
+            ft_c2r(&J->ft[l], re, im, (size_t)k * Np, prof, (size_t)Np, n, fts);
             /* block sigma over the valid prefix */
             int64_t Ntot = (int64_t)nb * nvalid;
             int ns = 0;
@@ -466,7 +732,7 @@ static void* worker(void* arg) {
             pthread_mutex_unlock(&J->mu);
         }
     }
-    free(re); free(im); free(row); free(prof); free(E); free(O); free(sig); free(mv); free(psT);
+    free(re); free(im); free(row); free(prof); free(fts); free(sig); free(mv); free(psT);
     return NULL;
 }
 
@@ -547,14 +813,7 @@ int64_t csref_search_blocks_ex(const float* amps, int64_t namps, int64_t N, int 
         }
         if (np_ == 0) { memcpy(J.widths[l], full, sizeof(int) * nf); np_ = nf; }
         J.nw[l] = np_;
-        J.C2[l] = (double*)calloc((size_t)Hk * (Hk + 1), sizeof(double));
-        J.S2[l] = (double*)calloc((size_t)Hk * (Hk + 1), sizeof(double));
-        for (int j = 1; j < Hk; ++j)
-            for (int q = 0; q <= Hk; ++q) {
-                double ang = 2.0 * M_PI * (double)(((int64_t)j * q) % nb) / (double)nb;
-                J.C2[l][(size_t)j * (Hk + 1) + q] = 2.0 * cos(ang);
-                J.S2[l][(size_t)j * (Hk + 1) + q] = -2.0 * sin(ang);
-            }
+        ft_init(&J.ft[l], Hk);
     }
     J.plans = build_plans(nharms, m, hidr, r_lo);
     pthread_t th[256];
@@ -564,7 +823,7 @@ int64_t csref_search_blocks_ex(const float* amps, int64_t namps, int64_t N, int 
     for (int t = 0; t < nt; ++t) { wa[t].job = &J; wa[t].tid = t; pthread_create(&th[t], NULL, worker, &wa[t]); }
     for (int t = 0; t < nt; ++t) pthread_join(th[t], NULL);
     free_plans(J.plans, nharms);
-    for (int l = 0; l < nl; ++l) { free(J.C2[l]); free(J.S2[l]); }
+    for (int l = 0; l < nl; ++l) ft_free(&J.ft[l]);
     pthread_mutex_destroy(&J.mu);
     clock_gettime(CLOCK_MONOTONIC, &t1);
     if (seconds) *seconds = (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);

@@ -35,6 +35,8 @@ def load():
             ctypes.c_int64, ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
             ctypes.c_int64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p,
             ctypes.c_void_p]
+        lib.csref_c2r.restype = ctypes.c_int
+        lib.csref_c2r.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         _lib = lib
     return _lib
 
@@ -49,6 +51,22 @@ def interp_chunk(amps, N, nharms, m, hidr, r_lo, t0, n):
     if rc != 0:
         raise ValueError("csref_interp_chunk: bad arguments")
     return out
+
+
+def c2r(X):
+    """The port's profile-stage transform of harmonic stacks X, complex (H+1, n)
+    (row j = harmonic j of n trials; row 0 unused): the (2H, n) FP64 profiles
+    and the number of FFT stages used (0: the direct DFT)."""
+    lib = load()
+    X = np.asarray(X, np.complex128)
+    H, n = X.shape[0] - 1, X.shape[1]
+    re = np.ascontiguousarray(X.real)
+    im = np.ascontiguousarray(X.imag)
+    prof = np.zeros((2 * H, n), np.float64)
+    nst = lib.csref_c2r(re.ctypes.data, im.ctypes.data, int(H), int(n), prof.ctypes.data)
+    if nst < 0:
+        raise ValueError("csref_c2r: bad arguments")
+    return prof, nst
 
 
 def plan_tables(nharms, m, hidr, r_lo, h, cap=1 << 16):

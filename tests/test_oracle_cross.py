@@ -199,3 +199,74 @@ def test_oracle_detects_the_pulsar(psr):
     dd = o.remove_duplicates(raw)
     db = max(dd, key=lambda x: x.metric)
     assert db.freq == rb.freq and db.metric == rb.metric
+
+
+@pytest.mark.parametrize("nharms,maxdecim,band", [(32, 4, (1.0, 60.0)), (60, 6, (0.1, 3.0)),
+                                                  (32, 4, (3890.0, 3920.0)), (20, 3, (5.0, 12.0))])
+def test_c_port_search_equals_numpy_oracle(nharms, maxdecim, band):
+    """The two restatements of `_search_region!` (src/search.jl:1768-1894) over
+    every block of a band: the C port (the timed CPU baseline and the checker
+    of the full-size GPU runs: threaded, batched FP32 gate, its own c2r
+    transform) and the numpy oracle (one task, numpy's irfft).  Their FP32
+    interpolations round differently (sequential fmaf against numpy's float32
+    sums), so: valid trial counts exact, block sigma and S/N within 1e-5,
+    candidate (block, k, trial) sets equal outside |S/N - thr| < 1e-5 thr.
+    The bands cover the decimated levels' Nyquist cut
+    (3890-3920 Hz: 2f crosses N/2 mid-band, every harmonic from the 2nd up
+    lies beyond the spectrum), the six bin counts 120..20 of nharms 60, and
+    nharms 20 (profiles of 40, 20 and 12 bins)."""
+    from tests.fixtures import multi_spectrum
+    amps, N, dt = multi_spectrum()
+    dec = o.decimation_set(nharms, maxdecim)
+    thr = 7.0
+    op = o.SearchParams(nharms=nharms, m=16, decimations=dec, threshold=thr)
+    T, lodr, r_lo, r_hi, total, Nprof = o.search_setup(N, dt, op, band[0], band[1], 100, 2048)
+    cands, blocks = o.search_region(amps, N, T, op, r_lo, r_hi, total, Nprof, thr, thr - op.boxcar_medmargin,
+                                    keep_blocks=True)
+    port = cs_cpu.search_blocks_ex(amps, N, dt, nharms, 16, op.hidr, dec, r_lo, total, 2048, thr, 3)
+    levk = [1] + [k for k in dec if k > 1]
+    nblk = -(-total // 2048)
+    nv = np.zeros((nblk, len(levk)), np.int32)
+    sig = np.zeros((nblk, len(levk)))
+    for b in blocks:
+        nv[b.block, levk.index(b.k)] = b.nvalid
+        sig[b.block, levk.index(b.k)] = b.sigma
+    assert np.array_equal(port["nvalid"], nv)
+    assert np.any(nv[:, -1] < np.minimum(2048, total - 2048 * np.arange(nblk))) == (band[0] > 1000)
+    assert np.allclose(port["sigma"], sig, rtol=1e-5, atol=0.0)
+    want = {(c[0], c[1], c[2]): c[3].metric for c in cands}
+    got = {(int(c["blk"]), int(c["k"]), int(c["j"])): float(c["metric"]) for c in port["cands"]}
+    assert len(want) > 0
+    edge = thr * (1 + 1e-5)
+    for key in set(want) ^ set(got):
+        assert max(want.get(key, 0.0), got.get(key, 0.0)) < edge, key
+    for key in set(want) & set(got):
+        assert abs(got[key] - want[key]) <= 1e-5 * want[key], (key, got[key], want[key])
+
+
+@pytest.mark.parametrize("H", [1, 2, 3, 4, 5, 6, 7, 8, 10, 11, 12, 15, 16, 20, 30, 32, 45, 60, 64, 120])
+def test_c_port_transform_equals_irfft(H):
+    """The C port's profile-stage transform (mixed-radix FFT; direct DFT for
+    lengths with a prime factor above 5) against numpy's irfft: the
+    unnormalised brfft of (0, X[1..H]) with the imaginary part of Nyquist
+    dropped (src/search.jl:1291, :1675), for lane counts below, at and above
+    the port's lane tile."""
+    rng = np.random.default_rng(H)
+    for n in (1, 63, 64, 65, 200):
+        X = rng.standard_normal((H + 1, n)) + 1j * rng.standard_normal((H + 1, n))
+        got, nst = cs_cpu.c2r(X)
+        X[0] = 0.0
+        want = np.fft.irfft(X, 2 * H, axis=0) * (2 * H)
+        assert np.max(np.abs(got - want)) <= 1e-14 * np.max(np.abs(want)), (H, n)
+        smooth = all(f in (2, 3, 5) for f in _factors(H))
+        assert (nst > 0) == (smooth and H > 1), (H, nst)
+
+
+def _factors(n):
+    out, f = [], 2
+    while n > 1:
+        while n % f == 0:
+            out.append(f)
+            n //= f
+        f += 1
+    return out

@@ -308,22 +308,25 @@ __device__ __forceinline__ void push_cand(const WaveArgs& a, int blk, int l, int
 
 __device__ __forceinline__ float inv_sigma(float sig) { return sig > 0.0f ? 1.0f / sig : 0.0f; }
 
-// Exponent s >= 0 of the FP16 A-tile scale 2^-s: the smallest with
-// 16 * amax * 2^-s < 65504.  An interpolated amplitude is at most about
-// 2.7 * sqrt(2) times the largest |Re| or |Im| of the spectrum (the sum of the
-// 16 taps' |sinc| weights), so 16 leaves a further factor 4 of headroom for
-// the tiles.  The gate is linear in the amplitudes: it comes back exactly by
-// 2^s.
+// Exponent s of the FP16 A-tile scale 2^-s: the smallest with
+// 16 * amax * 2^-s < 65504, so that amax * 2^-s lies in [2047, 4094).  An
+// interpolated amplitude is at most about 2.7 * sqrt(2) times the largest |Re|
+// or |Im| of the spectrum (the sum of the 16 taps' |sinc| weights), so 16
+// leaves a further factor 4 of headroom for the tiles.  s is negative for a
+// faint spectrum: its amplitudes are scaled up into FP16's normal range instead
+// of rounding to subnormals or zero.  FP16 rounding of normal values and the
+// FP32 sums are exact under a power of two, so the gate comes back exactly by
+// 2^s and does not depend on the spectrum's overall scale.  |s| <= 100.
 __device__ __forceinline__ int ascale_exp(const uint32_t* amax_bits, int cidx) {
     if (!amax_bits) return 0;
     uint32_t mx = 0;   // non-negative floats order as their bits
     for (int c = 0; c <= cidx; ++c) mx = max(mx, amax_bits[c]);
     const float r = __uint_as_float(mx) * (16.0f / 65504.0f);
-    if (!(r >= 1.0f)) return 0;
     if (!(r < 1e30f)) return 100;                 // inf or NaN in the spectrum
+    if (!(r > 0.0f)) return 0;                    // every bin read is zero
     int e;
     frexpf(r, &e);                                // r = f * 2^e, f in [0.5, 1): r < 2^e
-    return min(e, 100);
+    return max(min(e, 100), -100);
 }
 __device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }   // |e| <= 126
 // The scale exponent of wave block blk's A tiles.

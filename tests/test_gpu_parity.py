@@ -279,24 +279,35 @@ def test_tensor_gate_skip_keeps_the_flagged_set(synth, ladder):
     assert np.array_equal(out[0][0], out[2][0])
 
 
-@pytest.mark.parametrize("synth", ["bf16", "fp16"])
-def test_tensor_bright_spectrum_scale_invariant(synth):
-    """A spectrum scaled by 2^17 (noise amplitudes ~1e5, past FP16's 65504)
-    reports exactly the unscaled spectrum's candidates: a power of two scales
-    every FP32 value exactly, and the FP16 A tiles carry a power-of-two range
-    scale taken from the largest component of the spectrum chunks their block
-    reads, undone in the gate."""
+@pytest.mark.parametrize("synth", ["bf16", "fp16", "fp16_split"])
+@pytest.mark.parametrize("e", [17, -36])
+def test_tensor_bright_spectrum_scale_invariant(synth, e):
+    """A spectrum scaled by 2^17 (noise amplitudes ~1e5, past FP16's 65504) or
+    by 2^-36 (every component below FP16's smallest subnormal, 2^-24) reports
+    exactly the unscaled spectrum's candidates: a power of two scales every
+    FP32 value exactly, and the FP16 A tiles carry a power-of-two range scale,
+    up or down, taken from the largest component of the spectrum chunks their
+    block reads and undone in the gate.  The FP16 gate values themselves scale
+    exactly: the tiles of both spectra hold the same 16-bit values."""
     amps, N, dt = multi_spectrum()
-    big = (amps * np.float32(2.0 ** 17)).astype(np.complex64)
-    assert np.abs(big.real).max() > 65504.0
+    scaled = (amps * np.float32(2.0 ** e)).astype(np.complex64)
+    if e > 0:
+        assert np.abs(scaled.real).max() > 65504.0
+    else:
+        assert np.abs(scaled.view(np.float32)).max() < 2.0 ** -24
     cs = _cs()
     dec = cs.decimation_set(60, 6)
     plain = _engine(cs.SearchParams(nharms=60, m=16, decimations=dec, synth="fp32"), amps, N, dt, diag=0)
     want = plain.search_raw(0.2, 180.0, 100, 2048, 8.0)
-    eng = _engine(cs.SearchParams(nharms=60, m=16, decimations=dec, synth=synth), big, N, dt, diag=0)
+    eng = _engine(cs.SearchParams(nharms=60, m=16, decimations=dec, synth=synth), scaled, N, dt, diag=2)
     got = eng.search_raw(0.2, 180.0, 100, 2048, 8.0)
     assert len(want) > 0
     assert np.array_equal(got, want)
+    if synth != "bf16":
+        ref = _engine(cs.SearchParams(nharms=60, m=16, decimations=dec, synth=synth), amps, N, dt, diag=2)
+        ref.search_raw(0.2, 180.0, 100, 2048, 8.0)
+        g = eng.gate_values() * np.float32(2.0 ** -e)
+        assert np.array_equal(g, ref.gate_values(), equal_nan=True)
 
 
 @pytest.mark.parametrize("synth", ["fp32", "fp16"])

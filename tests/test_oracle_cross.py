@@ -270,3 +270,22 @@ def _factors(n):
             n //= f
         f += 1
     return out
+
+
+@pytest.mark.parametrize("e", [17, -36])
+def test_c_port_search_is_scale_invariant(e):
+    """The checker of the device's scale tests: the C port's search of a
+    spectrum scaled by 2^e returns the unscaled spectrum's records bit for bit
+    (a power of two scales every FP32 and FP64 value of the search exactly,
+    and the S/N is a ratio)."""
+    from tests.fixtures import multi_spectrum
+    amps, N, dt = multi_spectrum()
+    dec = o.decimation_set(60, 6)
+    op = o.SearchParams(nharms=60, m=16, decimations=dec)
+    T, lodr, r_lo, r_hi, total, Nprof = o.search_setup(N, dt, op, 0.2, 30.0, 100, 2048)
+    scaled = (np.asarray(amps) * np.float32(2.0 ** e)).astype(np.complex64)
+    runs = [cs_cpu.search_blocks_ex(a, N, dt, 60, 16, op.hidr, dec, r_lo, total, 2048, 8.0, 2)
+            for a in (amps, scaled)]
+    want, got = (np.sort(r["cands"], order=["blk", "k", "j"]) for r in runs)
+    assert len(want) > 0 and np.array_equal(got, want)
+    assert np.array_equal(runs[1]["sigma"], runs[0]["sigma"] * 2.0 ** e)
